@@ -1,0 +1,419 @@
+"""ctypes binding of libcelgpu.so (include/celgpu.h).
+
+The Python names mirror the reference's entry points so that tests read
+like the reference's own drivers:
+
+  Handle                      one GPU, one stream (cel_omp / solver context)
+  Handle.matrix_from_csr      cel_sp_mat_to_csr + cel_sp_mat_distr_from_sp_mat_local
+  Matrix.to_jad               cel_sp_mat_jad_from_sp_mat_local
+  Matrix.jacobi               cel_sp_mat_distr_set_jacobi
+  Matrix.scale_diagonal       cel_sp_mat_distr_scale
+  Handle.spmv                 cel_fop_mv_axy_distr
+  Handle.dot / norm2 / axpy / xpby / jacobi_apply
+                              cel_fop_vec_distr_* (dot, norm2, scale, scale_1,
+                              vec_mult_distr_jacobi)
+  Handle.pcg_jacobi / cg / gmres_jacobi
+                              cel_cgalg_jacobi / cel_cgalg / cel_gmresalg_2jacobi
+  Handle.elm_*                cel_elmSolver* (Initialization ... Destroy)
+
+Device vectors are passed as integer device pointers (e.g.
+torch.Tensor.data_ptr()); host vectors as numpy arrays.  Every call raises
+CelgError with the library's status code on failure; there is no CPU
+fallback: if the library cannot be loaded, importing the binding fails.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcelgpu.so")
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_BREAKDOWN = 3
+ERR_NOCONV = 4
+ERR_TIMEOUT = 5
+ERR_STATE = 6
+
+FMT_CSR = 0
+FMT_JAD = 1
+X0_REF_ONES = 0
+X0_ZERO = 1
+X0_USER = 2
+PREC_FP64 = 0
+PREC_FP32_IR = 1
+SOLVER_PCG = 0
+SOLVER_CG = 1
+SOLVER_GMRES = 2
+
+
+class CelgError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} ({status})")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("x0_mode", ctypes.c_int), ("eps_abs", ctypes.c_double), ("eps_rel", ctypes.c_double),
+        ("iter_max", ctypes.c_int), ("fmt", ctypes.c_int), ("precision", ctypes.c_int),
+        ("literal_ref_bugs", ctypes.c_int), ("restart", ctypes.c_int),
+        ("inner_eps_rel", ctypes.c_double), ("inner_iter_max", ctypes.c_int),
+        ("outer_max", ctypes.c_int),
+    ]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("iter_done", ctypes.c_int), ("final_norm2", ctypes.c_double), ("bnorm", ctypes.c_double),
+        ("verified_relres", ctypes.c_double), ("err", ctypes.c_int),
+        ("arnoldi_steps", ctypes.c_int), ("history", ctypes.POINTER(ctypes.c_double)),
+        ("history_cap", ctypes.c_int), ("history_len", ctypes.c_int),
+    ]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"libcelgpu.so not built ({LIB_PATH}); run `python -m cel_v3_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    ip, dp = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+    sigs = {
+        "celg_params_default": (None, [ctypes.POINTER(Params)]),
+        "celg_create": (i, [ctypes.POINTER(vp), i, vp]),
+        "celg_destroy": (i, [vp]),
+        "celg_set_stream": (i, [vp, vp]),
+        "celg_status_string": (ctypes.c_char_p, [i]),
+        "celg_sm_count": (i, [vp, ip]),
+        "celg_mat_from_csr": (i, [vp, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_mat_from_csr_device": (i, [vp, i, i, vp, vp, vp, ctypes.POINTER(vp)]),
+        "celg_mat_destroy": (i, [vp]),
+        "celg_mat_info": (i, [vp, ip, ip, ip]),
+        "celg_mat_to_jad": (i, [vp, vp]),
+        "celg_mat_get_jad": (i, [vp, vp, vp, vp, vp]),
+        "celg_mat_jacobi": (i, [vp]),
+        "celg_mat_get_jacobi": (i, [vp, vp]),
+        "celg_mat_scale_diagonal": (i, [vp]),
+        "celg_mat_make_fp32": (i, [vp]),
+        "celg_spmv": (i, [vp, vp, i, vp, vp, i]),
+        "celg_spmv_f32": (i, [vp, vp, vp, vp, i]),
+        "celg_dot": (i, [vp, i, vp, vp, dp]),
+        "celg_norm2": (i, [vp, i, vp, dp]),
+        "celg_axpy": (i, [vp, i, d, vp, vp]),
+        "celg_xpby": (i, [vp, i, vp, d, vp]),
+        "celg_jacobi_apply": (i, [vp, vp, vp, vp]),
+        "celg_pcg_jacobi": (i, [vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+        "celg_cg": (i, [vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+        "celg_gmres_jacobi": (i, [vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+        "celg_solve_host": (i, [vp, vp, i, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+        "celg_elm_init": (i, [vp, i, i, i, vp]),
+        "celg_elm_set_solver": (i, [vp, i, ctypes.POINTER(Params), i]),
+        "celg_elm_row_start": (i, [vp, i]),
+        "celg_elm_insert": (i, [vp, i, d]),
+        "celg_elm_reinsert": (i, [vp, i, d]),
+        "celg_elm_row_completed": (i, [vp]),
+        "celg_elm_insert_rows": (i, [vp, i, i, vp, vp, vp]),
+        "celg_elm_matrix_completed": (i, [vp]),
+        "celg_elm_doit": (i, [vp, vp, ip, ip, dp]),
+        "celg_elm_redoit": (i, [vp, vp, ip, ip, dp]),
+        "celg_elm_collect_solution": (i, [vp, vp]),
+        "celg_elm_performance": (i, [vp, dp, ip, dp]),
+        "celg_elm_destroy": (i, [vp]),
+    }
+    for name, (res, args) in sigs.items():
+        if hasattr(lib, name):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def status_string(s):
+    return lib.celg_status_string(int(s)).decode()
+
+
+def _check(status, what, allow=()):
+    if status != OK and status not in allow:
+        raise CelgError(status, what)
+    return status
+
+
+def _host_ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def params(**kw):
+    """celg_params with the library defaults, overridden by keyword."""
+    p = Params()
+    lib.celg_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+class SolveInfo(dict):
+    __getattr__ = dict.__getitem__
+
+
+def _info(res, hist, status):
+    out = SolveInfo(iter_done=res.iter_done, final_norm2=res.final_norm2, bnorm=res.bnorm,
+                    verified_relres=res.verified_relres, err=res.err, status=status,
+                    arnoldi_steps=res.arnoldi_steps)
+    out["history"] = hist[: res.history_len].copy() if hist is not None else None
+    return out
+
+
+class Matrix:
+    def __init__(self, handle, ptr):
+        self.handle = handle
+        self.ptr = ptr
+
+    def info(self):
+        n, nnz, mm = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib.celg_mat_info(self.ptr, ctypes.byref(n), ctypes.byref(nnz), ctypes.byref(mm)),
+               "celg_mat_info")
+        return n.value, nnz.value, mm.value
+
+    @property
+    def n(self):
+        return self.info()[0]
+
+    def to_jad(self):
+        n = self.n
+        perm = np.zeros(max(n, 1), np.int32)
+        _check(lib.celg_mat_to_jad(self.ptr, _host_ptr(perm)), "celg_mat_to_jad")
+        return perm[:n]
+
+    def get_jad(self):
+        n, nnz, mmax = self.info()
+        perm = np.zeros(max(n, 1), np.int32)
+        jb = np.zeros(mmax + 1, np.int32)
+        jci = np.zeros(max(nnz, 1), np.int32)
+        jv = np.zeros(max(nnz, 1), np.float64)
+        _check(lib.celg_mat_get_jad(self.ptr, _host_ptr(perm), _host_ptr(jb), _host_ptr(jci),
+                                    _host_ptr(jv)), "celg_mat_get_jad")
+        return dict(perm=perm[:n], jbegin=jb, jci=jci[:nnz], jv=jv[:nnz], mmax=mmax)
+
+    def jacobi(self):
+        _check(lib.celg_mat_jacobi(self.ptr), "celg_mat_jacobi")
+        return self
+
+    def get_jacobi(self):
+        J = np.zeros(max(self.n, 1))
+        _check(lib.celg_mat_get_jacobi(self.ptr, _host_ptr(J)), "celg_mat_get_jacobi")
+        return J[: self.n]
+
+    def scale_diagonal(self):
+        _check(lib.celg_mat_scale_diagonal(self.ptr), "celg_mat_scale_diagonal")
+        return self
+
+    def make_fp32(self):
+        _check(lib.celg_mat_make_fp32(self.ptr), "celg_mat_make_fp32")
+        return self
+
+    def destroy(self):
+        if self.ptr:
+            lib.celg_mat_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Handle:
+    """One GPU and one CUDA stream (borrowed when `stream` is given)."""
+
+    def __init__(self, device=0, stream=None):
+        h = ctypes.c_void_p()
+        _check(lib.celg_create(ctypes.byref(h), int(device),
+                               ctypes.c_void_p(stream) if stream else None), "celg_create")
+        self.ptr = h
+        self.mats = []
+
+    def close(self):
+        if self.ptr:
+            for m in self.mats:
+                m.destroy()
+            self.mats = []
+            lib.celg_destroy(self.ptr)
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sm_count(self):
+        s = ctypes.c_int()
+        _check(lib.celg_sm_count(self.ptr, ctypes.byref(s)), "celg_sm_count")
+        return s.value
+
+    def set_stream(self, stream):
+        _check(lib.celg_set_stream(self.ptr, ctypes.c_void_p(stream) if stream else None),
+               "celg_set_stream")
+
+    # ---- matrices
+    def matrix_from_csr(self, rp, ci, v, index_base=0):
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, np.float64)
+        m = ctypes.c_void_p()
+        n = rp.size - 1
+        _check(lib.celg_mat_from_csr(self.ptr, n, int(ci.size), _host_ptr(rp), _host_ptr(ci),
+                                     _host_ptr(v), int(index_base), ctypes.byref(m)),
+               "celg_mat_from_csr")
+        mat = Matrix(self, m)
+        self.mats.append(mat)
+        return mat
+
+    def matrix_from_csr_device(self, n, nnz, rp_d, ci_d, v_d):
+        m = ctypes.c_void_p()
+        _check(lib.celg_mat_from_csr_device(self.ptr, int(n), int(nnz), ctypes.c_void_p(rp_d),
+                                            ctypes.c_void_p(ci_d), ctypes.c_void_p(v_d),
+                                            ctypes.byref(m)), "celg_mat_from_csr_device")
+        mat = Matrix(self, m)
+        self.mats.append(mat)
+        return mat
+
+    # ---- operators on device pointers
+    def spmv(self, mat, x_d, y_d, fmt=FMT_CSR, accumulate=False):
+        _check(lib.celg_spmv(self.ptr, mat.ptr, int(fmt), ctypes.c_void_p(x_d),
+                             ctypes.c_void_p(y_d), int(accumulate)), "celg_spmv")
+
+    def spmv_f32(self, mat, x_d, y_d, accumulate=False):
+        _check(lib.celg_spmv_f32(self.ptr, mat.ptr, ctypes.c_void_p(x_d), ctypes.c_void_p(y_d),
+                                 int(accumulate)), "celg_spmv_f32")
+
+    def dot(self, n, a_d, b_d):
+        out = ctypes.c_double()
+        _check(lib.celg_dot(self.ptr, int(n), ctypes.c_void_p(a_d), ctypes.c_void_p(b_d),
+                            ctypes.byref(out)), "celg_dot")
+        return out.value
+
+    def norm2(self, n, a_d):
+        out = ctypes.c_double()
+        _check(lib.celg_norm2(self.ptr, int(n), ctypes.c_void_p(a_d), ctypes.byref(out)),
+               "celg_norm2")
+        return out.value
+
+    def axpy(self, n, alpha, x_d, y_d):
+        _check(lib.celg_axpy(self.ptr, int(n), float(alpha), ctypes.c_void_p(x_d),
+                             ctypes.c_void_p(y_d)), "celg_axpy")
+
+    def xpby(self, n, x_d, beta, y_d):
+        _check(lib.celg_xpby(self.ptr, int(n), ctypes.c_void_p(x_d), float(beta),
+                             ctypes.c_void_p(y_d)), "celg_xpby")
+
+    def jacobi_apply(self, mat, r_d, z_d):
+        _check(lib.celg_jacobi_apply(self.ptr, mat.ptr, ctypes.c_void_p(r_d), ctypes.c_void_p(z_d)),
+               "celg_jacobi_apply")
+
+    # ---- solvers on device pointers
+    def _solve(self, fn, name, mat, b_d, x_d, p, history):
+        res = Result()
+        hist = None
+        if history:
+            cap = history if isinstance(history, int) and history > 1 else p.iter_max + 1
+            hist = np.zeros(cap)
+            res.history = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            res.history_cap = cap
+        st = fn(self.ptr, mat.ptr, ctypes.c_void_p(b_d), ctypes.c_void_p(x_d), ctypes.byref(p),
+                ctypes.byref(res))
+        _check(st, name, allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return _info(res, hist, st)
+
+    def pcg_jacobi(self, mat, b_d, x_d, p=None, history=False, **kw):
+        p = p or params(**kw)
+        return self._solve(lib.celg_pcg_jacobi, "celg_pcg_jacobi", mat, b_d, x_d, p, history)
+
+    def cg(self, mat, b_d, x_d, p=None, history=False, **kw):
+        p = p or params(**kw)
+        return self._solve(lib.celg_cg, "celg_cg", mat, b_d, x_d, p, history)
+
+    def gmres_jacobi(self, mat, b_d, x_d, p=None, history=False, **kw):
+        p = p or params(**kw)
+        return self._solve(lib.celg_gmres_jacobi, "celg_gmres_jacobi", mat, b_d, x_d, p, history)
+
+    def solve_host(self, mat, b, x=None, solver=SOLVER_PCG, p=None, **kw):
+        """Solve from host arrays (the copies are part of the call)."""
+        p = p or params(**kw)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b) if x is None else np.ascontiguousarray(x, np.float64)
+        res = Result()
+        st = lib.celg_solve_host(self.ptr, mat.ptr, int(solver), _host_ptr(b), _host_ptr(x),
+                                 ctypes.byref(p), ctypes.byref(res))
+        _check(st, "celg_solve_host", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return x, _info(res, None, st)
+
+    # ---- ELM assembly API
+    def elm_init(self, n_total, n_local=None, row_low=1, nnz_hint=(7, 0)):
+        hint = (ctypes.c_int * 2)(*nnz_hint)
+        _check(lib.celg_elm_init(self.ptr, int(n_total), int(n_local if n_local is not None else n_total),
+                                 int(row_low), hint), "celg_elm_init")
+
+    def elm_set_solver(self, solver, p=None, diag_scaling=True, **kw):
+        p = p or params(**kw)
+        _check(lib.celg_elm_set_solver(self.ptr, int(solver), ctypes.byref(p), int(diag_scaling)),
+               "celg_elm_set_solver")
+
+    def elm_row_start(self, row):
+        _check(lib.celg_elm_row_start(self.ptr, int(row)), "celg_elm_row_start")
+
+    def elm_insert(self, col, value):
+        _check(lib.celg_elm_insert(self.ptr, int(col), float(value)), "celg_elm_insert")
+
+    def elm_reinsert(self, col, value):
+        _check(lib.celg_elm_reinsert(self.ptr, int(col), float(value)), "celg_elm_reinsert")
+
+    def elm_row_completed(self):
+        _check(lib.celg_elm_row_completed(self.ptr), "celg_elm_row_completed")
+
+    def elm_insert_rows(self, first_row, rp, ci, v):
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, np.float64)
+        _check(lib.celg_elm_insert_rows(self.ptr, int(first_row), rp.size - 1, _host_ptr(rp),
+                                        _host_ptr(ci), _host_ptr(v)), "celg_elm_insert_rows")
+
+    def elm_matrix_completed(self):
+        _check(lib.celg_elm_matrix_completed(self.ptr), "celg_elm_matrix_completed")
+
+    def elm_doit(self, b, redo=False):
+        b = np.ascontiguousarray(b, np.float64)
+        ierr, niter, ftol = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        fn = lib.celg_elm_redoit if redo else lib.celg_elm_doit
+        st = fn(self.ptr, _host_ptr(b), ctypes.byref(ierr), ctypes.byref(niter), ctypes.byref(ftol))
+        _check(st, "celg_elm_doit", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return ierr.value, niter.value, ftol.value
+
+    def elm_collect_solution(self, n, out=None):
+        x = np.zeros(n) if out is None else out
+        _check(lib.celg_elm_collect_solution(self.ptr, _host_ptr(x)), "celg_elm_collect_solution")
+        return x
+
+    def elm_performance(self):
+        ms, it, bpi = ctypes.c_double(), ctypes.c_int(), ctypes.c_double()
+        _check(lib.celg_elm_performance(self.ptr, ctypes.byref(ms), ctypes.byref(it),
+                                        ctypes.byref(bpi)), "celg_elm_performance")
+        return ms.value, it.value, bpi.value
+
+    def elm_destroy(self):
+        _check(lib.celg_elm_destroy(self.ptr), "celg_elm_destroy")

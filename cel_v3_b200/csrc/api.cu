@@ -1,0 +1,615 @@
+// api.cu -- the extern "C" entry points of libcelgpu.so declared in
+// include/celgpu.h: handle, matrix upload and set-up, operators, solvers and
+// the ELM assembly API.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "tile_kernels.cuh"
+
+namespace celg {
+
+int cuda_status(cudaError_t e, const char* what) {
+  if (std::getenv("CELG_VERBOSE"))
+    std::fprintf(stderr, "libcelgpu: %s failed: %s\n", what, cudaGetErrorString(e));
+  (void)cudaGetLastError();  // clear sticky-free errors
+  return CELG_ERR_CUDA;
+}
+
+// ---- matrix set-up kernels ---------------------------------------------------
+
+// 0-based conversion, padding of the row-pointer tail and validation.
+// bad[0] is set when row_ptr is not monotone or its ends are wrong, bad[1]
+// when a column index is out of range.
+__global__ void csr_prepare_kernel(int n, int nnz, int base, int* rp, int* ci, int pad_rp,
+                                   int* bad) {
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long stride = (long)gridDim.x * blockDim.x;
+  for (long i = tid; i <= n; i += stride) {
+    const int v = rp[i] - base;
+    rp[i] = v;
+    if (v < 0 || v > nnz) atomicExch(&bad[0], 1);
+  }
+  for (long k = tid; k < nnz; k += stride) {
+    const int c = ci[k] - base;
+    ci[k] = c;
+    if (c < 0 || c >= n) atomicExch(&bad[1], 1);
+  }
+  for (long i = tid; i < pad_rp; i += stride) rp[n + 1 + i] = nnz;
+}
+
+__global__ void csr_check_rows_kernel(int n, int nnz, const int* rp, int* bad) {
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long stride = (long)gridDim.x * blockDim.x;
+  if (tid == 0 && (rp[0] != 0 || rp[n] != nnz)) atomicExch(&bad[0], 1);
+  for (long i = tid; i < n; i += stride)
+    if (rp[i + 1] < rp[i]) atomicExch(&bad[0], 1);
+}
+
+__global__ void row_len_kernel(int n, const int* __restrict__ rp, int* __restrict__ len_key,
+                               int* __restrict__ idx, int* __restrict__ maxlen) {
+  int best = 0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int L = rp[i + 1] - rp[i];
+    len_key[i] = L;
+    idx[i] = (int)i;
+    best = max(best, L);
+  }
+  for (int off = 16; off >= 1; off >>= 1) best = max(best, __shfl_xor_sync(0xffffffffu, best, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(maxlen, best);
+}
+
+// key = mmax - len, so an ascending stable sort gives descending lengths with
+// ties in ascending row order (the reference's dcsort order)
+__global__ void jad_key_kernel(int n, int mmax, int* key, int* hist) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int L = key[i];
+    atomicAdd(&hist[L], 1);
+    key[i] = mmax - L;
+  }
+}
+
+__global__ void jad_fill_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                const double* __restrict__ v, const int* __restrict__ perm,
+                                const int* __restrict__ jb, int* __restrict__ jci,
+                                double* __restrict__ jv) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int r = perm[i];
+    const int b = rp[r], L = rp[r + 1] - b;
+    for (int k = 0; k < L; ++k) {
+      const long q = (long)jb[k] + i;
+      jci[q] = ci[b + k];
+      jv[q] = v[b + k];
+    }
+  }
+}
+
+static int ew_grid(celg_handle* h, long n) {
+  return (int)std::max(1L, std::min((n + 255) / 256, (long)h->sms * 16));
+}
+
+static void free_mat_arrays(celg_mat* m) {
+  cudaFree(m->csr.rp);
+  cudaFree(m->csr.ci);
+  cudaFree(m->csr.v);
+  cudaFree(m->csr.v32);
+  cudaFree(m->jad.begin);
+  cudaFree(m->jad.ci);
+  cudaFree(m->jad.v);
+  cudaFree(m->jad.perm);
+  cudaFree(m->diag);
+  cudaFree(m->jacobi);
+  cudaFree(m->jacobi32);
+  cudaFree(m->scale);
+}
+
+// Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.
+static int alloc_csr(celg_mat* m, int n, int nnz) {
+  m->csr.n = n;
+  m->csr.nnz = nnz;
+  CELG_CUDA(cudaMalloc(&m->csr.rp, sizeof(int) * ((size_t)n + 1 + 8)));
+  CELG_CUDA(cudaMalloc(&m->csr.ci, sizeof(int) * ((size_t)nnz + 8)));
+  CELG_CUDA(cudaMalloc(&m->csr.v, sizeof(double) * ((size_t)nnz + 8)));
+  CELG_CUDA(cudaMemsetAsync(m->csr.ci + nnz, 0, sizeof(int) * 8, m->h->stream));
+  CELG_CUDA(cudaMemsetAsync(m->csr.v + nnz, 0, sizeof(double) * 8, m->h->stream));
+  return CELG_OK;
+}
+
+static int finish_csr(celg_handle* h, celg_mat* m, int base) {
+  const int n = m->csr.n, nnz = m->csr.nnz;
+  int* bad = h->err_d + 2;
+  CELG_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int), h->stream));
+  csr_prepare_kernel<<<ew_grid(h, std::max(n + 1, nnz)), 256, 0, h->stream>>>(
+      n, nnz, base, m->csr.rp, m->csr.ci, 8, bad);
+  CELG_CUDA(cudaGetLastError());
+  csr_check_rows_kernel<<<ew_grid(h, n + 1), 256, 0, h->stream>>>(n, nnz, m->csr.rp, bad);
+  CELG_CUDA(cudaGetLastError());
+  int hb[2] = {0, 0};
+  CELG_CUDA(cudaMemcpyAsync(hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  if (hb[0] || hb[1]) return CELG_ERR_ARG;
+  return csr_compute_cap(h, m->csr);
+}
+
+static int build_jad(celg_mat* m) {
+  celg_handle* h = m->h;
+  const int n = m->csr.n, nnz = m->csr.nnz;
+  JadDev& J = m->jad;
+  cudaFree(J.begin);
+  cudaFree(J.ci);
+  cudaFree(J.v);
+  cudaFree(J.perm);
+  J = JadDev();
+  int *key = nullptr, *key2 = nullptr, *idx = nullptr, *hist = nullptr;
+  void* tmp = nullptr;
+  int st = CELG_OK;
+  auto fail = [&](cudaError_t e, const char* w) {
+    st = cuda_status(e, w);
+  };
+  int* maxlen_d = h->err_d + 4;
+  int mmax = 0;
+  cudaError_t e;
+  do {
+    if ((e = cudaMalloc(&key, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&key2, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&idx, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&J.perm, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
+    cudaMemsetAsync(maxlen_d, 0, sizeof(int), h->stream);
+    if (n > 0) row_len_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, m->csr.rp, key, idx, maxlen_d);
+    cudaMemcpyAsync(&mmax, maxlen_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) { fail(e, "jad lengths"); break; }
+    if ((e = cudaMalloc(&hist, sizeof(int) * (size_t)(mmax + 1))) != cudaSuccess) { fail(e, "jad"); break; }
+    cudaMemsetAsync(hist, 0, sizeof(int) * (size_t)(mmax + 1), h->stream);
+    if (n > 0) jad_key_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, mmax, key, hist);
+    int bits = 1;
+    while ((1 << bits) <= mmax) ++bits;
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key2, idx, J.perm, n, 0, bits,
+                                    h->stream);
+    if ((e = cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16))) != cudaSuccess) { fail(e, "jad"); break; }
+    if (n > 0 && (e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, key, key2, idx, J.perm, n, 0,
+                                                      bits, h->stream)) != cudaSuccess) {
+      fail(e, "radix sort");
+      break;
+    }
+    std::vector<int> hh((size_t)mmax + 1), jb((size_t)mmax + 1);
+    cudaMemcpyAsync(hh.data(), hist, sizeof(int) * (size_t)(mmax + 1), cudaMemcpyDeviceToHost,
+                    h->stream);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) { fail(e, "jad hist"); break; }
+    // rows with length > k, k = 0..mmax-1
+    int above = n;
+    jb[0] = 0;
+    for (int k = 0; k < mmax; ++k) {
+      above -= hh[(size_t)k];  // remove rows of length k
+      jb[(size_t)k + 1] = jb[(size_t)k] + above;
+    }
+    if ((e = cudaMalloc(&J.begin, sizeof(int) * (size_t)(mmax + 1))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&J.ci, sizeof(int) * ((size_t)nnz + 8))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&J.v, sizeof(double) * ((size_t)nnz + 8))) != cudaSuccess) { fail(e, "jad"); break; }
+    cudaMemcpyAsync(J.begin, jb.data(), sizeof(int) * (size_t)(mmax + 1), cudaMemcpyHostToDevice,
+                    h->stream);
+    if (n > 0)
+      jad_fill_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, m->csr.rp, m->csr.ci, m->csr.v, J.perm,
+                                                          J.begin, J.ci, J.v);
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) { fail(e, "jad fill"); break; }
+    J.mmax = mmax;
+  } while (0);
+  cudaFree(key);
+  cudaFree(key2);
+  cudaFree(idx);
+  cudaFree(hist);
+  cudaFree(tmp);
+  return st;
+}
+
+}  // namespace celg
+
+using namespace celg;
+
+// ---------------------------------------------------------------------------
+// handle
+// ---------------------------------------------------------------------------
+
+extern "C" void celg_params_default(celg_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->x0_mode = CELG_X0_ZERO;
+  p->eps_abs = 0.0;
+  p->eps_rel = 1e-8;
+  p->iter_max = 1000;
+  p->fmt = CELG_FMT_CSR;
+  p->precision = CELG_PREC_FP64;
+  p->literal_ref_bugs = 0;
+  p->restart = 30;
+  p->inner_eps_rel = 1e-4;
+  p->inner_iter_max = 1000;
+  p->outer_max = 20;
+}
+
+extern "C" const char* celg_status_string(int s) {
+  switch (s) {
+    case CELG_OK: return "ok";
+    case CELG_ERR_ARG: return "invalid argument";
+    case CELG_ERR_CUDA: return "CUDA error";
+    case CELG_ERR_BREAKDOWN: return "breakdown (non-finite step length)";
+    case CELG_ERR_NOCONV: return "iteration limit reached";
+    case CELG_ERR_TIMEOUT: return "device wait timed out";
+    case CELG_ERR_STATE: return "call out of order";
+    default: return "unknown status";
+  }
+}
+
+extern "C" int celg_create(celg_handle** out, int device, void* stream) {
+  if (!out) return CELG_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  CELG_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(device));
+  celg_handle* h = new celg_handle();
+  h->device = device;
+  if (stream) {
+    h->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete h;
+      return CELG_ERR_CUDA;
+    }
+    h->own_stream = true;
+  }
+  cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMalloc(&h->ticket, 64) != cudaSuccess || cudaMalloc(&h->err_d, 64) != cudaSuccess ||
+      cudaMalloc(&h->scal_d, 64 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost(&h->scal_h, 64 * sizeof(double)) != cudaSuccess ||
+      cudaEventCreate(&h->ev0) != cudaSuccess || cudaEventCreate(&h->ev1) != cudaSuccess) {
+    celg_destroy(h);
+    return CELG_ERR_CUDA;
+  }
+  cudaMemset(h->ticket, 0, 64);
+  cudaMemset(h->err_d, 0, 64);
+  cudaDeviceSynchronize();
+  *out = h;
+  return CELG_OK;
+}
+
+extern "C" int celg_elm_destroy(celg_handle* h);
+
+extern "C" int celg_destroy(celg_handle* h) {
+  if (!h) return CELG_OK;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->elm) celg_elm_destroy(h);
+  graph_cache_clear(h);
+  cudaFree(h->partials);
+  cudaFree(h->sb);
+  cudaFree(h->sx);
+  cudaFree(h->f32);
+  cudaFree(h->ir_d);
+  cudaFree(h->ticket);
+  cudaFree(h->err_d);
+  cudaFree(h->scal_d);
+  cudaFreeHost(h->scal_h);
+  cudaFree(h->wr);
+  cudaFree(h->wp);
+  cudaFree(h->wv);
+  cudaFree(h->state_d);
+  cudaFreeHost(h->state_h);
+  cudaFree(h->hist_d);
+  if (h->ev0) cudaEventDestroy(h->ev0);
+  if (h->ev1) cudaEventDestroy(h->ev1);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return CELG_OK;
+}
+
+extern "C" int celg_set_stream(celg_handle* h, void* stream) {
+  if (!h) return CELG_ERR_ARG;
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  h->own_stream = false;
+  h->stream = (cudaStream_t)stream;
+  if (!stream) {
+    CELG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return CELG_OK;
+}
+
+extern "C" int celg_sm_count(celg_handle* h, int* sms) {
+  if (!h || !sms) return CELG_ERR_ARG;
+  *sms = h->sms;
+  return CELG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// matrix
+// ---------------------------------------------------------------------------
+
+extern "C" int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr,
+                                 const int* cols, const double* vals, int index_base,
+                                 celg_mat** out) {
+  if (!h || !out || n < 0 || nnz < 0 || !row_ptr || (nnz > 0 && (!cols || !vals)) ||
+      (index_base != 0 && index_base != 1))
+    return CELG_ERR_ARG;
+  *out = nullptr;
+  CELG_CUDA(cudaSetDevice(h->device));
+  celg_mat* m = new celg_mat();
+  m->h = h;
+  int st = alloc_csr(m, n, nnz);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(m->csr.rp, row_ptr, sizeof(int) * ((size_t)n + 1),
+                                    cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->csr.ci, cols, sizeof(int) * (size_t)nnz, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->csr.v, vals, sizeof(double) * (size_t)nnz, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "matrix upload");
+  }
+  if (!st) st = finish_csr(h, m, index_base);
+  if (st) {
+    cudaStreamSynchronize(h->stream);
+    free_mat_arrays(m);
+    delete m;
+    return st;
+  }
+  *out = m;
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_d,
+                                        const int* cols_d, const double* vals_d, celg_mat** out) {
+  if (!h || !out || n < 0 || nnz < 0 || !row_ptr_d || (nnz > 0 && (!cols_d || !vals_d)))
+    return CELG_ERR_ARG;
+  *out = nullptr;
+  CELG_CUDA(cudaSetDevice(h->device));
+  celg_mat* m = new celg_mat();
+  m->h = h;
+  int st = alloc_csr(m, n, nnz);
+  if (!st) {
+    cudaError_t e = cudaMemcpyAsync(m->csr.rp, row_ptr_d, sizeof(int) * ((size_t)n + 1),
+                                    cudaMemcpyDeviceToDevice, h->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->csr.ci, cols_d, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToDevice,
+                          h->stream);
+    if (e == cudaSuccess && nnz > 0)
+      e = cudaMemcpyAsync(m->csr.v, vals_d, sizeof(double) * (size_t)nnz, cudaMemcpyDeviceToDevice,
+                          h->stream);
+    if (e != cudaSuccess) st = cuda_status(e, "matrix copy");
+  }
+  if (!st) st = finish_csr(h, m, 0);
+  if (st) {
+    cudaStreamSynchronize(h->stream);
+    free_mat_arrays(m);
+    delete m;
+    return st;
+  }
+  *out = m;
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_destroy(celg_mat* m) {
+  if (!m) return CELG_OK;
+  celg_handle* h = m->h;
+  cudaSetDevice(h->device);
+  cudaStreamSynchronize(h->stream);
+  // cached solve graphs may reference this matrix
+  graph_cache_drop_matrix(h, m);
+  free_mat_arrays(m);
+  delete m;
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_info(const celg_mat* m, int* n, int* nnz, int* jad_mmax) {
+  if (!m) return CELG_ERR_ARG;
+  if (n) *n = m->csr.n;
+  if (nnz) *nnz = m->csr.nnz;
+  if (jad_mmax) *jad_mmax = m->jad.mmax;
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_to_jad(celg_mat* m, int* perm_out) {
+  if (!m) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(m->h->device));
+  int st = build_jad(m);
+  if (st) return st;
+  if (perm_out && m->csr.n > 0)
+    CELG_CUDA(cudaMemcpy(perm_out, m->jad.perm, sizeof(int) * (size_t)m->csr.n, cudaMemcpyDeviceToHost));
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_get_jad(const celg_mat* m, int* perm, int* begin, int* cols, double* vals) {
+  if (!m || m->jad.mmax < 0) return CELG_ERR_STATE;
+  CELG_CUDA(cudaStreamSynchronize(m->h->stream));
+  const size_t n = (size_t)m->csr.n, nnz = (size_t)m->csr.nnz;
+  if (perm && n) CELG_CUDA(cudaMemcpy(perm, m->jad.perm, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  if (begin) CELG_CUDA(cudaMemcpy(begin, m->jad.begin, sizeof(int) * ((size_t)m->jad.mmax + 1), cudaMemcpyDeviceToHost));
+  if (cols && nnz) CELG_CUDA(cudaMemcpy(cols, m->jad.ci, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
+  if (vals && nnz) CELG_CUDA(cudaMemcpy(vals, m->jad.v, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_jacobi(celg_mat* m) {
+  if (!m) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(m->h->device));
+  int st = launch_jacobi_setup(m->h, m);
+  if (st) return st;
+  CELG_CUDA(cudaStreamSynchronize(m->h->stream));
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_get_jacobi(const celg_mat* m, double* jacobi_host) {
+  if (!m || !jacobi_host) return CELG_ERR_ARG;
+  if (!m->jacobi) return CELG_ERR_STATE;
+  CELG_CUDA(cudaStreamSynchronize(m->h->stream));
+  if (m->csr.n)
+    CELG_CUDA(cudaMemcpy(jacobi_host, m->jacobi, sizeof(double) * (size_t)m->csr.n, cudaMemcpyDeviceToHost));
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_scale_diagonal(celg_mat* m) {
+  if (!m) return CELG_ERR_ARG;
+  if (m->scaled) return CELG_OK;
+  CELG_CUDA(cudaSetDevice(m->h->device));
+  m->scaled = false;
+  int st = launch_jacobi_setup(m->h, m);  // unscaled diagonal
+  if (!st) st = launch_row_scale(m->h, m);
+  if (st) return st;
+  m->scaled = true;
+  st = launch_jacobi_setup(m->h, m);  // jacobi = sqrt|d| / d
+  if (st) return st;
+  if (m->jad.mmax >= 0) st = build_jad(m);
+  if (!st && m->csr.v32) st = launch_to_f32(m->h, m->csr.nnz, m->csr.v, m->csr.v32);
+  if (st) return st;
+  CELG_CUDA(cudaStreamSynchronize(m->h->stream));
+  return CELG_OK;
+}
+
+extern "C" int celg_mat_make_fp32(celg_mat* m) {
+  if (!m) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(m->h->device));
+  if (!m->csr.v32) {
+    CELG_CUDA(cudaMalloc(&m->csr.v32, sizeof(float) * ((size_t)m->csr.nnz + 8)));
+    CELG_CUDA(cudaMemsetAsync(m->csr.v32 + m->csr.nnz, 0, sizeof(float) * 8, m->h->stream));
+  }
+  int st = launch_to_f32(m->h, m->csr.nnz, m->csr.v, m->csr.v32);
+  if (!st && m->jacobi) {
+    if (!m->jacobi32) CELG_CUDA(cudaMalloc(&m->jacobi32, sizeof(float) * std::max(1, m->csr.n)));
+    st = launch_to_f32(m->h, m->csr.n, m->jacobi, m->jacobi32);
+  }
+  if (st) return st;
+  CELG_CUDA(cudaStreamSynchronize(m->h->stream));
+  return CELG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// operators
+// ---------------------------------------------------------------------------
+
+extern "C" int celg_spmv(celg_handle* h, const celg_mat* m, int fmt, const double* x_d, double* y_d,
+                         int accumulate) {
+  if (!h || !m || (m->csr.n > 0 && (!x_d || !y_d))) return CELG_ERR_ARG;
+  if (fmt == CELG_FMT_JAD) {
+    if (accumulate) return CELG_ERR_ARG;  // the reference's JAD kernel overwrites y
+    return launch_spmv_jad(h, m->csr, m->jad, x_d, y_d);
+  }
+  if (fmt != CELG_FMT_CSR) return CELG_ERR_ARG;
+  return launch_spmv_csr(h, m->csr, x_d, y_d, accumulate);
+}
+
+extern "C" int celg_spmv_f32(celg_handle* h, const celg_mat* m, const float* x_d, float* y_d,
+                             int accumulate) {
+  if (!h || !m || (m->csr.n > 0 && (!x_d || !y_d))) return CELG_ERR_ARG;
+  return launch_spmv_csr_f32(h, m->csr, x_d, y_d, accumulate);
+}
+
+static int blas_scalar(celg_handle* h, long n, const double* a, const double* b, double* out,
+                       int take_sqrt) {
+  if (!h || !out || n < 0 || (n > 0 && (!a || !b))) return CELG_ERR_ARG;
+  int st = launch_dot(h, n, a, b, h->scal_d, take_sqrt);
+  if (st) return st;
+  if (n == 0) CELG_CUDA(cudaMemsetAsync(h->scal_d, 0, sizeof(double), h->stream));
+  CELG_CUDA(cudaMemcpyAsync(h->scal_h, h->scal_d, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  *out = h->scal_h[0];
+  return CELG_OK;
+}
+
+extern "C" int celg_dot(celg_handle* h, int n, const double* a_d, const double* b_d, double* out) {
+  return blas_scalar(h, n, a_d, b_d, out, 0);
+}
+
+extern "C" int celg_norm2(celg_handle* h, int n, const double* a_d, double* out) {
+  return blas_scalar(h, n, a_d, a_d, out, 1);
+}
+
+extern "C" int celg_axpy(celg_handle* h, int n, double alpha, const double* x_d, double* y_d) {
+  if (!h || n < 0) return CELG_ERR_ARG;
+  return launch_axpy(h, n, alpha, x_d, y_d);
+}
+
+extern "C" int celg_xpby(celg_handle* h, int n, const double* x_d, double beta, double* y_d) {
+  if (!h || n < 0) return CELG_ERR_ARG;
+  return launch_xpby(h, n, x_d, beta, y_d);
+}
+
+extern "C" int celg_jacobi_apply(celg_handle* h, const celg_mat* m, const double* r_d, double* z_d) {
+  if (!h || !m) return CELG_ERR_ARG;
+  if (!m->jacobi) return CELG_ERR_STATE;
+  return launch_mul(h, m->csr.n, r_d, m->jacobi, z_d);
+}
+
+// ---------------------------------------------------------------------------
+// solvers
+// ---------------------------------------------------------------------------
+
+static int check_solve_args(celg_handle* h, celg_mat* m, const double* b, double* x,
+                            const celg_params* p) {
+  if (!h || !m || !p || (m->csr.n > 0 && (!b || !x))) return CELG_ERR_ARG;
+  if (p->fmt != CELG_FMT_CSR && p->fmt != CELG_FMT_JAD) return CELG_ERR_ARG;
+  if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER) return CELG_ERR_ARG;
+  if (m->h != h) return CELG_ERR_ARG;
+  return CELG_OK;
+}
+
+extern "C" int celg_pcg_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
+                               const celg_params* p, celg_result* res) {
+  int st = check_solve_args(h, m, b_d, x_d, p);
+  if (st) return st;
+  CELG_CUDA(cudaSetDevice(h->device));
+  if (p->precision == CELG_PREC_FP32_IR) return ir_solve(h, m, b_d, x_d, p, res);
+  return pcg_solve(h, m, b_d, x_d, p, res);
+}
+
+extern "C" int celg_cg(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
+                       const celg_params* p, celg_result* res) {
+  int st = check_solve_args(h, m, b_d, x_d, p);
+  if (st) return st;
+  CELG_CUDA(cudaSetDevice(h->device));
+  return cg_solve(h, m, b_d, x_d, p, res);
+}
+
+extern "C" int celg_gmres_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
+                                 const celg_params* p, celg_result* res) {
+  int st = check_solve_args(h, m, b_d, x_d, p);
+  if (st) return st;
+  CELG_CUDA(cudaSetDevice(h->device));
+  return gmres_solve(h, m, b_d, x_d, p, res);
+}
+
+extern "C" int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_host,
+                               double* x_host, const celg_params* p, celg_result* res) {
+  int st = check_solve_args(h, m, b_host, x_host, p);
+  if (st) return st;
+  CELG_CUDA(cudaSetDevice(h->device));
+  const size_t n = (size_t)m->csr.n;
+  if (n > h->scap || !h->sb) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(h->sb);
+    cudaFree(h->sx);
+    h->sb = h->sx = nullptr;
+    const size_t cap = std::max<size_t>(n, 1024);
+    CELG_CUDA(cudaMalloc(&h->sb, sizeof(double) * cap));
+    CELG_CUDA(cudaMalloc(&h->sx, sizeof(double) * cap));
+    h->scap = cap;
+  }
+  // host -> device copies of this solve's inputs, on the handle's stream
+  CELG_CUDA(cudaMemcpyAsync(h->sb, b_host, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+  if (p->x0_mode == CELG_X0_USER)
+    CELG_CUDA(cudaMemcpyAsync(h->sx, x_host, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+  int ret;
+  if (solver == CELG_SOLVER_PCG) ret = celg_pcg_jacobi(h, m, h->sb, h->sx, p, res);
+  else if (solver == CELG_SOLVER_CG) ret = cg_solve(h, m, h->sb, h->sx, p, res);
+  else if (solver == CELG_SOLVER_GMRES) ret = gmres_solve(h, m, h->sb, h->sx, p, res);
+  else ret = CELG_ERR_ARG;
+  if (ret == CELG_OK || ret == CELG_ERR_NOCONV) {
+    // device -> host copy of the solution
+    CELG_CUDA(cudaMemcpyAsync(x_host, h->sx, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+  }
+  return ret;
+}

@@ -1,0 +1,178 @@
+// celg_device.cuh -- device-side building blocks shared by the libcelgpu
+// kernels: bulk-copy/mbarrier wrappers (sm_90+ PTX, used here on sm_100a),
+// bounded waits, and the fixed-order block-tree reduction.
+//
+// Reduction order (kept identical in the CPU oracle so that a GPU solve can
+// be reproduced bit for bit):
+//   * a vector of length n is cut into tiles of kTile = 1024 consecutive
+//     elements; lane j (0..255) of the tile sums elements j, j+256, j+512,
+//     j+768 from 0.0 in that order;
+//   * each 32-lane warp folds its lanes with a butterfly (xor 16, 8, 4, 2, 1);
+//   * the eight warp sums are added in warp order, giving the tile partial;
+//   * the tile partials are reduced the same way (lane j sums partials j,
+//     j+256, ... then butterfly and warp order) by the last CTA to finish.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace celg {
+
+constexpr int kTile = 1024;     // rows per reduction tile
+constexpr int kLanes = 256;     // lanes per tile
+constexpr int kSub = 256;       // rows per pipeline sub-tile of the CSR kernel
+constexpr int kSubPerTile = kTile / kSub;
+constexpr int kStages = 4;      // bulk-copy pipeline depth of the CSR kernel
+constexpr int kConsumerWarps = 8;
+constexpr int kCsrThreads = (kConsumerWarps + 1) * 32;  // + one producer warp
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // bounded wait on an mbarrier: 2 s
+
+constexpr int kErrTimeout = 5;   // CELG_ERR_TIMEOUT
+constexpr int kErrBreakdown = 3; // CELG_ERR_BREAKDOWN
+
+// Cross-block reduction context: per-tile partials (nred rows of ntiles) and
+// a completion ticket reset by the last block.
+struct RedCtx {
+  double* partials;
+  unsigned* ticket;
+  long ntiles;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for the given phase parity; give up after about kWaitLimitNs, record
+// CELG_ERR_TIMEOUT in *err and return false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned i = 1;; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63u) == 0 && global_ns() - t0 > limit_ns) break;
+  }
+  atomicExch(err, kErrTimeout);
+  return false;
+}
+
+// Untiled bulk copy global -> shared, completion signalled on `bar`.
+// dst, src 16-byte aligned and bytes a multiple of 16 (checked by callers).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// exact IEEE binary64 operations with no contraction into FMA
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+
+template <typename VT>
+__device__ __forceinline__ VT vadd(VT a, VT b);
+template <>
+__device__ __forceinline__ double vadd<double>(double a, double b) { return __dadd_rn(a, b); }
+template <>
+__device__ __forceinline__ float vadd<float>(float a, float b) { return __fadd_rn(a, b); }
+template <typename VT>
+__device__ __forceinline__ VT vmul(VT a, VT b);
+template <>
+__device__ __forceinline__ double vmul<double>(double a, double b) { return __dmul_rn(a, b); }
+template <>
+__device__ __forceinline__ float vmul<float>(float a, float b) { return __fmul_rn(a, b); }
+
+__device__ __forceinline__ double warp_fold(double v) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));
+  return v;
+}
+
+// Fold one value per lane of a 256-thread group (lane = tid 0..255) into
+// thread 0.  `scratch` holds 8 doubles of shared memory.  All 256 threads of
+// the group must call it; `bar_id`/named barrier restricts the sync to them.
+__device__ __forceinline__ double group_fold256(double v, double* scratch, int tid, int bar_id) {
+  v = warp_fold(v);
+  if ((tid & 31) == 0) scratch[tid >> 5] = v;
+  named_bar_sync(bar_id, kLanes);
+  double tot = 0.0;
+  if (tid == 0) {
+    tot = scratch[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) tot = dadd(tot, scratch[w]);
+  }
+  named_bar_sync(bar_id, kLanes);
+  return tot;
+}
+
+// Last-block-done completion for NRED reductions whose tile partials are in
+// red.partials[r * ntiles + t].  Called by the 256 lanes of each CTA after
+// all of its partials were written (by lane 0).  Returns true in lane 0 of
+// the last CTA, with the totals in tot[].
+template <int NRED>
+__device__ __forceinline__ bool grid_finish(const RedCtx& red, double (&tot)[NRED],
+                                            double* scratch, int* s_flag, int tid, int bar_id) {
+  if (tid == 0) {
+    __threadfence();
+    unsigned tk = atomicAdd(red.ticket, 1u);
+    *s_flag = (tk == gridDim.x - 1) ? 1 : 0;
+  }
+  named_bar_sync(bar_id, kLanes);
+  if (*s_flag == 0) return false;
+  __threadfence();
+#pragma unroll
+  for (int r = 0; r < NRED; ++r) {
+    double s = 0.0;
+    const double* p = red.partials + (long)r * red.ntiles;
+    for (long k = tid; k < red.ntiles; k += kLanes) s = dadd(s, __ldcg(p + k));
+    tot[r] = group_fold256(s, scratch, tid, bar_id);
+  }
+  if (tid == 0) *red.ticket = 0u;
+  return tid == 0;
+}
+
+}  // namespace celg

@@ -1,0 +1,142 @@
+// celg_internal.h -- host-side objects of libcelgpu.so (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/celgpu.h"
+
+namespace celg {
+
+// Device copy of a CSR matrix, 0-based.  row_ptr has n+1+4 entries and
+// cols/vals nnz+4 (tails filled with nnz / 0) so that the 16-byte rounded
+// bulk copies of the SpMV pipeline never leave the allocation.
+struct CsrDev {
+  int n = 0;
+  int nnz = 0;
+  int* rp = nullptr;
+  int* ci = nullptr;
+  double* v = nullptr;
+  float* v32 = nullptr;   // FP32 copy (refinement inner solve)
+  int cap = 0;            // staged entries per 256-row sub-tile
+};
+
+struct JadDev {
+  int mmax = -1;          // -1: not built
+  int* begin = nullptr;   // mmax+1
+  int* ci = nullptr;      // nnz
+  double* v = nullptr;    // nnz
+  int* perm = nullptr;    // n
+};
+
+struct PcgState;  // device scalar state of one solve (pcg_internal.cuh)
+
+struct GraphEntry {
+  std::string key;
+  cudaGraph_t graph;
+  cudaGraphExec_t exec;
+};
+
+}  // namespace celg
+
+struct celg_handle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sms = 148;
+  // reduction scratch: partials (2 rows of max tiles) and a completion ticket
+  double* partials = nullptr;
+  size_t partials_cap = 0;   // doubles
+  unsigned* ticket = nullptr;
+  int* err_d = nullptr;      // device error word (bounded waits)
+  double* scal_d = nullptr;  // small device scalars for blas1 results
+  double* scal_h = nullptr;  // pinned mirror
+  // PCG work vectors
+  double* wr = nullptr;
+  double* wp = nullptr;
+  double* wv = nullptr;
+  size_t wcap = 0;           // elements
+  celg::PcgState* state_d = nullptr;
+  celg::PcgState* state_h = nullptr;  // pinned
+  // cached solve graphs (keyed by matrix, vectors and parameters)
+  std::vector<celg::GraphEntry> graphs;
+  double* hist_d = nullptr;
+  int hist_cap = 0;
+  // host-buffer solve staging (stable pointers keep cached graphs valid)
+  double* sb = nullptr;
+  double* sx = nullptr;
+  size_t scap = 0;
+  // FP32 refinement work vectors
+  float* f32 = nullptr;   // 6 vectors of f32cap floats
+  size_t f32cap = 0;
+  double* ir_d = nullptr; // FP64 correction / residual
+  size_t ircap = 0;
+  // ELM assembly state
+  struct Elm* elm = nullptr;
+  // last solve timing
+  float last_ms = 0.f;
+  int last_iters = 0;
+  double last_bytes_per_iter = 0.0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct celg_mat {
+  celg_handle* h = nullptr;
+  celg::CsrDev csr;
+  celg::JadDev jad;
+  double* diag = nullptr;     // n
+  double* jacobi = nullptr;   // n
+  float* jacobi32 = nullptr;  // n
+  double* scale = nullptr;    // sqrt|d| when row-scaled, else null
+  bool scaled = false;
+};
+
+namespace celg {
+
+int cuda_status(cudaError_t e, const char* what);
+#define CELG_CUDA(call)                                       \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return ::celg::cuda_status(e_, #call); \
+  } while (0)
+
+int ensure_partials(celg_handle* h, long ntiles, int nred);
+void graph_cache_clear(celg_handle* h);
+void graph_cache_drop_matrix(celg_handle* h, const void* m);
+int ensure_work(celg_handle* h, size_t n);
+long ntiles_of(long n);
+int grid_for_tiles(celg_handle* h, long ntiles, int blocks_per_sm);
+
+// spmv.cu
+int launch_spmv_csr(celg_handle* h, const CsrDev& A, const double* x, double* y, int accumulate);
+int launch_spmv_csr_f32(celg_handle* h, const CsrDev& A, const float* x, float* y, int accumulate);
+int launch_spmv_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x, double* y);
+int csr_compute_cap(celg_handle* h, CsrDev& A);
+
+// blas1.cu
+int launch_dot(celg_handle* h, long n, const double* a, const double* b, double* out_d, int take_sqrt);
+int launch_axpy(celg_handle* h, long n, double alpha, const double* x, double* y);
+int launch_xpby(celg_handle* h, long n, const double* x, double beta, double* y);
+int launch_mul(celg_handle* h, long n, const double* a, const double* b, double* z);
+int launch_residual(celg_handle* h, celg_mat* m, int fmt, const double* b, const double* x,
+                    double* r, double* norm_out_d);
+int launch_jacobi_setup(celg_handle* h, celg_mat* m);
+int launch_row_scale(celg_handle* h, celg_mat* m);
+int launch_to_f32(celg_handle* h, long n, const double* a, float* b);
+int launch_scale_vec(celg_handle* h, long n, const double* a, const double* s, double* out, int divide);
+
+// pcg.cu / gmres.cu / ir.cu
+int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+              celg_result* res);
+int cg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+             celg_result* res);
+int gmres_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+                celg_result* res);
+int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+             celg_result* res);
+
+}  // namespace celg

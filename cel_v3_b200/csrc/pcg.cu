@@ -1,0 +1,297 @@
+// pcg.cu -- Jacobi-PCG (cel_cgalg_jacobi, src/fcgalg/cel_cgalg_module.f90:178-305)
+// as three fused sweeps per iteration, run to convergence inside one CUDA
+// graph whose WHILE conditional node is driven from the device.
+//
+// Per iteration (reference lines in brackets):
+//   K1  v = 0 + A p, pv = v.p, sigma = alpha/pv          [:251-261]
+//   K2  x += sigma p, r += (-sigma) v, z = J r (not stored),
+//       rz = r.z, rr = r.r, beta = rz/alpha, alpha = rz,
+//       ||r|| = sqrt(rr), convergence test               [:263-277, :287, :247-249]
+//   K3  p = beta p + J r                                  [:282]
+// Set-up: x0, ||b|| and eps (Kpre); r = b - A x, p = J r, alpha = r.p,
+// ||r|| (Kinit) [:207-236].  After the loop one more sweep recomputes
+// ||b - A x|| in FP64 (verification; not part of the reference).
+//
+// The same kernels serve the FP32-storage inner solve of the iterative
+// refinement (VT = float): matrix values and vectors are float, every
+// vector update is computed in double from the float operands and rounded
+// once, reductions and scalars are double.  For VT = double the arithmetic
+// is exactly the reference's.
+// Algorithmic bytes per FP64 CSR iteration: 12 nnz + 4 (n+1) + 104 n.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "pcg_internal.cuh"
+
+namespace celg {
+
+int ensure_work(celg_handle* h, size_t n) {
+  if (n <= h->wcap && h->wr) return CELG_OK;
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  graph_cache_clear(h);
+  cudaFree(h->wr);
+  cudaFree(h->wp);
+  cudaFree(h->wv);
+  h->wr = h->wp = h->wv = nullptr;
+  const size_t cap = std::max<size_t>(n, 1024);
+  CELG_CUDA(cudaMalloc(&h->wr, cap * sizeof(double)));
+  CELG_CUDA(cudaMalloc(&h->wp, cap * sizeof(double)));
+  CELG_CUDA(cudaMalloc(&h->wv, cap * sizeof(double)));
+  h->wcap = cap;
+  return CELG_OK;
+}
+
+int ensure_state(celg_handle* h, int hist_cap) {
+  if (!h->state_d) {
+    CELG_CUDA(cudaMalloc(&h->state_d, sizeof(PcgState)));
+    CELG_CUDA(cudaMallocHost(&h->state_h, sizeof(PcgState)));
+  }
+  if (hist_cap > h->hist_cap) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(h->hist_d);
+    h->hist_d = nullptr;
+    CELG_CUDA(cudaMalloc(&h->hist_d, sizeof(double) * (size_t)hist_cap));
+    h->hist_cap = hist_cap;
+  }
+  return CELG_OK;
+}
+
+void graph_cache_clear(celg_handle* h) {
+  for (auto& e : h->graphs) {
+    if (e.exec) cudaGraphExecDestroy(e.exec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+  }
+  h->graphs.clear();
+}
+
+void graph_cache_drop_matrix(celg_handle* h, const void* m) {
+  char tag[64];
+  std::snprintf(tag, sizeof(tag), "|%p|", m);
+  for (size_t i = 0; i < h->graphs.size();) {
+    if (h->graphs[i].key.find(tag) != std::string::npos) {
+      if (h->graphs[i].exec) cudaGraphExecDestroy(h->graphs[i].exec);
+      if (h->graphs[i].graph) cudaGraphDestroy(h->graphs[i].graph);
+      h->graphs.erase(h->graphs.begin() + (long)i);
+    } else {
+      ++i;
+    }
+  }
+}
+
+// Append a WHILE conditional node after the work captured so far on
+// h->stream and capture the loop body (recorded by `body`) into it.
+template <class Body>
+static int capture_while(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cap_graph;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  CELG_CUDA(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cap_graph, &deps, &ndeps));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  CELG_CUDA(cudaGraphAddNode(&cnode, cap_graph, deps, ndeps, &cp));
+  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+  CELG_CUDA(cudaStreamUpdateCaptureDependencies(h->stream, &cnode, 1,
+                                                cudaStreamSetCaptureDependencies));
+  cudaStream_t side;
+  CELG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCaptureToGraph(side, bodyg, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeRelaxed);
+  int st = CELG_OK;
+  if (e == cudaSuccess) {
+    cudaStream_t main_stream = h->stream;
+    h->stream = side;
+    st = body();
+    h->stream = main_stream;
+    cudaGraph_t out;
+    e = cudaStreamEndCapture(side, &out);
+  }
+  cudaStreamDestroy(side);
+  if (st) return st;
+  CELG_CUDA(e);
+  return CELG_OK;
+}
+
+template <typename VT>
+static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
+  const long n = B.A->n;
+  constexpr bool kF64 = std::is_same<VT, double>::value;
+  int st = launch_tile(h, n, OpPre<VT>{B.b, B.x, p->x0_mode, p->eps_abs, p->eps_rel, a});
+  if (st) return st;
+  if constexpr (kF64) {
+    if (B.jad) {
+      st = launch_jad(h, *B.A, *B.jad, B.x, EpiStore<double>{B.r, 0});
+      if (!st) st = launch_tile(h, n, OpInitNat<double>{B.b, B.r, B.p, B.J, a});
+    } else {
+      st = launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
+    }
+  } else {
+    st = launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
+  }
+  if (st) return st;
+  st = capture_while(h, a.cond, [&]() -> int {
+    int s2 = CELG_OK;
+    if constexpr (kF64) {
+      if (B.jad)
+        s2 = launch_jad(h, *B.A, *B.jad, B.p, EpiAp<double>{B.v, B.p, a});
+      else
+        s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+    } else {
+      s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+    }
+    if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.x, B.r, B.p, B.v, B.J, a, 0.0});
+    if (!s2) s2 = launch_tile(h, n, OpDirection<VT>{B.p, B.r, B.J, a, 0.0});
+    return s2;
+  });
+  if (st) return st;
+  if constexpr (kF64) {
+    if (!B.verify_vals) return CELG_OK;
+    // verification sweep in FP64
+    if (B.jad) {
+      st = launch_jad(h, *B.A, *B.jad, B.x, EpiStore<double>{B.v, 0});
+      if (!st) st = launch_tile(h, n, OpVerifyNat{B.b, B.v, a.st});
+    } else {
+      st = launch_csr<double>(h, *B.A, B.verify_vals, B.x, EpiVerify{B.b, a.st});
+    }
+  }
+  return st;
+}
+
+template <typename VT>
+static std::string pcg_key(const PcgBind<VT>& B, const celg_params* p, int hist_cap,
+                           const void* mat) {
+  char buf[640];
+  std::snprintf(buf, sizeof(buf), "pcg%d|%p|%d|%d|%p|%p|%p|%p|%p|%p|%d|%.17g|%.17g|%d|%d|%p|%p",
+                (int)sizeof(VT), mat, B.A->n, B.jad ? 1 : 0, (const void*)B.b, (const void*)B.x,
+                (const void*)B.r, (const void*)B.p, (const void*)B.v, (const void*)B.J,
+                p->x0_mode, p->eps_abs, p->eps_rel, p->iter_max, hist_cap,
+                (const void*)B.vals, (const void*)B.verify_vals);
+  return std::string(buf);
+}
+
+template <typename VT>
+int pcg_run(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, const void* mat,
+            PcgState* out_state) {
+  const long n = B.A->n;
+  if (p->iter_max < 0) return CELG_ERR_ARG;
+  int st = ensure_partials(h, ntiles_of(n), 2);
+  const int hist_cap = p->iter_max + 1;
+  if (!st) st = ensure_state(h, hist_cap);
+  if (st) return st;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+
+  const std::string key = pcg_key(B, p, hist_cap, mat);
+  GraphEntry* ge = nullptr;
+  for (auto& e : h->graphs)
+    if (e.key == key) ge = &e;
+  if (!ge) {
+    if (h->graphs.size() >= 8) {
+      cudaStreamSynchronize(h->stream);
+      graph_cache_clear(h);
+    }
+    CELG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cap_graph;
+    cudaError_t e = cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cap_graph, nullptr, nullptr);
+    cudaGraphConditionalHandle cond = 0;
+    if (e == cudaSuccess)
+      e = cudaGraphConditionalHandleCreate(&cond, cap_graph, 1, cudaGraphCondAssignDefault);
+    PcgArgs a{h->state_d, h->hist_d, hist_cap, p->iter_max, cond, h->err_d};
+    int rst = e == cudaSuccess ? record_pcg<VT>(h, B, p, a) : CELG_ERR_CUDA;
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return cuda_status(e, "conditional handle");
+    }
+    if (rst || e2 != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return rst ? rst : cuda_status(e2, "cudaStreamEndCapture");
+    }
+    cudaGraphExec_t gx;
+    cudaError_t e3 = cudaGraphInstantiate(&gx, g, 0);
+    if (e3 != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_status(e3, "cudaGraphInstantiate");
+    }
+    h->graphs.push_back(GraphEntry{key, g, gx});
+    ge = &h->graphs.back();
+  }
+  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(h->state_h, h->state_d, sizeof(PcgState), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(h->scal_h + 8, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  *out_state = *h->state_h;
+  int err_word = 0;
+  std::memcpy(&err_word, h->scal_h + 8, sizeof(int));
+  if (err_word) return err_word;
+  const PcgState& s = *out_state;
+  if (s.err) return s.err;
+  if (!(s.norm <= s.eps) && s.iter >= p->iter_max && std::fabs(s.alpha) > kRealSmall)
+    return CELG_ERR_NOCONV;
+  return CELG_OK;
+}
+
+template int pcg_run<double>(celg_handle*, const PcgBind<double>&, const celg_params*, const void*,
+                             PcgState*);
+template int pcg_run<float>(celg_handle*, const PcgBind<float>&, const celg_params*, const void*,
+                            PcgState*);
+
+int copy_history(celg_handle* h, int len, celg_result* res) {
+  res->history_len = 0;
+  if (res->history && res->history_cap > 0 && len > 0) {
+    const int l = std::min(len, res->history_cap);
+    CELG_CUDA(cudaMemcpy(res->history, h->hist_d, sizeof(double) * (size_t)l, cudaMemcpyDeviceToHost));
+    res->history_len = l;
+  }
+  return CELG_OK;
+}
+
+int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+              celg_result* res) {
+  const long n = m->csr.n;
+  if (!m->jacobi) return CELG_ERR_STATE;
+  const bool jad = p->fmt == CELG_FMT_JAD;
+  if (jad && m->jad.mmax < 0) return CELG_ERR_STATE;
+  int st = ensure_work(h, (size_t)n);
+  if (st) return st;
+  PcgBind<double> B;
+  B.A = &m->csr;
+  B.jad = jad ? &m->jad : nullptr;
+  B.vals = m->csr.v;
+  B.verify_vals = m->csr.v;
+  B.b = b;
+  B.x = x;
+  B.r = h->wr;
+  B.p = h->wp;
+  B.v = h->wv;
+  B.J = m->jacobi;
+  PcgState s;
+  std::memset(&s, 0, sizeof(s));
+  const int ret = pcg_run<double>(h, B, p, m, &s);
+  h->last_iters = s.iter;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 104.0 * n;
+  if (res) {
+    res->iter_done = s.iter;
+    res->final_norm2 = s.norm;
+    res->bnorm = s.bnorm;
+    res->verified_relres = s.vres;
+    res->err = ret;
+    res->arnoldi_steps = 0;
+    st = copy_history(h, std::min(s.hist_len, p->iter_max + 1), res);
+    if (st) return st;
+  }
+  return ret;
+}
+
+}  // namespace celg

@@ -1,0 +1,278 @@
+// pcg_internal.cuh -- device state, argument packs and the fused sweeps of
+// the Jacobi-PCG iteration (see pcg.cu), shared with the refinement and
+// batched solvers.
+#pragma once
+#include <type_traits>
+
+#include "tile_kernels.cuh"
+
+namespace celg {
+
+constexpr double kRealSmall = 1.1 * 2.220446049250313e-16;  // cel_real_small
+
+struct PcgState {
+  double alpha, sigma, beta, norm, bnorm, eps, pvd, rz, vres;
+  int iter, active, err, hist_len;
+};
+
+struct PcgArgs {
+  PcgState* st;
+  double* hist;
+  int hist_cap;
+  int iter_max;
+  cudaGraphConditionalHandle cond;
+  const int* errw;  // device error word of the handle (bounded-wait timeouts)
+};
+
+// Vectors and matrix one PCG solve runs on.
+template <typename VT>
+struct PcgBind {
+  const CsrDev* A = nullptr;
+  const JadDev* jad = nullptr;  // FP64 JAD path when set
+  const VT* vals = nullptr;     // CSR values used by the iteration
+  const double* verify_vals = nullptr;  // FP64 values for the final check (null: skip)
+  const VT* b = nullptr;
+  VT* x = nullptr;
+  VT* r = nullptr;
+  VT* p = nullptr;
+  VT* v = nullptr;
+  const VT* J = nullptr;
+};
+
+int ensure_state(celg_handle* h, int hist_cap);
+template <typename VT>
+int pcg_run(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, const void* mat,
+            PcgState* out_state);
+int copy_history(celg_handle* h, int len, celg_result* res);
+
+template <typename VT>
+__device__ __forceinline__ double D(VT v) { return (double)v; }
+template <typename VT>
+__device__ __forceinline__ VT R(double v) { return (VT)v; }
+
+__device__ __forceinline__ void set_cond(cudaGraphConditionalHandle c, int v) {
+  if (c) cudaGraphSetConditional(c, (unsigned)v);
+}
+
+__device__ __forceinline__ int pcg_go(const PcgState* st, int iter_max, const int* errw) {
+  return (st->err == 0 && *(volatile const int*)errw == 0 && st->iter < iter_max &&
+          fabs(st->alpha) > kRealSmall && st->norm > st->eps)
+             ? 1
+             : 0;
+}
+
+__device__ __forceinline__ void init_finish(const PcgArgs& a, double rp, double rr) {
+  PcgState* st = a.st;
+  st->alpha = rp;
+  st->norm = sqrt(rr);
+  st->iter = 0;
+  if (a.hist && a.hist_cap > 0) a.hist[0] = st->norm;
+  st->hist_len = 1;
+  st->active = pcg_go(st, a.iter_max, a.errw);
+  set_cond(a.cond, st->active);
+}
+
+// Kpre: x0 and ||b||, eps = max(eps_abs, eps_rel ||b||)
+template <typename VT>
+struct OpPre {
+  static constexpr int NRED = 1;
+  struct Regs { VT b; };
+  const VT* b;
+  VT* x;
+  int x0_mode;
+  double eps_abs, eps_rel;
+  PcgArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    if (x0_mode == CELG_X0_REF_ONES) x[i] = VT(1);
+    else if (x0_mode == CELG_X0_ZERO) x[i] = VT(0);
+    acc[0] = dadd(acc[0], dmul(D(g.b), D(g.b)));
+  }
+  __device__ void finish(double* tot) const {
+    PcgState* st = a.st;
+    st->bnorm = sqrt(tot[0]);
+    double e = eps_abs;
+    if (eps_rel > 0.0 && eps_rel * st->bnorm > e) e = eps_rel * st->bnorm;
+    st->eps = e;
+    st->err = 0;
+    st->iter = 0;
+    st->active = 1;
+    st->alpha = st->sigma = st->beta = st->pvd = st->rz = 0.0;
+    st->vres = 0.0;
+  }
+};
+
+// Kinit on CSR: r = b - (0 + A x); p = J r; alpha = r.p; rr = r.r
+template <typename VT>
+struct EpiInit {
+  static constexpr int NRED = 2;
+  const VT* b;
+  VT* r;
+  VT* p;
+  const VT* J;
+  PcgArgs a;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, VT s, double* acc) const {
+    const VT ri = R<VT>(__dsub_rn(D(b[i]), D(vadd(VT(0), s))));
+    r[i] = ri;
+    const double z = dmul(D(ri), D(J[i]));
+    p[i] = R<VT>(z);
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
+  }
+  __device__ void finish(double* tot) const { init_finish(a, tot[0], tot[1]); }
+};
+
+// Kinit tail on JAD (after r = A x by the JAD kernel), natural row order
+template <typename VT>
+struct OpInitNat {
+  static constexpr int NRED = 2;
+  struct Regs { VT b, r, J; };
+  const VT* b;
+  VT* r;
+  VT* p;
+  const VT* J;
+  PcgArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); g.r = r[i]; g.J = __ldg(J + i); }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    const VT ri = R<VT>(__dsub_rn(D(g.b), D(vadd(VT(0), g.r))));
+    r[i] = ri;
+    const double z = dmul(D(ri), D(g.J));
+    p[i] = R<VT>(z);
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
+  }
+  __device__ void finish(double* tot) const { init_finish(a, tot[0], tot[1]); }
+};
+
+// K1: v = 0 + A p; pv = v.p; sigma = alpha / pv
+template <typename VT>
+struct EpiAp {
+  static constexpr int NRED = 1;
+  VT* v;
+  const VT* p;
+  PcgArgs a;
+  __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
+  __device__ void row(long i, VT s, double* acc) const {
+    const VT vi = vadd(VT(0), s);
+    v[i] = vi;
+    acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
+  }
+  __device__ void finish(double* tot) const {
+    PcgState* st = a.st;
+    st->pvd = tot[0];
+    const double sg = st->alpha / tot[0];
+    st->sigma = sg;
+    if (!isfinite(sg)) {
+      st->err = kErrBreakdown;
+      st->active = 0;
+    }
+  }
+};
+
+// K2: x += sigma p; r += (-sigma) v; z = J r; rz, rr; scalars and stopping test
+template <typename VT>
+struct OpUpdate {
+  static constexpr int NRED = 2;
+  struct Regs { VT x, r, p, v, J; };
+  VT* x;
+  VT* r;
+  const VT* p;
+  const VT* v;
+  const VT* J;
+  PcgArgs a;
+  double sg;
+  __device__ bool prepare() {
+    if (*(volatile int*)&a.st->active == 0) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(a.cond, 0);
+      return false;
+    }
+    sg = a.st->sigma;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const {
+    g.x = x[i];
+    g.r = r[i];
+    g.p = __ldg(p + i);
+    g.v = __ldg(v + i);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    x[i] = R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
+    const VT ri = R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
+    r[i] = ri;
+    const double z = dmul(D(ri), D(g.J));
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
+  }
+  __device__ void finish(double* tot) const {
+    PcgState* st = a.st;
+    st->rz = tot[0];
+    st->beta = tot[0] / st->alpha;
+    st->alpha = tot[0];
+    st->norm = sqrt(tot[1]);
+    st->iter += 1;
+    if (a.hist && st->iter < a.hist_cap) a.hist[st->iter] = st->norm;
+    st->hist_len = st->iter + 1;
+    st->active = pcg_go(st, a.iter_max, a.errw);
+    set_cond(a.cond, st->active);
+  }
+};
+
+// K3: p = beta p + J r
+template <typename VT>
+struct OpDirection {
+  static constexpr int NRED = 0;
+  struct Regs { VT p, r, J; };
+  VT* p;
+  const VT* r;
+  const VT* J;
+  PcgArgs a;
+  double bt;
+  __device__ bool prepare() {
+    if (*(volatile int*)&a.st->active == 0) return false;
+    bt = a.st->beta;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  __device__ void compute(long i, Regs& g, double*) const {
+    p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish(double*) const {}
+};
+
+// verification: ||b - A x|| / ||b|| (residual not stored)
+struct EpiVerify {
+  static constexpr int NRED = 1;
+  const double* b;
+  PcgState* st;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const {
+    st->vres = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : sqrt(tot[0]);
+  }
+};
+
+struct OpVerifyNat {
+  static constexpr int NRED = 1;
+  struct Regs { double b, r; };
+  const double* b;
+  const double* r;
+  PcgState* st;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); g.r = __ldg(r + i); }
+  __device__ void compute(long, Regs& g, double* acc) const {
+    const double ri = __dsub_rn(g.b, dadd(0.0, g.r));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const {
+    st->vres = st->bnorm > 0.0 ? sqrt(tot[0]) / st->bnorm : sqrt(tot[0]);
+  }
+};
+
+}  // namespace celg

@@ -1,0 +1,266 @@
+// spmv_kernels.cuh -- the SpMV kernels of libcelgpu, templated on an
+// epilogue so that each solver step fuses its vector update and dot
+// products into the matrix sweep.
+//
+// CSR (reference: src/fop/cel_fop_mv_module.f90:189-247).  Persistent CTAs
+// walk 1024-row reduction tiles (tile b, b+grid, ...), each as four 256-row
+// sub-tiles.  A producer warp stages every sub-tile's row pointers, column
+// indices and values into shared memory with bulk copies
+// (cp.async.bulk + mbarrier, kStages deep); eight consumer warps compute one
+// row per thread from shared memory, gathering x through the read-only
+// path.  Row sums start at 0.0 and add value*x in stored order with separate
+// multiply and add roundings, exactly like the Fortran loop at :216-228.
+// A sub-tile whose entries exceed the staging capacity (very long rows) is
+// read straight from global memory with the same arithmetic.
+//
+// JAD (reference: src/fop/cel_fop_mv_module.f90:250-352).  One thread per
+// permuted row, four rows per thread per 1024-row tile, jagged diagonals
+// read column-major (coalesced) and accumulated in a register in diagonal
+// order; the result is written through perm (y(perm(i)) = tmp(i), :325).
+#pragma once
+#include "celg_device.cuh"
+
+namespace celg {
+
+// Shared-memory layout of one pipeline stage for `cap` staged entries.
+struct StageLayout {
+  int ci_off, v_off, bytes;
+  __host__ __device__ StageLayout(int cap, int vt_size) {
+    ci_off = (kSub + 4) * 4;                                   // 1040, 16B multiple
+    v_off = ci_off + (cap + 8) * 4;                            // cap % 4 == 0
+    int end = v_off + (cap + 8) * vt_size;
+    bytes = (end + 127) & ~127;
+  }
+};
+constexpr int kCsrHeader = 256;  // mbarriers, stage meta, fold scratch
+
+template <int N>
+struct Acc {
+  double a[N > 0 ? N : 1];
+};
+
+template <typename VT, class Epi>
+__global__ void __launch_bounds__(kCsrThreads, 2)
+    csr_tma_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+                   const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
+                   RedCtx red, int* err) {
+  constexpr int NR = Epi::NRED;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* empty = full + kStages;
+  int* meta = reinterpret_cast<int*>(empty + kStages);        // a0, fallback per stage
+  double* scratch = reinterpret_cast<double*>(smem + 128);    // 8 doubles
+  int* s_flag = reinterpret_cast<int*>(smem + 192);
+  unsigned char* stages = smem + kCsrHeader;
+  const StageLayout L(cap, (int)sizeof(VT));
+
+  if (!epi.active()) return;
+  const long nsub = ((long)n + kSub - 1) / kSub;
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kConsumerWarps);
+    }
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == kConsumerWarps) {
+    // ---------------- producer warp ----------------
+    long t = blockIdx.x;
+    int it = 0;
+    int bnd = 0;  // lane q (0..4) holds rp at sub-tile boundary q of tile t
+    if (t < ntiles && lane <= kSubPerTile)
+      bnd = __ldg(rp + min(t * kTile + (long)lane * kSub, (long)n));
+    for (; t < ntiles; t += gridDim.x) {
+      const int cur = bnd;
+      const long tn = t + gridDim.x;
+      if (tn < ntiles && lane <= kSubPerTile)
+        bnd = __ldg(rp + min(tn * kTile + (long)lane * kSub, (long)n));
+      for (int q = 0; q < kSubPerTile; ++q) {
+        const long s = t * kSubPerTile + q;
+        if (s >= nsub) break;
+        const int e0 = __shfl_sync(0xffffffffu, cur, q);
+        const int e1 = __shfl_sync(0xffffffffu, cur, q + 1);
+        int abort_ = 0;
+        if (lane == 0) {
+          const int st = it % kStages;
+          if (it >= kStages &&
+              !mbar_wait_bounded(&empty[st], (uint32_t)(((it / kStages) - 1) & 1), err)) {
+            abort_ = 1;
+          } else {
+            const long row0 = s * kSub;
+            const int rows = (int)min((long)kSub, (long)n - row0);
+            const int a0 = e0 & ~3;
+            const int a1 = (e1 + 3) & ~3;
+            const int cnt = a1 - a0;
+            const int fb = cnt > cap ? 1 : 0;
+            meta[2 * st] = a0;
+            meta[2 * st + 1] = fb;
+            const uint32_t rpb = (uint32_t)(((rows + 1 + 3) & ~3) * 4);
+            const uint32_t mb = fb ? 0u : (uint32_t)cnt * (uint32_t)(4 + sizeof(VT));
+            unsigned char* sb = stages + (size_t)st * L.bytes;
+            mbar_arrive_expect_tx(&full[st], rpb + mb);
+            bulk_g2s(sb, rp + row0, rpb, &full[st]);
+            if (!fb && cnt > 0) {
+              bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * 4u, &full[st]);
+              bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
+            }
+          }
+        }
+        abort_ = __shfl_sync(0xffffffffu, abort_, 0);
+        if (abort_) return;
+        ++it;
+      }
+    }
+    return;
+  }
+
+  // ---------------- consumer warps (256 threads, lane j = row in sub-tile) ----
+  const int j = threadIdx.x;
+  int it = 0;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    Acc<NR> acc;
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
+    for (int q = 0; q < kSubPerTile; ++q) {
+      const long s = t * kSubPerTile + q;
+      if (s >= nsub) break;
+      const int st = it % kStages;
+      if (!mbar_wait_bounded(&full[st], (uint32_t)((it / kStages) & 1), err)) return;
+      const unsigned char* sb = stages + (size_t)st * L.bytes;
+      const int* rps = reinterpret_cast<const int*>(sb);
+      const int* cis = reinterpret_cast<const int*>(sb + L.ci_off);
+      const VT* vs = reinterpret_cast<const VT*>(sb + L.v_off);
+      const int a0 = meta[2 * st];
+      const int fb = meta[2 * st + 1];
+      const long row = s * kSub + j;
+      if (row < n) {
+        const int b = rps[j], e = rps[j + 1];
+        VT sum = VT(0);
+        if (!fb) {
+          int k = b - a0;
+          const int ke = e - a0;
+          for (; k + 4 <= ke; k += 4) {
+            const int c0 = cis[k], c1 = cis[k + 1], c2 = cis[k + 2], c3 = cis[k + 3];
+            const VT v0 = vs[k], v1 = vs[k + 1], v2 = vs[k + 2], v3 = vs[k + 3];
+            const VT x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2),
+                     x3 = __ldg(x + c3);
+            sum = vadd(sum, vmul(v0, x0));
+            sum = vadd(sum, vmul(v1, x1));
+            sum = vadd(sum, vmul(v2, x2));
+            sum = vadd(sum, vmul(v3, x3));
+          }
+          for (; k < ke; ++k) sum = vadd(sum, vmul(vs[k], __ldg(x + cis[k])));
+        } else {
+          for (int k = b; k < e; ++k) sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + __ldg(ci + k))));
+        }
+        epi.row(row, sum, acc.a);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[st]);
+      ++it;
+    }
+    if (NR > 0) {
+#pragma unroll
+      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
+        const double tot = group_fold256(acc.a[r], scratch, j, 1);
+        if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
+      }
+    }
+  }
+  if (NR > 0) {
+    double tot[NR > 0 ? NR : 1];
+    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) epi.finish(tot);
+  }
+}
+
+template <class Epi>
+__global__ void __launch_bounds__(kLanes)
+    jad_kernel(const int* __restrict__ jb, const int* __restrict__ jci,
+               const double* __restrict__ jv, const int* __restrict__ perm, int n, int mmax,
+               const double* __restrict__ x, Epi epi, RedCtx red) {
+  constexpr int NR = Epi::NRED;
+  __shared__ double scratch[8];
+  __shared__ int s_flag;
+  if (!epi.active()) return;
+  const int j = threadIdx.x;
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    Acc<NR> acc;
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
+    long i[4];
+    double sum[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      i[k] = t * kTile + (long)k * kLanes + j;
+      sum[k] = 0.0;
+    }
+    for (int d = 0; d < mmax; ++d) {
+      const int beg = __ldg(jb + d);
+      const int len = __ldg(jb + d + 1) - beg;
+      if (i[0] >= len) break;  // permuted rows are sorted by decreasing length
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (i[k] < len) {
+          const long q = beg + i[k];
+          sum[k] = dadd(sum[k], dmul(__ldg(jv + q), __ldg(x + __ldg(jci + q))));
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (i[k] < n) epi.row((long)__ldg(perm + i[k]), sum[k], acc.a);
+    if (NR > 0) {
+#pragma unroll
+      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
+        const double tot = group_fold256(acc.a[r], scratch, j, 1);
+        if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
+      }
+    }
+  }
+  if (NR > 0) {
+    double tot[NR > 0 ? NR : 1];
+    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, &s_flag, j, 1)) epi.finish(tot);
+  }
+}
+
+// ---- plain epilogues -------------------------------------------------------
+
+// y = (accumulate ? y : 0) + row sum
+template <typename VT>
+struct EpiStore {
+  static constexpr int NRED = 0;
+  VT* y;
+  int accumulate;
+  __device__ bool active() const { return true; }
+  __device__ void row(long r, VT s, double*) const {
+    y[r] = vadd(accumulate ? y[r] : VT(0), s);
+  }
+  __device__ void finish(double*) const {}
+};
+
+// r = b - (0 + A x), and ||r||^2 into *out (sqrt taken in finish)
+struct EpiResidual {
+  static constexpr int NRED = 1;
+  const double* b;
+  double* r;
+  double* out;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = dsub_exact(b[i], s);
+    r[i] = ri;
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ static double dsub_exact(double a, double s) { return __dsub_rn(a, dadd(0.0, s)); }
+  __device__ void finish(double* tot) const { *out = sqrt(tot[0]); }
+};
+
+// Host helpers (spmv.cu)
+int csr_smem_bytes(int cap, int vt_size);
+
+}  // namespace celg

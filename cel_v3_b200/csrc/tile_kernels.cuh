@@ -1,0 +1,145 @@
+// tile_kernels.cuh -- streaming vector kernels over 1024-row tiles with the
+// fixed-order reductions of celg_device.cuh, plus the host launch helpers
+// for them and for the SpMV kernel templates.
+//
+// An Op supplies
+//   NRED                                  number of fused reductions
+//   bool prepare()                        read device scalars; false = skip
+//   void load(long i, Regs& r)            all global loads of row i
+//   void compute(long i, Regs& r, acc)    arithmetic, stores, reductions
+//   void finish(double* tot)              lane 0 of the last CTA
+// Each lane handles rows t*1024 + j + 256k (k = 0..3): loads of the four rows
+// are issued before any arithmetic so that 4 x (loads per row) requests are
+// in flight per thread, and the reduction order is the oracle's.
+#pragma once
+#include <algorithm>
+
+#include "celg_internal.h"
+#include "spmv_kernels.cuh"
+
+namespace celg {
+
+template <class Op>
+__global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx red) {
+  constexpr int NR = Op::NRED;
+  __shared__ double scratch[8];
+  __shared__ int s_flag;
+  Op op = op_in;
+  if (!op.prepare()) return;
+  const int j = threadIdx.x;
+  const long ntiles = (n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    Acc<NR> acc;
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
+    typename Op::Regs regs[4];
+    const long base = t * kTile + j;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (base + (long)k * kLanes < n) op.load(base + (long)k * kLanes, regs[k]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (base + (long)k * kLanes < n) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+    if (NR > 0) {
+#pragma unroll
+      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
+        const double tot = group_fold256(acc.a[r], scratch, j, 1);
+        if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
+      }
+    }
+  }
+  if (NR > 0) {
+    double tot[NR > 0 ? NR : 1];
+    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, &s_flag, j, 1)) op.finish(tot);
+  }
+}
+
+template <class Op>
+int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
+  const long nt = ntiles_of(n);
+  RedCtx red{h->partials, h->ticket, nt};
+  if (Op::NRED > 0) {
+    int st = ensure_partials(h, nt, Op::NRED);
+    if (st) return st;
+    red.partials = h->partials;
+  }
+  const int grid = grid_for_tiles(h, nt, blocks_per_sm);
+  tile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, op, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+template <typename VT, class Epi>
+int launch_csr(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{nullptr, h->ticket, nt};
+  if (Epi::NRED > 0) {
+    int st = ensure_partials(h, nt, Epi::NRED);
+    if (st) return st;
+    red.partials = h->partials;
+  }
+  if (A.n == 0) return CELG_OK;
+  const int smem = csr_smem_bytes(A.cap, (int)sizeof(VT));
+  auto kern = csr_tma_kernel<VT, Epi>;
+  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
+  per_sm = std::max(1, per_sm);
+  const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * per_sm));
+  kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, A.ci, vals, A.n, A.cap, x, epi, red,
+                                               h->err_d);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+template <class Epi>
+int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{nullptr, h->ticket, nt};
+  if (Epi::NRED > 0) {
+    int st = ensure_partials(h, nt, Epi::NRED);
+    if (st) return st;
+    red.partials = h->partials;
+  }
+  if (A.n == 0) return CELG_OK;
+  const int grid = grid_for_tiles(h, nt, 8);
+  jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
+                                                    red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+// ---- simple ops ----------------------------------------------------------
+
+// acc += a*b ; finish: *out = tot (or sqrt(tot))
+struct OpDot {
+  static constexpr int NRED = 1;
+  struct Regs { double a, b; };
+  const double* a;
+  const double* b;
+  double* out;
+  int take_sqrt;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& r) const { r.a = __ldg(a + i); r.b = __ldg(b + i); }
+  __device__ void compute(long, Regs& r, double* acc) const { acc[0] = dadd(acc[0], dmul(r.a, r.b)); }
+  __device__ void finish(double* tot) const { *out = take_sqrt ? sqrt(tot[0]) : tot[0]; }
+};
+
+// r = b - (0 + r) in place, acc += r*r; finish *out = sqrt(tot)
+struct OpResidNat {
+  static constexpr int NRED = 1;
+  struct Regs { double b, r; };
+  const double* b;
+  double* r;
+  double* out;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); g.r = r[i]; }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    const double ri = __dsub_rn(g.b, dadd(0.0, g.r));
+    r[i] = ri;
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const { *out = sqrt(tot[0]); }
+};
+
+}  // namespace celg

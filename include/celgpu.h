@@ -1,0 +1,192 @@
+/*
+ * celgpu.h -- C ABI of libcelgpu.so, the B200 (sm_100a) implementation of the
+ * CEL solver hot path: CSR/JAD SpMV, point-Jacobi, the fused PCG / CG /
+ * GMRES(m) iteration bodies, FP32-storage iterative refinement, batched
+ * and multi-right-hand-side PCG, and the adjoint gradient of a PCG solve.
+ *
+ * Every entry point returns an int status (CELG_OK == 0) and never aborts.
+ * Index arrays are int32 as in the reference (ik=4,
+ * src/fbase/cel_types_module.f90:14); values are binary64 (rk=8, :13).
+ * Pointers named *_d are device pointers on the handle's device; all other
+ * pointers are host pointers owned by the caller.  A handle owns one CUDA
+ * stream (or borrows the caller's) and its work buffers; a handle is not
+ * thread-safe, distinct handles may be used from distinct threads.
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * file:line within hpcdkhab/cel_v3.
+ */
+#ifndef CELGPU_H
+#define CELGPU_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference's integer err_code convention,
+ *      src/fbase/cel_error_module.f90:17-32, without its STOP) ------------- */
+#define CELG_OK 0
+#define CELG_ERR_ARG 1        /* bad argument or malformed matrix          */
+#define CELG_ERR_CUDA 2       /* a CUDA runtime call failed                */
+#define CELG_ERR_BREAKDOWN 3  /* alpha/beta/sigma not finite (p.Ap == 0)   */
+#define CELG_ERR_NOCONV 4     /* iteration limit reached before tolerance  */
+#define CELG_ERR_TIMEOUT 5    /* a device-side bounded wait gave up        */
+#define CELG_ERR_STATE 6      /* call out of order (e.g. DoIt before MatrixCompleted) */
+
+/* ---- formats and modes (mv_algorithm, src/fbase/cel_types_module.f90:58-81) */
+#define CELG_FMT_CSR 0
+#define CELG_FMT_JAD 1
+
+#define CELG_X0_REF_ONES 0 /* x0 = 1 as in src/fcgalg/cel_cgalg_module.f90:209 */
+#define CELG_X0_ZERO 1
+#define CELG_X0_USER 2     /* x_d holds the start vector on entry */
+
+#define CELG_PREC_FP64 0
+#define CELG_PREC_FP32_IR 1 /* FP32 matrix/Krylov vectors inside FP64 refinement */
+
+#define CELG_SOLVER_PCG 0   /* cel_cgalg_jacobi   (BENCHMARK_CG + Jacobi)     */
+#define CELG_SOLVER_CG 1    /* cel_cgalg          (BENCHMARK_CG, no precond.) */
+#define CELG_SOLVER_GMRES 2 /* cel_gmresalg_2jacobi (BENCHMARK_GMRES + Jacobi) */
+
+typedef struct celg_handle celg_handle;
+typedef struct celg_mat celg_mat;
+
+/* Solver parameters: cel_cgalg_parameter_type / cel_gmresalg_parameter_type
+ * (src/fcgalg/cel_alg_module.f90:26-54) plus the selections the reference
+ * keeps in input_parameters (src/fbase/cel_input_parameters_module.f90:128-170). */
+typedef struct {
+  int x0_mode;          /* CELG_X0_*                                             */
+  double eps_abs;       /* stop when ||r||_2 <= eps (reference: absolute, :247-249) */
+  double eps_rel;       /* if > 0, eps = max(eps_abs, eps_rel * ||b||_2)          */
+  int iter_max;         /* PCG/CG iterations; GMRES outer iterations            */
+  int fmt;              /* CELG_FMT_CSR or CELG_FMT_JAD                          */
+  int precision;        /* CELG_PREC_*                                           */
+  int literal_ref_bugs; /* CG: alpha-as-beta (:151); GMRES: unrotated Givens (:722-727) */
+  int restart;          /* GMRES(m): m (gmres_max_restart)                      */
+  double inner_eps_rel; /* FP32-IR: inner PCG relative tolerance (default 1e-4) */
+  int inner_iter_max;   /* FP32-IR: inner iteration cap                         */
+  int outer_max;        /* FP32-IR: refinement steps cap                        */
+} celg_params;
+
+/* Solve report.  history (caller-owned host buffer of history_cap doubles,
+ * nullable) receives ||r||_2 per iteration (PCG/CG), |gamma_{j+1}| per
+ * Arnoldi step (GMRES) or the outer residual per refinement (FP32-IR). */
+typedef struct {
+  int iter_done;          /* niter of cel_elmSolverDoIt                   */
+  double final_norm2;     /* ftol: last recurrence ||r||_2                */
+  double bnorm;           /* ||b||_2                                      */
+  double verified_relres; /* ||b - A x||_2 / ||b||_2 recomputed in FP64   */
+  int err;                /* same as the return value                     */
+  int arnoldi_steps;      /* GMRES inner steps; FP32-IR inner iterations  */
+  double* history;
+  int history_cap;
+  int history_len;        /* entries written                              */
+} celg_result;
+
+void celg_params_default(celg_params* p);
+
+/* ---- handle ---------------------------------------------------------------- */
+int celg_create(celg_handle** h, int device, void* stream /* cudaStream_t or NULL */);
+int celg_destroy(celg_handle* h);
+int celg_set_stream(celg_handle* h, void* stream);
+const char* celg_status_string(int status);
+int celg_sm_count(celg_handle* h, int* sms);
+
+/* ---- matrix ---------------------------------------------------------------- */
+/* CSR upload.  Replaces cel_sp_mat_to_csr (src/fspmt/cel_sp_mat_module.f90:430-456)
+ * and the single-subdomain case of cel_sp_mat_distr_from_sp_mat_local
+ * (src/fspmtdistr/cel_sp_mat_distr_module.f90:34-301).  index_base 0 or 1
+ * (the reference is 1-based, xadj(1)=1).  Rows must be given in order;
+ * columns may be in any order inside a row and are summed in the given order.
+ * Host arrays are copied; the caller keeps ownership. */
+int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr, const int* cols,
+                      const double* vals, int index_base, celg_mat** out);
+/* same with device arrays (0-based), copied device to device */
+int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_d,
+                             const int* cols_d, const double* vals_d, celg_mat** out);
+int celg_mat_destroy(celg_mat* m);
+int celg_mat_info(const celg_mat* m, int* n, int* nnz, int* jad_mmax);
+/* CSR -> JAD, cel_sp_mat_jad_from_sp_mat_local
+ * (src/fspmtconverter/cel_sp_mat_jad_converter_module.f90:93-175): the reference's
+ * permutation (stable sort by descending row length) and Saad's jagged
+ * diagonals.  perm_out (host, n entries, nullable) receives the 0-based
+ * permutation. */
+int celg_mat_to_jad(celg_mat* m, int* perm_out);
+/* JAD arrays back to the host (for checking): perm n, begin mmax+1, cols/vals nnz */
+int celg_mat_get_jad(const celg_mat* m, int* perm, int* begin, int* cols, double* vals);
+/* Point-Jacobi set-up, cel_sp_mat_distr_set_jacobi
+ * (src/fspmtdistr/cel_sp_mat_distr_format_module.f90:149-203) with the diagonal
+ * of src/fspmtdistr/cel_sp_mat_distr_module.f90:197-207 (last stored diagonal
+ * entry wins; missing diagonal -> 1/0 = inf, as in the reference). */
+int celg_mat_jacobi(celg_mat* m);
+int celg_mat_get_jacobi(const celg_mat* m, double* jacobi_host);
+/* Diagonal row scaling, cel_sp_mat_distr_scale
+ * (src/fspmtdistr/cel_sp_mat_distr_format_module.f90:91-145): A_ij /= sqrt|d_i|,
+ * jacobi = sqrt|d|/d; right-hand sides are scaled inside the solvers. */
+int celg_mat_scale_diagonal(celg_mat* m);
+/* FP32 copy of the matrix values for the refinement inner solve */
+int celg_mat_make_fp32(celg_mat* m);
+
+/* ---- operators (device pointers, on the handle's stream) -------------------- */
+/* y = (accumulate ? y : 0) + A x.  cel_fop_mv_axy_distr
+ * (src/fop/cel_fop_mv_module.f90:28-87) -> worker_local_csr (:189-247) or
+ * worker_local_jad (:250-352).  Each row is summed left to right from 0.0 in
+ * stored order, multiply and add rounded separately. */
+int celg_spmv(celg_handle* h, const celg_mat* m, int fmt, const double* x_d, double* y_d,
+              int accumulate);
+int celg_spmv_f32(celg_handle* h, const celg_mat* m, const float* x_d, float* y_d, int accumulate);
+/* cel_fop_vec_distr_dot_allreduce (src/fop/cel_fop_vec_distr_module.f90:724-775) */
+int celg_dot(celg_handle* h, int n, const double* a_d, const double* b_d, double* out);
+/* cel_fop_vec_distr_norm2_allreduce (:433-483), returns the square root */
+int celg_norm2(celg_handle* h, int n, const double* a_d, double* out);
+/* y = y + alpha x: cel_fop_vec_distr_scale (:836-874) */
+int celg_axpy(celg_handle* h, int n, double alpha, const double* x_d, double* y_d);
+/* y = beta y + x: cel_fop_vec_distr_scale_1 (:918-956) */
+int celg_xpby(celg_handle* h, int n, const double* x_d, double beta, double* y_d);
+/* z = r * jacobi: cel_fop_vec_mult_distr_jacobi (:338-375) */
+int celg_jacobi_apply(celg_handle* h, const celg_mat* m, const double* r_d, double* z_d);
+
+/* ---- solvers (b_d, x_d device vectors of length n) ---------------------------- */
+/* Jacobi-PCG, cel_cgalg_jacobi (src/fcgalg/cel_cgalg_module.f90:178-305).
+ * precision CELG_PREC_FP32_IR runs FP32-storage PCG sweeps inside FP64
+ * iterative refinement; the outer residual, update and test stay FP64. */
+int celg_pcg_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
+                    const celg_params* p, celg_result* res);
+/* Unpreconditioned CG, cel_cgalg (src/fcgalg/cel_cgalg_module.f90:34-175). */
+int celg_cg(celg_handle* h, celg_mat* m, const double* b_d, double* x_d, const celg_params* p,
+            celg_result* res);
+/* Restarted GMRES(m) with right Jacobi, cel_gmresalg_2jacobi
+ * (src/fcgalg/cel_gmresalg_module.f90:570-851), Givens update corrected unless
+ * literal_ref_bugs. */
+int celg_gmres_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
+                      const celg_params* p, celg_result* res);
+/* Host-buffer convenience: copies b in and x out on the handle's stream. */
+int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_host,
+                    double* x_host, const celg_params* p, celg_result* res);
+
+/* ---- ELM assembly API (src/felmsolver/cel_elmsolver_module.f90) -------------- */
+/* cel_elmSolverInitialization (:103-153): n_total rows, n_local local rows
+ * starting at 1-based row row_low, nnz_hint[2] nonzeros per row (diagonal and
+ * off-diagonal block).  Defaults as the reference: GMRES(3) + Jacobi +
+ * diagonal scaling, eps 1e-8, iter_max 5000 (:134-151). */
+int celg_elm_init(celg_handle* h, int n_total, int n_local, int row_low, const int nnz_hint[2]);
+int celg_elm_set_solver(celg_handle* h, int solver, const celg_params* p, int diag_scaling);
+int celg_elm_row_start(celg_handle* h, int row);                     /* :155-159 */
+int celg_elm_insert(celg_handle* h, int col, double value);          /* :161-172 */
+int celg_elm_reinsert(celg_handle* h, int col, double value);        /* :174-187 */
+int celg_elm_row_completed(celg_handle* h);                          /* :189-191 */
+/* bulk form of row_start/insert for whole rows, 1-based like the above */
+int celg_elm_insert_rows(celg_handle* h, int first_row, int nrows, const int* row_ptr,
+                         const int* cols, const double* vals);
+int celg_elm_matrix_completed(celg_handle* h);                       /* :193-439 */
+/* cel_elmSolverDoIt (:441-651): b on the host; iierr/niter/ftol as the reference */
+int celg_elm_doit(celg_handle* h, const double* b, int* iierr, int* niter, double* ftol);
+int celg_elm_redoit(celg_handle* h, const double* b, int* iierr, int* niter, double* ftol);
+/* cel_elmSolverCollectSolution (:790-815): x into a caller-owned buffer of n_local */
+int celg_elm_collect_solution(celg_handle* h, double* x);
+/* cel_elmSolverPerformance (:879-900): last solve's device time and counters */
+int celg_elm_performance(celg_handle* h, double* solve_ms, int* iters, double* bytes_per_iter);
+int celg_elm_destroy(celg_handle* h);                                /* :817-877 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif
