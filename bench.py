@@ -1,0 +1,397 @@
+"""Benchmark: Jacobi-PCG solves/s on the 256^3 7-point Poisson system.
+
+Workload (plain FP64 path): interior 256^3 Poisson (16,777,216 rows,
+117,047,296 non-zeros), CSR FP64, b = A x_true with x_true ~ U[0,1) from
+numpy default_rng(1), x0 = 0, stop at ||r|| <= 1e-8 ||b||, every solve
+verified by an FP64 recomputation of ||b - A x|| / ||b||.  Data are seeded
+synthetic (no dataset is used).  A step is one complete solve; the matrix
+and b stay resident in HBM (1.9 GB, far above the 126 MB L2, so no L2 flush
+is needed between steps).
+
+Also reported on the same line:
+  roofline      the dominant kernel (the CSR SpMV), timed alone with CUDA
+                events, algorithmic bytes 12 nnz + 4 (n+1) + 16 n per launch
+  e2e           the same solves through the reference-facing ELM interface
+                (celg_elm_doit + celg_elm_collect_solution: b copied from
+                pinned host memory, x copied back) inside the timed region
+  forms         FP32-storage refinement to rel-res 1e-10 and plain FP64 PCG
+                to 1e-10 on the same system (solves/s of each)
+  cpu_baseline  the C restatement of the reference's MPI+OpenMP PCG (oracle/)
+                on the host cores, on a bounded sample of iterations
+
+--impl reference times that CPU restatement alone (the Fortran reference
+cannot be built here: no Fortran compiler or MPI), each step a bounded sample
+of iterations of the same solve, scaled to solves/s.
+
+Multi-GPU (torchrun, N > 1): every rank solves its own copy of the system
+(independent replicas, no collective on the data path); value = all ranks'
+solves / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIDE = 256
+SEED = 1
+EPS_REL = 1e-8
+METRIC = "PCG solves/s at 256^3 to rel-res 1e-8 (Jacobi-PCG, CSR FP64)"
+UNIT = "solves/s"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_tag):
+    """dram bytes per launch of the kernel from the committed ncu summary."""
+    for f in sorted(os.listdir(os.path.join(ROOT, "profiles"))) if os.path.isdir(
+            os.path.join(ROOT, "profiles")) else []:
+        if not f.endswith((".txt", ".md")):
+            continue
+        for line in open(os.path.join(ROOT, "profiles", f)):
+            m = re.match(r"\s*dram_bytes_per_launch\[(\w+)\]\s*=\s*([0-9.eE+]+)", line)
+            if m and m.group(1) == kernel_tag:
+                return float(m.group(2)), f
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def build_problem():
+    from cel_v3_b200 import synth
+    rp, ci, v, x_true = synth.plain(SIDE, SEED)
+    return rp, ci, v, x_true
+
+
+def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
+    """Time the oracle's reference-order PCG on the host cores for a bounded
+    number of iterations and scale to solves/s."""
+    from oracle import celref as R
+    cores = os.cpu_count() or 1
+    workers = max(1, cores - 1)  # reference thread model: 1 idle master + workers
+    A = R.Matrix(rp, ci, v)
+    J = R.jacobi(R.diag(rp, ci, v))
+    red = R.RED_SEQ if red_seq else R.RED_TREE
+    t0 = time.perf_counter()
+    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=2, red=red, nworkers=workers)
+    probe = time.perf_counter() - t0
+    k = max(3, min(400, int(target_s / max(probe / 2.0, 1e-3))))
+    t0 = time.perf_counter()
+    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=k, red=red, nworkers=workers)
+    t = time.perf_counter() - t0
+    per_iter = t / (k + 1)  # set-up sweep ~ one iteration
+    return {"value": 1.0 / (per_iter * iters_per_solve), "unit": UNIT, "cores": cores,
+            "threads": workers + 1, "kind": "port",
+            "sample": f"oracle Jacobi-PCG (reference order, {workers} workers + idle master) on the "
+                      f"256^3 system: {k} iterations in {t:.2f} s, scaled by {iters_per_solve} "
+                      f"iterations per solve"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the reference path, timed."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import celref as R
+    rp, ci, v, x_true = build_problem()
+    b = R.spmv_csr(rp, ci, v, x_true, nworkers=max(1, (os.cpu_count() or 2) - 1))
+    cores = os.cpu_count() or 1
+    workers = max(1, cores - 1)
+    A = R.Matrix(rp, ci, v)
+    J = R.jacobi(R.diag(rp, ci, v))
+    # iterations of a full solve: the recurrence is the same as the GPU's; the
+    # count is taken from one full reference-order solve
+    t0 = time.perf_counter()
+    _, full = R.pcg_jacobi(A, J, b, eps_rel=EPS_REL, iter_max=5000, red=R.RED_SEQ, nworkers=workers)
+    t_full = time.perf_counter() - t0
+    iters = full["iter_done"]
+    sample_iters = max(2, int(round(6.0 / max(t_full / max(iters, 1), 1e-4))))
+    sample_iters = min(sample_iters, iters)
+
+    def step():
+        R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=sample_iters, red=R.RED_SEQ,
+                     nworkers=workers)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    t = time.perf_counter() - t0
+    per_iter = t / (args.steps * (sample_iters + 1))
+    value = 1.0 / (per_iter * iters)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "poisson7_256^3_pcg_jacobi_csr_fp64", "rows": int(rp.size - 1),
+                   "nnz": int(rp[-1]), "rel_res": EPS_REL, "x0": "zero",
+                   "reference_iterations": iters, "reference_full_solve_s": t_full,
+                   "sample_iterations_per_step": sample_iters},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "threads": workers + 1,
+                         "kind": "port",
+                         "sample": f"{args.steps} steps of {sample_iters} PCG iterations, scaled "
+                                   f"by the {iters} iterations of a full reference-order solve"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the Fortran reference cannot be built here (no gfortran/MPI); this arm times "
+                "oracle/, the C restatement of its MPI+OpenMP path, at mpirun -n 1",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from cel_v3_b200 import celgpu
+
+    rp, ci, v, x_true = build_problem()
+    n, nnz = rp.size - 1, int(rp[-1])
+    stream = torch.cuda.current_stream()
+    h = celgpu.Handle(local, stream.cuda_stream)
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    xt = torch.from_numpy(x_true).cuda()
+    b = torch.empty(n, dtype=torch.float64, device="cuda")
+    h.spmv(m, xt.data_ptr(), b.data_ptr())            # b = A x_true (bit-exact to the oracle)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    p = celgpu.params(eps_rel=EPS_REL, iter_max=5000, x0_mode=celgpu.X0_ZERO)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(val):
+        if world == 1:
+            return val
+        t = torch.tensor([val], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident solves (value) ----
+    infos = []
+    for _ in range(args.warmup):
+        infos.append(h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), p))
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        infos.append(h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), p))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    barrier()
+    ms = max_over_ranks(ms)
+    last = infos[-1]
+    assert all(i.status == celgpu.OK for i in infos), [i.status for i in infos]
+    iters = last.iter_done
+    value = world * args.steps / (ms / 1e3)
+    ms_per_step = ms / args.steps
+    pcg_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
+
+    # ---- roofline: the CSR SpMV kernel alone ----
+    y = torch.empty_like(b)
+    for _ in range(3):
+        h.spmv(m, xt.data_ptr(), y.data_ptr())
+    reps = 50
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        h.spmv(m, xt.data_ptr(), y.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = e0.elapsed_time(e1) / reps
+    spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    peak, peak_kind = measured_peaks()
+    achieved = spmv_bytes / (spmv_ms / 1e3) / 1e9
+    traffic, traffic_src = ncu_traffic("spmv_csr_256")
+
+    # ---- other precision forms on the same system (reported, not the value) ----
+    forms = {}
+    if not args.quick:
+        for name, kw in (("fp64_pcg_1e-10", dict(eps_rel=1e-10)),
+                         ("fp32_ir_1e-10", dict(eps_rel=1e-10, precision=celgpu.PREC_FP32_IR,
+                                                inner_eps_rel=1e-4)),
+                         ("fp32_ru_1e-10", dict(eps_rel=1e-10, precision=celgpu.PREC_FP32_RU,
+                                                inner_eps_rel=1e-2))):
+            pf = celgpu.params(iter_max=5000, x0_mode=celgpu.X0_ZERO, **kw)
+            h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            k = 3
+            for _ in range(k):
+                inf = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fms = e0.elapsed_time(e1) / k
+            forms[name] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
+                           "inner_iters": inf.arnoldi_steps, "verified_relres": inf.verified_relres,
+                           "status": inf.status}
+        base = forms["fp64_pcg_1e-10"]["solves_per_s"]
+        for k in ("fp32_ir_1e-10", "fp32_ru_1e-10"):
+            forms[k]["speedup_vs_fp64_at_1e-10"] = forms[k]["solves_per_s"] / base
+
+    # ---- e2e through the ELM interface with host buffers ----
+    h.elm_init(n, n, 1, (7, 0))
+    h.elm_insert_rows(1, rp + 1, ci + 1, v)
+    h.elm_set_solver(celgpu.SOLVER_PCG, p, diag_scaling=False)
+    h.elm_matrix_completed()
+    b_host = b.cpu().pin_memory()
+    x_host = torch.empty(n, dtype=torch.float64).pin_memory()
+    bh, xh = b_host.numpy(), x_host.numpy()
+    for _ in range(max(1, min(args.warmup, 2))):
+        h.elm_doit(bh)
+        h.elm_collect_solution(n, xh)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.steps):
+        ierr, niter, ftol = h.elm_doit(bh)
+        h.elm_collect_solution(n, xh)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall_e2e = time.perf_counter() - t0
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    h.elm_destroy()
+    assert ierr == 0, ierr
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_sample(rp, ci, v, b.cpu().numpy(), iters)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "poisson7_256^3_pcg_jacobi_csr_fp64", "rows": n, "nnz": nnz,
+                   "rel_res": EPS_REL, "x0": "zero", "rhs": "A*x_true, x_true~U[0,1) seed 1",
+                   "iterations": iters, "verified_relres": last.verified_relres,
+                   "l2": "inputs 1.9 GB resident, > 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "pcg": {"ms_per_iteration": ms_per_step / max(iters, 1),
+                "bytes_per_iteration": pcg_bytes,
+                "achieved_gbs": pcg_bytes * iters / (ms_per_step / 1e3) / 1e9,
+                "frac_of_peak": pcg_bytes * iters / (ms_per_step / 1e3) / 1e9 / peak},
+        "roofline": {"kernel": "csr_tma_kernel<double, EpiStore> (SpMV 256^3)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs (copy, burst)",
+                     "bytes_per_launch": spmv_bytes, "ms_per_launch": spmv_ms,
+                     "traffic": traffic, "traffic_source": traffic_src},
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                "api": "celg_elm_doit + celg_elm_collect_solution (pinned host b/x)",
+                "wall_s": wall_e2e},
+        "forms": forms,
+        "gpu_launches": args.steps * (3 * iters + 3),
+        "clocks": clk,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    m.destroy()
+    h.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="skip the extra precision forms")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

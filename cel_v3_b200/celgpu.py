@@ -44,6 +44,7 @@ X0_ZERO = 1
 X0_USER = 2
 PREC_FP64 = 0
 PREC_FP32_IR = 1
+PREC_FP32_RU = 2
 SOLVER_PCG = 0
 SOLVER_CG = 1
 SOLVER_GMRES = 2
@@ -231,13 +232,25 @@ class Matrix:
             pass
 
 
+STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream
+
+
+def _stream_arg(stream):
+    """None -> library-owned stream; 0 (torch's default stream) -> the legacy
+    default stream; anything else is a cudaStream_t handle."""
+    if stream is None:
+        return None
+    return ctypes.c_void_p(STREAM_LEGACY if int(stream) == 0 else int(stream))
+
+
 class Handle:
-    """One GPU and one CUDA stream (borrowed when `stream` is given)."""
+    """One GPU and one CUDA stream.  stream=None: the library creates its own;
+    otherwise the caller's cudaStream_t (0 = the legacy default stream, e.g.
+    torch.cuda.current_stream().cuda_stream on the default stream)."""
 
     def __init__(self, device=0, stream=None):
         h = ctypes.c_void_p()
-        _check(lib.celg_create(ctypes.byref(h), int(device),
-                               ctypes.c_void_p(stream) if stream else None), "celg_create")
+        _check(lib.celg_create(ctypes.byref(h), int(device), _stream_arg(stream)), "celg_create")
         self.ptr = h
         self.mats = []
 
@@ -267,8 +280,7 @@ class Handle:
         return s.value
 
     def set_stream(self, stream):
-        _check(lib.celg_set_stream(self.ptr, ctypes.c_void_p(stream) if stream else None),
-               "celg_set_stream")
+        _check(lib.celg_set_stream(self.ptr, _stream_arg(stream)), "celg_set_stream")
 
     # ---- matrices
     def matrix_from_csr(self, rp, ci, v, index_base=0):

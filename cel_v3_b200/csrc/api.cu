@@ -261,6 +261,10 @@ extern "C" int celg_create(celg_handle** out, int device, void* stream) {
     }
     h->own_stream = true;
   }
+  if (cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    celg_destroy(h);
+    return CELG_ERR_CUDA;
+  }
   cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
   if (cudaMalloc(&h->ticket, 64) != cudaSuccess || cudaMalloc(&h->err_d, 64) != cudaSuccess ||
       cudaMalloc(&h->scal_d, 64 * sizeof(double)) != cudaSuccess ||
@@ -298,10 +302,13 @@ extern "C" int celg_destroy(celg_handle* h) {
   cudaFree(h->wv);
   cudaFree(h->state_d);
   cudaFreeHost(h->state_h);
+  cudaFree(h->ru_state_d);
+  cudaFreeHost(h->ru_state_h);
   cudaFree(h->hist_d);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
   delete h;
   return CELG_OK;
 }
@@ -561,6 +568,7 @@ extern "C" int celg_pcg_jacobi(celg_handle* h, celg_mat* m, const double* b_d, d
   if (st) return st;
   CELG_CUDA(cudaSetDevice(h->device));
   if (p->precision == CELG_PREC_FP32_IR) return ir_solve(h, m, b_d, x_d, p, res);
+  if (p->precision == CELG_PREC_FP32_RU) return ru_solve(h, m, b_d, x_d, p, res);
   return pcg_solve(h, m, b_d, x_d, p, res);
 }
 

@@ -45,8 +45,9 @@ struct GraphEntry {
 
 struct celg_handle {
   int device = 0;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // work stream (owned, or the caller's)
   bool own_stream = false;
+  cudaStream_t cap_stream = nullptr;  // private stream used only to capture graphs
   int sms = 148;
   // reduction scratch: partials (2 rows of max tiles) and a completion ticket
   double* partials = nullptr;
@@ -62,6 +63,8 @@ struct celg_handle {
   size_t wcap = 0;           // elements
   celg::PcgState* state_d = nullptr;
   celg::PcgState* state_h = nullptr;  // pinned
+  void* ru_state_d = nullptr;         // reliable-update solver state
+  void* ru_state_h = nullptr;         // pinned
   // cached solve graphs (keyed by matrix, vectors and parameters)
   std::vector<celg::GraphEntry> graphs;
   double* hist_d = nullptr;
@@ -138,5 +141,8 @@ int gmres_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const c
                 celg_result* res);
 int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
              celg_result* res);
+int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+             celg_result* res);
+int ensure_f32(celg_handle* h, size_t n);
 
 }  // namespace celg

@@ -3,8 +3,8 @@
 //   x = x0;  for k = 0, 1, ...:
 //     r = b - A x,  ||r||            (FP64 matrix, FP64 vectors, on the GPU)
 //     stop when ||r|| <= max(eps_abs, eps_rel ||b||)
-//     d = PCG_fp32(A32, r32)          (inner tolerance inner_eps_rel ||r32||)
-//     x = x + d                       (FP64)
+//     d = PCG_fp32(A32, r/||r||)      (inner tolerance inner_eps_rel)
+//     x = x + ||r|| d                 (FP64)
 // The outer residual, update and stopping test stay in binary64, so the
 // reported accuracy is the FP64-verified ||b - A x|| / ||b||.  The inner
 // solve reads 8 bytes per non-zero (float value + int32 column) and float
@@ -17,15 +17,21 @@
 
 namespace celg {
 
-// x = x + (double) d   and r32 = (float) r handled by small sweeps
+// The inner system is solved for the normalised residual r / ||r|| (so that
+// its scale does not meet the absolute |alpha| guard of the PCG loop or the
+// FP32 range) and the correction is scaled back:
+//   r32 = (float)(r * (1/||r||)),   x = x + ||r|| * (double) d32
 struct OpAddF32 {
   static constexpr int NRED = 0;
   struct Regs { double x; float d; };
   double* x;
   const float* d;
+  double scale;
   __device__ bool prepare() { return true; }
   __device__ void load(long i, Regs& g) const { g.x = x[i]; g.d = __ldg(d + i); }
-  __device__ void compute(long i, Regs& g, double*) const { x[i] = dadd(g.x, (double)g.d); }
+  __device__ void compute(long i, Regs& g, double*) const {
+    x[i] = dadd(g.x, dmul(scale, (double)g.d));
+  }
   __device__ void finish(double*) const {}
 };
 
@@ -34,9 +40,10 @@ struct OpToF32 {
   struct Regs { double r; };
   const double* r;
   float* r32;
+  double inv;
   __device__ bool prepare() { return true; }
   __device__ void load(long i, Regs& g) const { g.r = __ldg(r + i); }
-  __device__ void compute(long i, Regs& g, double*) const { r32[i] = (float)g.r; }
+  __device__ void compute(long i, Regs& g, double*) const { r32[i] = (float)dmul(g.r, inv); }
   __device__ void finish(double*) const {}
 };
 
@@ -51,7 +58,7 @@ struct OpX0 {
   __device__ void finish(double*) const {}
 };
 
-static int ensure_f32(celg_handle* h, size_t n) {
+int ensure_f32(celg_handle* h, size_t n) {
   if (n <= h->f32cap && h->f32 && h->ir_d) return CELG_OK;
   CELG_CUDA(cudaStreamSynchronize(h->stream));
   graph_cache_clear(h);
@@ -60,7 +67,7 @@ static int ensure_f32(celg_handle* h, size_t n) {
   h->f32 = nullptr;
   h->ir_d = nullptr;
   const size_t cap = std::max<size_t>(n, 1024);
-  CELG_CUDA(cudaMalloc(&h->f32, sizeof(float) * cap * 5));
+  CELG_CUDA(cudaMalloc(&h->f32, sizeof(float) * cap * 5));  // 5 float vectors
   CELG_CUDA(cudaMalloc(&h->ir_d, sizeof(double) * cap));
   h->f32cap = cap;
   h->ircap = cap;
@@ -142,7 +149,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
       break;
     }
     if (outer >= outer_max) break;
-    st = launch_tile(h, n, OpToF32{r, b32});
+    st = launch_tile(h, n, OpToF32{r, b32, 1.0 / rn});
     if (st) break;
     PcgState s;
     const int ist = pcg_run<float>(h, B, &ip, m, &s);
@@ -151,7 +158,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
       st = ist;
       break;
     }
-    st = launch_tile(h, n, OpAddF32{x, d32});
+    st = launch_tile(h, n, OpAddF32{x, d32, rn});
     ++outer;
   }
   cudaEventRecord(e1, h->stream);

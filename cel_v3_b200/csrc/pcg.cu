@@ -20,9 +20,11 @@
 // Algorithmic bytes per FP64 CSR iteration: 12 nnz + 4 (n+1) + 104 n.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
+#include "graph.cuh"
 #include "pcg_internal.cuh"
 
 namespace celg {
@@ -81,45 +83,8 @@ void graph_cache_drop_matrix(celg_handle* h, const void* m) {
   }
 }
 
-// Append a WHILE conditional node after the work captured so far on
-// h->stream and capture the loop body (recorded by `body`) into it.
-template <class Body>
-static int capture_while(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t cap_graph;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  CELG_CUDA(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cap_graph, &deps, &ndeps));
-  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-  cp.conditional.handle = cond;
-  cp.conditional.type = cudaGraphCondTypeWhile;
-  cp.conditional.size = 1;
-  cudaGraphNode_t cnode;
-  CELG_CUDA(cudaGraphAddNode(&cnode, cap_graph, deps, ndeps, &cp));
-  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
-  CELG_CUDA(cudaStreamUpdateCaptureDependencies(h->stream, &cnode, 1,
-                                                cudaStreamSetCaptureDependencies));
-  cudaStream_t side;
-  CELG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-  cudaError_t e = cudaStreamBeginCaptureToGraph(side, bodyg, nullptr, nullptr, 0,
-                                                cudaStreamCaptureModeRelaxed);
-  int st = CELG_OK;
-  if (e == cudaSuccess) {
-    cudaStream_t main_stream = h->stream;
-    h->stream = side;
-    st = body();
-    h->stream = main_stream;
-    cudaGraph_t out;
-    e = cudaStreamEndCapture(side, &out);
-  }
-  cudaStreamDestroy(side);
-  if (st) return st;
-  CELG_CUDA(e);
-  return CELG_OK;
-}
-
 template <typename VT>
-static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
+static int pcg_setup(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
   const long n = B.A->n;
   constexpr bool kF64 = std::is_same<VT, double>::value;
   int st = launch_tile(h, n, OpPre<VT>{B.b, B.x, p->x0_mode, p->eps_abs, p->eps_rel, a});
@@ -128,38 +93,72 @@ static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p
     if (B.jad) {
       st = launch_jad(h, *B.A, *B.jad, B.x, EpiStore<double>{B.r, 0});
       if (!st) st = launch_tile(h, n, OpInitNat<double>{B.b, B.r, B.p, B.J, a});
-    } else {
-      st = launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
+      return st;
     }
-  } else {
-    st = launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
   }
-  if (st) return st;
-  st = capture_while(h, a.cond, [&]() -> int {
-    int s2 = CELG_OK;
-    if constexpr (kF64) {
-      if (B.jad)
-        s2 = launch_jad(h, *B.A, *B.jad, B.p, EpiAp<double>{B.v, B.p, a});
-      else
-        s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
-    } else {
+  return launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
+}
+
+template <typename VT>
+static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
+  const long n = B.A->n;
+  int s2 = CELG_OK;
+  if constexpr (std::is_same<VT, double>::value) {
+    if (B.jad)
+      s2 = launch_jad(h, *B.A, *B.jad, B.p, EpiAp<double>{B.v, B.p, a});
+    else
       s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
-    }
-    if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.x, B.r, B.p, B.v, B.J, a, 0.0});
-    if (!s2) s2 = launch_tile(h, n, OpDirection<VT>{B.p, B.r, B.J, a, 0.0});
-    return s2;
-  });
-  if (st) return st;
-  if constexpr (kF64) {
+  } else {
+    s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+  }
+  if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.x, B.r, B.p, B.v, B.J, a, 0.0});
+  if (!s2) s2 = launch_tile(h, n, OpDirection<VT>{B.p, B.r, B.J, a, 0.0});
+  return s2;
+}
+
+template <typename VT>
+static int pcg_tail(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
+  const long n = B.A->n;
+  if constexpr (std::is_same<VT, double>::value) {
     if (!B.verify_vals) return CELG_OK;
     // verification sweep in FP64
     if (B.jad) {
-      st = launch_jad(h, *B.A, *B.jad, B.x, EpiStore<double>{B.v, 0});
+      int st = launch_jad(h, *B.A, *B.jad, B.x, EpiStore<double>{B.v, 0});
       if (!st) st = launch_tile(h, n, OpVerifyNat{B.b, B.v, a.st});
-    } else {
-      st = launch_csr<double>(h, *B.A, B.verify_vals, B.x, EpiVerify{B.b, a.st});
+      return st;
     }
+    return launch_csr<double>(h, *B.A, B.verify_vals, B.x, EpiVerify{B.b, a.st});
   }
+  return CELG_OK;
+}
+
+template <typename VT>
+static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
+  int st = pcg_setup(h, B, p, a);
+  if (st) return st;
+  st = capture_while(h, a.cond, [&]() -> int { return pcg_body(h, B, a); });
+  if (st) return st;
+  return pcg_tail(h, B, a);
+}
+
+// Profiling mode (CELG_GRAPH=0): the same kernels launched one by one from a
+// host loop, so that kernel profilers can attribute time to each of them
+// (they cannot see into graphs with conditional nodes).  Chunks of 8
+// iterations are queued between reads of the device's continue flag; the
+// kernels of an inactive solve return at once.
+template <typename VT>
+static int run_host_loop(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
+  a.cond = 0;
+  int st = pcg_setup(h, B, p, a);
+  for (int it = 0; !st && it < p->iter_max; it += 8) {
+    for (int k = 0; k < 8 && !st; ++k) st = pcg_body(h, B, a);
+    if (st) break;
+    CELG_CUDA(cudaMemcpyAsync(h->state_h, h->state_d, sizeof(PcgState), cudaMemcpyDeviceToHost,
+                              h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    if (!h->state_h->active) break;
+  }
+  if (!st) st = pcg_tail(h, B, a);
   return st;
 }
 
@@ -186,46 +185,24 @@ int pcg_run(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, const vo
   if (st) return st;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
 
-  const std::string key = pcg_key(B, p, hist_cap, mat);
-  GraphEntry* ge = nullptr;
-  for (auto& e : h->graphs)
-    if (e.key == key) ge = &e;
-  if (!ge) {
-    if (h->graphs.size() >= 8) {
-      cudaStreamSynchronize(h->stream);
-      graph_cache_clear(h);
+  if (!graphs_enabled()) {
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = run_host_loop(h, B, p, PcgArgs{h->state_d, h->hist_d, hist_cap, p->iter_max, 0, h->err_d});
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    const std::string key = pcg_key(B, p, hist_cap, mat);
+    GraphEntry* ge = graph_cache_find(h, key);
+    if (!ge) {
+      st = graph_build(h, key, [&](cudaGraphConditionalHandle cond) -> int {
+        return record_pcg<VT>(h, B, p, PcgArgs{h->state_d, h->hist_d, hist_cap, p->iter_max, cond, h->err_d});
+      }, &ge);
+      if (st) return st;
     }
-    CELG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeRelaxed));
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t cap_graph;
-    cudaError_t e = cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cap_graph, nullptr, nullptr);
-    cudaGraphConditionalHandle cond = 0;
-    if (e == cudaSuccess)
-      e = cudaGraphConditionalHandleCreate(&cond, cap_graph, 1, cudaGraphCondAssignDefault);
-    PcgArgs a{h->state_d, h->hist_d, hist_cap, p->iter_max, cond, h->err_d};
-    int rst = e == cudaSuccess ? record_pcg<VT>(h, B, p, a) : CELG_ERR_CUDA;
-    cudaGraph_t g = nullptr;
-    cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
-    if (e != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return cuda_status(e, "conditional handle");
-    }
-    if (rst || e2 != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      return rst ? rst : cuda_status(e2, "cudaStreamEndCapture");
-    }
-    cudaGraphExec_t gx;
-    cudaError_t e3 = cudaGraphInstantiate(&gx, g, 0);
-    if (e3 != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return cuda_status(e3, "cudaGraphInstantiate");
-    }
-    h->graphs.push_back(GraphEntry{key, g, gx});
-    ge = &h->graphs.back();
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   }
-  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
-  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
-  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   CELG_CUDA(cudaMemcpyAsync(h->state_h, h->state_d, sizeof(PcgState), cudaMemcpyDeviceToHost,
                             h->stream));
   CELG_CUDA(cudaMemcpyAsync(h->scal_h + 8, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));

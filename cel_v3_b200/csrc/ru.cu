@@ -1,0 +1,355 @@
+// ru.cu -- FP32-storage Jacobi-PCG with FP64 reliable updates.
+//
+// A refinement scheme that keeps the Krylov direction across corrections
+// (the "reliable update" mixed-precision CG of Clark, Babich, Barros,
+// Brower and Rebbi, Comput. Phys. Commun. 181 (2010) 1517, with point-Jacobi
+// preconditioning):
+//
+//   x64 = x0;  r64 = b - A x64;  r = (float) r64;  d = 0;  p = J r;  rz = r.J r
+//   loop (FP32 matrix and vectors, FP64 scalars and reductions):
+//     v = A32 p;  sigma = rz / (p.v)
+//     d += sigma p;  r -= sigma v;  rz' = r.J r;  ||r||
+//     if ||r|| < delta * ||r64|| or ||r|| <= eps:          reliable update
+//         x64 += d;  d = 0;                                 (FP64)
+//         r64 = b - A x64 with the FP64 matrix;  r = (float) r64
+//         stop when ||r64|| <= eps                          (FP64 test)
+//         rz' = r.J r
+//     beta = rz'/rz;  rz = rz';  p = J r + beta p
+//
+// Compared with restarting an inner solve at every correction (ir.cu), the
+// search direction survives the residual replacement, so the iteration count
+// stays close to the FP64 solver's while every sweep moves FP32 data.  The
+// update threshold delta is celg_params.inner_eps_rel.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "graph.cuh"
+#include "pcg_internal.cuh"
+
+namespace celg {
+
+struct RuState {
+  PcgState s;      // alpha = rz, sigma, beta, norm = ||r|| (FP32 recurrence), bnorm, eps
+  double maxr;     // ||r64|| at the last reliable update
+  double rz_prev;  // rz before the current iteration's update
+  double norm64;   // last FP64 residual norm
+  double delta;
+  int update;      // 1: the FP32 recurrence asks for a reliable update
+  int updates;
+};
+
+struct RuArgs {
+  RuState* st;
+  double* hist;
+  int hist_cap;
+  int iter_max;
+  cudaGraphConditionalHandle cond;
+  const int* errw;
+  PcgArgs pcg() const {
+    return PcgArgs{&st->s, hist, hist_cap, iter_max, cond, errw};
+  }
+};
+
+__device__ __forceinline__ int ru_go(const RuState* r, int iter_max, const int* errw) {
+  const PcgState* s = &r->s;
+  return (s->err == 0 && *(volatile const int*)errw == 0 && s->iter < iter_max &&
+          r->norm64 > s->eps)
+             ? 1
+             : 0;
+}
+
+// RU0: x0 and ||b||, eps
+struct OpRuPre {
+  static constexpr int NRED = 1;
+  struct Regs { double b; };
+  const double* b;
+  double* x;
+  int x0_mode;
+  double eps_abs, eps_rel, delta;
+  RuArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    if (x0_mode == CELG_X0_REF_ONES) x[i] = 1.0;
+    else if (x0_mode == CELG_X0_ZERO) x[i] = 0.0;
+    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+  }
+  __device__ void finish(double* tot) const {
+    RuState* r = a.st;
+    r->s.bnorm = sqrt(tot[0]);
+    double e = eps_abs;
+    if (eps_rel > 0.0 && eps_rel * r->s.bnorm > e) e = eps_rel * r->s.bnorm;
+    r->s.eps = e;
+    r->s.err = 0;
+    r->s.iter = 0;
+    r->s.active = 1;
+    r->s.vres = 0.0;
+    r->delta = delta;
+    r->update = 1;  // the set-up residual is a reliable update
+    r->updates = 0;
+  }
+};
+
+// FP64 residual with the FP64 matrix, and its FP32 copy:
+//   r64 = b - (0 + A x);  r = (float) r64;  z = (double) r * J;  rz = r.z;  ||r64||^2
+// init: also p = (float) z.  Active only when a reliable update is pending.
+struct EpiRuResidual {
+  static constexpr int NRED = 2;
+  const double* b;
+  float* r;
+  float* p;        // non-null only at set-up
+  const float* J;
+  RuArgs a;
+  int init;
+  __device__ bool active() const { return *(volatile int*)&a.st->update != 0; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double r64 = __dsub_rn(b[i], dadd(0.0, s));
+    const float rf = (float)r64;
+    r[i] = rf;
+    const double z = dmul((double)rf, (double)J[i]);
+    if (init) p[i] = (float)z;
+    acc[0] = dadd(acc[0], dmul((double)rf, z));
+    acc[1] = dadd(acc[1], dmul(r64, r64));
+  }
+  __device__ void finish(double* tot) const {
+    RuState* st = a.st;
+    st->norm64 = sqrt(tot[1]);
+    st->maxr = st->norm64;
+    st->update = 0;
+    st->updates += 1;
+    if (init) {
+      st->s.alpha = tot[0];
+      st->s.norm = st->norm64;
+      if (a.hist && a.hist_cap > 0) a.hist[0] = st->norm64;
+      st->s.hist_len = 1;
+    } else {
+      st->s.beta = tot[0] / st->rz_prev;
+      st->s.alpha = tot[0];
+      if (a.hist && st->s.iter < a.hist_cap) a.hist[st->s.iter] = st->norm64;
+    }
+    st->s.active = ru_go(st, a.iter_max, a.errw);
+    set_cond(a.cond, st->s.active);
+  }
+};
+
+// d += sigma p ; r -= sigma v ; rz' = r.J r ; ||r||^2 ; update decision
+struct OpRuStep {
+  static constexpr int NRED = 2;
+  struct Regs { float d, r, p, v, J; };
+  float* d;
+  float* r;
+  const float* p;
+  const float* v;
+  const float* J;
+  RuArgs a;
+  double sg;
+  __device__ bool prepare() {
+    if (*(volatile int*)&a.st->s.active == 0) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(a.cond, 0);
+      return false;
+    }
+    sg = a.st->s.sigma;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const {
+    g.d = d[i];
+    g.r = r[i];
+    g.p = __ldg(p + i);
+    g.v = __ldg(v + i);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    d[i] = (float)dadd((double)g.d, dmul(sg, (double)g.p));
+    const float ri = (float)dadd((double)g.r, dmul(-sg, (double)g.v));
+    r[i] = ri;
+    const double z = dmul((double)ri, (double)g.J);
+    acc[0] = dadd(acc[0], dmul((double)ri, z));
+    acc[1] = dadd(acc[1], dmul((double)ri, (double)ri));
+  }
+  __device__ void finish(double* tot) const {
+    RuState* st = a.st;
+    st->rz_prev = st->s.alpha;
+    st->s.beta = tot[0] / st->s.alpha;
+    st->s.alpha = tot[0];
+    st->s.norm = sqrt(tot[1]);
+    st->s.iter += 1;
+    if (a.hist && st->s.iter < a.hist_cap) a.hist[st->s.iter] = st->s.norm;
+    st->s.hist_len = min(st->s.iter + 1, a.hist_cap);
+    const int upd = (st->s.norm < st->delta * st->maxr) || (st->s.norm <= st->s.eps) ||
+                    (st->s.iter >= a.iter_max);
+    st->update = upd;
+    if (!upd) {
+      // FP32 recurrence continues; stop only on the iteration cap or an error
+      const int go = (st->s.err == 0 && *(volatile const int*)a.errw == 0 &&
+                      st->s.iter < a.iter_max && fabs(st->s.alpha) > 0.0)
+                         ? 1
+                         : 0;
+      st->s.active = go;
+      set_cond(a.cond, go);
+    }
+  }
+};
+
+// x64 += (double) d ; d = 0   (pending update, or unconditionally at the end)
+struct OpRuFlush {
+  static constexpr int NRED = 0;
+  struct Regs { double x; float d; };
+  double* x;
+  float* d;
+  RuArgs a;
+  int always;
+  __device__ bool prepare() { return always || *(volatile int*)&a.st->update != 0; }
+  __device__ void load(long i, Regs& g) const { g.x = x[i]; g.d = d[i]; }
+  __device__ void compute(long i, Regs& g, double*) const {
+    x[i] = dadd(g.x, (double)g.d);
+    d[i] = 0.0f;
+  }
+  __device__ void finish(double*) const {}
+};
+
+// final check ||b - A x|| / ||b|| in FP64
+struct EpiRuVerify {
+  static constexpr int NRED = 1;
+  const double* b;
+  RuState* st;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const {
+    st->s.vres = st->s.bnorm > 0.0 ? sqrt(tot[0]) / st->s.bnorm : sqrt(tot[0]);
+  }
+};
+
+struct OpZeroF {
+  static constexpr int NRED = 0;
+  struct Regs { int unused; };
+  float* d;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long, Regs&) const {}
+  __device__ void compute(long i, Regs&, double*) const { d[i] = 0.0f; }
+  __device__ void finish(double*) const {}
+};
+
+static int ru_setup(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+                    RuArgs a, float* r, float* pv, float* d) {
+  const long n = m->csr.n;
+  const double delta = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-2;
+  int st = launch_tile(h, n, OpRuPre{b, x, p->x0_mode, p->eps_abs, p->eps_rel, delta, a});
+  if (!st) st = launch_tile(h, n, OpZeroF{d});
+  if (!st)
+    st = launch_csr<double>(h, m->csr, m->csr.v, x, EpiRuResidual{b, r, pv, m->jacobi32, a, 1});
+  return st;
+}
+
+static int ru_body(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* r,
+                   float* pv, float* v, float* d) {
+  const long n = m->csr.n;
+  PcgArgs pa = a.pcg();
+  int st = launch_csr<float>(h, m->csr, m->csr.v32, pv, EpiAp<float>{v, pv, pa});
+  if (!st) st = launch_tile(h, n, OpRuStep{d, r, pv, v, m->jacobi32, a, 0.0});
+  if (!st) st = launch_tile(h, n, OpRuFlush{x, d, a, 0});
+  if (!st)
+    st = launch_csr<double>(h, m->csr, m->csr.v, x,
+                            EpiRuResidual{b, r, nullptr, m->jacobi32, a, 0});
+  if (!st) st = launch_tile(h, n, OpDirection<float>{pv, r, m->jacobi32, pa, 0.0});
+  return st;
+}
+
+static int ru_tail(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* d) {
+  int st = launch_tile(h, m->csr.n, OpRuFlush{x, d, a, 1});
+  if (!st) st = launch_csr<double>(h, m->csr, m->csr.v, x, EpiRuVerify{b, a.st});
+  return st;
+}
+
+int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
+             celg_result* res) {
+  const long n = m->csr.n;
+  if (!m->jacobi) return CELG_ERR_STATE;
+  if (!m->csr.v32 || !m->jacobi32) {
+    int st = celg_mat_make_fp32(m);
+    if (st) return st;
+  }
+  if (p->iter_max < 0) return CELG_ERR_ARG;
+  int st = ensure_f32(h, (size_t)n);
+  if (!st) st = ensure_partials(h, ntiles_of(n), 2);
+  const int hist_cap = p->iter_max + 1;
+  if (!st) st = ensure_state(h, hist_cap);
+  if (st) return st;
+  if (!h->ru_state_d) {
+    CELG_CUDA(cudaMalloc(&h->ru_state_d, sizeof(RuState)));
+    CELG_CUDA(cudaMallocHost(&h->ru_state_h, sizeof(RuState)));
+  }
+  RuState* sd = static_cast<RuState*>(h->ru_state_d);
+  RuState* sh = static_cast<RuState*>(h->ru_state_h);
+  const size_t cap = h->f32cap;
+  float* r = h->f32;
+  float* pv = r + cap;
+  float* v = pv + cap;
+  float* d = v + cap;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+
+  char kb[512];
+  std::snprintf(kb, sizeof(kb), "ru|%p|%d|%p|%p|%p|%d|%.17g|%.17g|%.17g|%d", (const void*)m,
+                m->csr.n, (const void*)b, (const void*)x, (const void*)r, p->x0_mode, p->eps_abs,
+                p->eps_rel, p->inner_eps_rel, p->iter_max);
+  const std::string key(kb);
+  RuArgs a0{sd, h->hist_d, hist_cap, p->iter_max, 0, h->err_d};
+  if (!graphs_enabled()) {
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = ru_setup(h, m, b, x, p, a0, r, pv, d);
+    for (int it = 0; !st && it < p->iter_max; it += 8) {
+      for (int k = 0; k < 8 && !st; ++k) st = ru_body(h, m, b, x, a0, r, pv, v, d);
+      if (st) break;
+      CELG_CUDA(cudaMemcpyAsync(sh, sd, sizeof(RuState), cudaMemcpyDeviceToHost, h->stream));
+      CELG_CUDA(cudaStreamSynchronize(h->stream));
+      if (!sh->s.active) break;
+    }
+    if (!st) st = ru_tail(h, m, b, x, a0, d);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    GraphEntry* ge = graph_cache_find(h, key);
+    if (!ge) {
+      st = graph_build(h, key, [&](cudaGraphConditionalHandle cond) -> int {
+        RuArgs a{sd, h->hist_d, hist_cap, p->iter_max, cond, h->err_d};
+        int s2 = ru_setup(h, m, b, x, p, a, r, pv, d);
+        if (!s2) s2 = capture_while(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d); });
+        if (!s2) s2 = ru_tail(h, m, b, x, a, d);
+        return s2;
+      }, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  }
+  CELG_CUDA(cudaMemcpyAsync(sh, sd, sizeof(RuState), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(h->scal_h + 8, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  int err_word = 0;
+  std::memcpy(&err_word, h->scal_h + 8, sizeof(int));
+  const RuState s = *sh;
+  int ret = CELG_OK;
+  if (err_word) ret = err_word;
+  else if (s.s.err) ret = s.s.err;
+  else if (!(s.norm64 <= s.s.eps)) ret = CELG_ERR_NOCONV;
+  h->last_iters = s.s.iter;
+  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 52.0 * n;
+  if (res) {
+    res->iter_done = s.s.iter;
+    res->final_norm2 = s.norm64;
+    res->bnorm = s.s.bnorm;
+    res->verified_relres = s.s.vres;
+    res->err = ret;
+    res->arnoldi_steps = s.updates;
+    st = copy_history(h, std::min(s.s.hist_len, hist_cap), res);
+    if (st) return st;
+  }
+  return ret;
+}
+
+}  // namespace celg

@@ -40,7 +40,11 @@ extern "C" {
 #define CELG_X0_USER 2     /* x_d holds the start vector on entry */
 
 #define CELG_PREC_FP64 0
-#define CELG_PREC_FP32_IR 1 /* FP32 matrix/Krylov vectors inside FP64 refinement */
+#define CELG_PREC_FP32_IR 1 /* FP32 matrix/Krylov vectors inside FP64 refinement:
+                             * each correction is a fresh inner PCG solve      */
+#define CELG_PREC_FP32_RU 2 /* FP32 PCG with FP64 reliable updates: the outer
+                             * residual, update and test in FP64, the search
+                             * direction kept across corrections              */
 
 #define CELG_SOLVER_PCG 0   /* cel_cgalg_jacobi   (BENCHMARK_CG + Jacobi)     */
 #define CELG_SOLVER_CG 1    /* cel_cgalg          (BENCHMARK_CG, no precond.) */
@@ -61,7 +65,8 @@ typedef struct {
   int precision;        /* CELG_PREC_*                                           */
   int literal_ref_bugs; /* CG: alpha-as-beta (:151); GMRES: unrotated Givens (:722-727) */
   int restart;          /* GMRES(m): m (gmres_max_restart)                      */
-  double inner_eps_rel; /* FP32-IR: inner PCG relative tolerance (default 1e-4) */
+  double inner_eps_rel; /* FP32-IR: inner PCG relative tolerance (default 1e-4);
+                         FP32-RU: residual drop that triggers an FP64 update */
   int inner_iter_max;   /* FP32-IR: inner iteration cap                         */
   int outer_max;        /* FP32-IR: refinement steps cap                        */
 } celg_params;
@@ -84,7 +89,11 @@ typedef struct {
 void celg_params_default(celg_params* p);
 
 /* ---- handle ---------------------------------------------------------------- */
-int celg_create(celg_handle** h, int device, void* stream /* cudaStream_t or NULL */);
+/* stream: NULL -> the handle creates and owns a non-blocking stream; any
+ * cudaStream_t otherwise, including cudaStreamLegacy ((cudaStream_t)0x1) for
+ * the legacy default stream.  Solve graphs are captured on a private stream
+ * and launched on this one. */
+int celg_create(celg_handle** h, int device, void* stream);
 int celg_destroy(celg_handle* h);
 int celg_set_stream(celg_handle* h, void* stream);
 const char* celg_status_string(int status);
@@ -120,7 +129,9 @@ int celg_mat_jacobi(celg_mat* m);
 int celg_mat_get_jacobi(const celg_mat* m, double* jacobi_host);
 /* Diagonal row scaling, cel_sp_mat_distr_scale
  * (src/fspmtdistr/cel_sp_mat_distr_format_module.f90:91-145): A_ij /= sqrt|d_i|,
- * jacobi = sqrt|d|/d; right-hand sides are scaled inside the solvers. */
+ * jacobi = sqrt|d|/d.  celg_elm_doit divides b by sqrt|d| itself
+ * (cel_sp_mat_distr_boundary_diag_scale); direct solver calls expect a
+ * right-hand side that is already scaled. */
 int celg_mat_scale_diagonal(celg_mat* m);
 /* FP32 copy of the matrix values for the refinement inner solve */
 int celg_mat_make_fp32(celg_mat* m);

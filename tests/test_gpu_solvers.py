@@ -192,10 +192,10 @@ def ir_oracle(rp, ci, v, b, tol=1e-10, inner=1e-4, outer_max=20):
             break
         if k == outer_max:
             break
-        d, info = R.pcg_jacobi_f32(rp, ci, v32, J32, r.astype(np.float32), eps_rel=inner,
-                                   red=R.RED_TREE)
+        r32 = (r * (1.0 / rn)).astype(np.float32)
+        d, info = R.pcg_jacobi_f32(rp, ci, v32, J32, r32, eps_rel=inner, red=R.RED_TREE)
         inner_total += info["iter_done"]
-        x = x + d.astype(np.float64)
+        x = x + rn * d.astype(np.float64)
     return x, np.array(hist), inner_total
 
 
@@ -281,3 +281,80 @@ def test_elm_rejects_offdiagonal_reinsert(gpu):
         h.elm_doit(np.ones(3))
     assert e.value.status == celgpu.ERR_STATE
     h.elm_destroy()
+
+
+def ru_oracle(rp, ci, v, b, eps_rel=1e-10, delta=1e-2, iter_max=5000):
+    """FP32 PCG with FP64 reliable updates, composed from oracle pieces in the
+    GPU's reduction order (see cel_v3_b200/csrc/ru.cu)."""
+    f32, f64 = np.float32, np.float64
+    J = R.jacobi(R.diag(rp, ci, v))
+    J32 = J.astype(f32).astype(f64)
+    v32 = v.astype(f32)
+    T = R.RED_TREE
+    n = rp.size - 1
+    x = np.zeros(n)
+    bn = np.sqrt(R.dot(b, b, T))
+    eps = eps_rel * bn
+
+    def residual(x):
+        r64 = b - R.spmv_csr(rp, ci, v, x)
+        r = r64.astype(f32)
+        z = r.astype(f64) * J32
+        return r, z, R.dot(r.astype(f64), z, T), np.sqrt(R.dot(r64, r64, T))
+
+    r, z, rz, norm64 = residual(x)
+    p = z.astype(f32)
+    d = np.zeros(n, f32)
+    maxr = norm64
+    hist = [norm64]
+    it, updates = 0, 1
+    active = norm64 > eps and it < iter_max
+    while active:
+        w = R.spmv_csr_f32(rp, ci, v32, p)
+        sigma = rz / R.dot(w.astype(f64), p.astype(f64), T)
+        d = (d.astype(f64) + sigma * p.astype(f64)).astype(f32)
+        r = (r.astype(f64) + (-sigma) * w.astype(f64)).astype(f32)
+        z = r.astype(f64) * J32
+        rz_new = R.dot(r.astype(f64), z, T)
+        norm = np.sqrt(R.dot(r.astype(f64), r.astype(f64), T))
+        rz_prev, beta, rz = rz, rz_new / rz, rz_new
+        it += 1
+        hist.append(norm)
+        if norm < delta * maxr or norm <= eps or it >= iter_max:
+            x = x + d.astype(f64)
+            d[:] = 0
+            r, z, rzh, norm64 = residual(x)
+            maxr = norm64
+            beta, rz = rzh / rz_prev, rzh
+            hist[it] = norm64
+            updates += 1
+            active = norm64 > eps and it < iter_max
+        else:
+            active = it < iter_max and abs(rz) > 0
+        if active:
+            p = (beta * p.astype(f64) + z).astype(f32)
+    x = x + d.astype(f64)
+    return x, np.array(hist), it, updates
+
+
+@pytest.mark.parametrize("name", ["poisson32", "diffusion"])
+def test_fp32_reliable_update_bitexact_and_accurate(gpu, name):
+    celgpu, h, torch = gpu
+    rp, ci, v, b = PROBS[name]
+    n = rp.size - 1
+    m = setup(h, rp, ci, v)
+    xd = dev(torch, np.zeros(n))
+    info = h.pcg_jacobi(m, dev(torch, b).data_ptr(), xd.data_ptr(), history=True,
+                        precision=celgpu.PREC_FP32_RU, eps_rel=1e-10, inner_eps_rel=1e-2,
+                        iter_max=5000)
+    xo, ho, it, updates = ru_oracle(rp, ci, v, b)
+    assert info.status == celgpu.OK
+    assert info.iter_done == it and info.arnoldi_steps == updates
+    assert np.array_equal(info.history, ho)
+    assert np.array_equal(xd.cpu().numpy(), xo)
+    assert info.verified_relres <= 1e-10
+    # iteration count close to the FP64 solver's at the same tolerance
+    _, i64 = R.pcg_jacobi(R.Matrix(rp, ci, v), R.jacobi(R.diag(rp, ci, v)), b, eps_rel=1e-10,
+                          red=R.RED_TREE, iter_max=5000)
+    assert it <= 1.25 * i64["iter_done"] + 5
+    m.destroy()
