@@ -1,0 +1,50 @@
+"""Runs one workload of the library for profiling (e.g. under ncu).
+
+  python -m cel_v3_b200.drive spmv SIDE [REPS]          REPS CSR SpMVs, SIDE^3 Poisson
+  python -m cel_v3_b200.drive pcg SIDE ITERS [fp64|ru|ir]
+                                                        one solve capped at ITERS iterations
+
+Set CELG_GRAPH=0 to launch the solver kernels from a host loop instead of
+one CUDA graph, so that a kernel profiler can attribute time to each kernel.
+"""
+import sys
+
+import numpy as np
+
+
+def main(argv):
+    import torch
+
+    from cel_v3_b200 import celgpu, synth
+    what, side = argv[0], int(argv[1])
+    rp, ci, v, xt = synth.plain(side, 1)
+    n = rp.size - 1
+    h = celgpu.Handle(0, torch.cuda.current_stream().cuda_stream)
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    x = torch.from_numpy(xt).cuda()
+    y = torch.zeros(n, dtype=torch.float64, device="cuda")
+    if what == "spmv":
+        for _ in range(int(argv[2]) if len(argv) > 2 else 4):
+            h.spmv(m, x.data_ptr(), y.data_ptr())
+        torch.cuda.synchronize()
+        print("spmv", side, float(y.sum()))
+    elif what == "pcg":
+        iters = int(argv[2])
+        mode = argv[3] if len(argv) > 3 else "fp64"
+        h.spmv(m, x.data_ptr(), y.data_ptr())  # b = A x_true
+        xs = torch.zeros_like(y)
+        prec = {"fp64": celgpu.PREC_FP64, "ru": celgpu.PREC_FP32_RU,
+                "ir": celgpu.PREC_FP32_IR}[mode]
+        kw = dict(inner_iter_max=iters, outer_max=1) if mode == "ir" else {}
+        info = h.pcg_jacobi(m, y.data_ptr(), xs.data_ptr(), precision=prec, eps_rel=1e-12,
+                            iter_max=iters, **kw)
+        torch.cuda.synchronize()
+        print("pcg", side, mode, info.iter_done, info.status)
+    else:
+        raise SystemExit(__doc__)
+    h.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))
