@@ -123,6 +123,7 @@ def _load():
         "celg_elm_collect_solution": (i, [vp, vp]),
         "celg_elm_performance": (i, [vp, dp, ip, dp]),
         "celg_elm_destroy": (i, [vp]),
+        "celg_dot_noalloc": (i, [i, vp, vp, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -158,6 +159,16 @@ def params(**kw):
             raise KeyError(k)
         setattr(p, k, v)
     return p
+
+
+NOALLOC_MAX_ROWS = 67108864
+
+
+def dot_noalloc(n, a_d, b_d, out_d, stream=0):
+    """celg_dot_noalloc: a.b into out_d[0] without any device allocation (see
+    include/celgpu.h); returns the status code."""
+    return lib.celg_dot_noalloc(int(n), ctypes.c_void_p(a_d), ctypes.c_void_p(b_d),
+                                ctypes.c_void_p(out_d), ctypes.c_void_p(int(stream)) if stream else None)
 
 
 class SolveInfo(dict):

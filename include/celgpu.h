@@ -173,6 +173,19 @@ int celg_gmres_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_
 int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_host,
                     double* x_host, const celg_params* p, celg_result* res);
 
+/* ---- allocation-free entry point ------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory (their device memory belongs to their own pool or to another
+ * framework's caching allocator): a dot product that needs no handle and
+ * keeps its reduction scratch in a fixed file-scope device array of the
+ * library.  out_d[0] = a.b in the same order as celg_dot.  n may not exceed
+ * CELG_NOALLOC_MAX_ROWS (CELG_ERR_ARG otherwise).  Calls share the array:
+ * calls whose kernels overlap on the GPU race.  The first call on a device
+ * resolves the array's address; make it before any stream capture.
+ * stream: a cudaStream_t of the current device, NULL for the default stream. */
+#define CELG_NOALLOC_MAX_ROWS 67108864
+int celg_dot_noalloc(int n, const double* a_d, const double* b_d, double* out_d, void* stream);
+
 /* ---- ELM assembly API (src/felmsolver/cel_elmsolver_module.f90) -------------- */
 /* cel_elmSolverInitialization (:103-153): n_total rows, n_local local rows
  * starting at 1-based row row_low, nnz_hint[2] nonzeros per row (diagonal and
