@@ -131,6 +131,47 @@ def build_problem():
     return rp, ci, v, x_true
 
 
+def batch_form(h, celgpu, torch, stream):
+    """64 variable-coefficient systems (sides 16..96, seed 4) to rel-res 1e-8:
+    one batched launch against the plain path solving them one by one."""
+    from cel_v3_b200 import synth
+    probs = synth.batch_problems()
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for _, rp, ci, v, _ in probs]
+    bs = [torch.from_numpy(b).cuda() for *_, b in probs]
+    xs = [torch.zeros_like(b) for b in bs]
+    p = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def one_by_one():
+        return [h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), p) for m, b, x in zip(mats, bs, xs)]
+
+    def batched():
+        return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p)
+
+    out = {}
+    for name, fn in (("one_by_one", one_by_one), ("batched", batched)):
+        fn()
+        torch.cuda.synchronize()
+        reps = 3
+        e0.record(stream)
+        for _ in range(reps):
+            infos = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "solves_per_s": len(mats) * 1e3 / ms,
+                     "max_iters": max(i.iter_done for i in infos),
+                     "sum_iters": sum(i.iter_done for i in infos),
+                     "worst_verified_relres": max(i.verified_relres for i in infos),
+                     "all_ok": all(i.status == celgpu.OK for i in infos)}
+    out["speedup_batched_vs_one_by_one"] = out["batched"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
+    out["systems"] = len(mats)
+    out["rows"] = int(sum(s ** 3 for s, *_ in probs))
+    for m in mats:
+        m.destroy()
+    return out
+
+
 def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
     """Time the oracle's reference-order PCG on the host cores for a bounded
     number of iterations and scale to solves/s."""
@@ -309,6 +350,7 @@ def run_gpu(args):
         base = forms["fp64_pcg_1e-10"]["solves_per_s"]
         for k in ("fp32_ir_1e-10", "fp32_ru_1e-10"):
             forms[k]["speedup_vs_fp64_at_1e-10"] = forms[k]["solves_per_s"] / base
+        forms["batched_64"] = batch_form(h, celgpu, torch, stream)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))

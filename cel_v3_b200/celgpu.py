@@ -124,6 +124,7 @@ def _load():
         "celg_elm_performance": (i, [vp, dp, ip, dp]),
         "celg_elm_destroy": (i, [vp]),
         "celg_dot_noalloc": (i, [i, vp, vp, vp, vp]),
+        "celg_pcg_batched": (i, [vp, i, vp, vp, vp, ctypes.POINTER(Params), vp]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -374,6 +375,19 @@ class Handle:
     def gmres_jacobi(self, mat, b_d, x_d, p=None, history=False, **kw):
         p = p or params(**kw)
         return self._solve(lib.celg_gmres_jacobi, "celg_gmres_jacobi", mat, b_d, x_d, p, history)
+
+    def pcg_batched(self, mats, b_ptrs, x_ptrs, p=None, **kw):
+        """Jacobi-PCG on many systems in one device-driven loop; returns a list
+        of per-system SolveInfo."""
+        p = p or params(**kw)
+        k = len(mats)
+        M = (ctypes.c_void_p * k)(*[m.ptr for m in mats])
+        B = (ctypes.c_void_p * k)(*[ctypes.c_void_p(int(b)) for b in b_ptrs])
+        X = (ctypes.c_void_p * k)(*[ctypes.c_void_p(int(x)) for x in x_ptrs])
+        res = (Result * k)()
+        st = lib.celg_pcg_batched(self.ptr, k, M, B, X, ctypes.byref(p), res)
+        _check(st, "celg_pcg_batched", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return [_info(r, None, r.err) for r in res]
 
     def solve_host(self, mat, b, x=None, solver=SOLVER_PCG, p=None, **kw):
         """Solve from host arrays (the copies are part of the call)."""

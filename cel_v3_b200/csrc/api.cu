@@ -287,6 +287,8 @@ extern "C" int celg_destroy(celg_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->elm) celg_elm_destroy(h);
+  batch_free(h->batch);
+  h->batch = nullptr;
   graph_cache_clear(h);
   cudaFree(h->partials);
   cudaFree(h->sb);
@@ -403,8 +405,13 @@ extern "C" int celg_mat_destroy(celg_mat* m) {
   celg_handle* h = m->h;
   cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
-  // cached solve graphs may reference this matrix
+  // cached solve graphs (and a cached batch) may reference this matrix
   graph_cache_drop_matrix(h, m);
+  if (h->batch) {
+    graph_cache_clear(h);
+    batch_free(h->batch);
+    h->batch = nullptr;
+  }
   free_mat_arrays(m);
   delete m;
   return CELG_OK;

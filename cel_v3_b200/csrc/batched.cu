@@ -1,0 +1,520 @@
+// batched.cu -- Jacobi-PCG on many independent systems of uneven size in one
+// device-driven loop.
+//
+// The systems are concatenated into one block-diagonal CSR matrix, each
+// system's rows padded to whole 1024-row tiles (padding rows are empty, with
+// b = x = 0 and Jacobi 0), so that every tile belongs to one system.  Every
+// system keeps its own scalars (alpha, sigma, beta, ||r||, iteration count,
+// active flag) in device memory.  One CUDA graph runs
+//   set-up sweeps, WHILE(any system active){K1, K2, K3}, verification
+// over all tiles at once; the tiles of systems that converged are skipped,
+// and each system's reductions are finished by the CTA that completes its
+// last tile, in the same order as a single solve.  A system's result is
+// therefore bit-identical to solving it alone with celg_pcg_jacobi, while the
+// small systems no longer leave most of the GPU idle and the per-iteration
+// launch cost is paid once for the whole batch.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "graph.cuh"
+#include "pcg_internal.cuh"
+
+namespace celg {
+
+struct BatchArgs {
+  double *alpha, *sigma, *beta, *norm, *bnorm, *eps, *vres;
+  int *iter, *active, *err, *n_active;
+  BatchRed br;
+  int nsys;
+  int nlive;  // systems with rows (empty systems are never active)
+  int iter_max;
+  cudaGraphConditionalHandle cond;
+  const int* errw;
+  __device__ int go(int s) const {
+    return (err[s] == 0 && *(volatile const int*)errw == 0 && iter[s] < iter_max &&
+            fabs(alpha[s]) > kRealSmall && norm[s] > eps[s])
+               ? 1
+               : 0;
+  }
+  __device__ void settle(int s) const {
+    const int g = go(s);
+    active[s] = g;
+    if (!g) atomicSub(n_active, 1);
+  }
+  __device__ int sys_of(long t) const { return br.tile_sys[t]; }
+};
+
+// x0, ||b|| and eps per system
+struct BOpPre {
+  static constexpr int NRED = 1;
+  static constexpr bool kBatched = true;
+  struct Regs { double b; };
+  const double* b;
+  double* x;
+  int x0_mode;
+  double eps_abs, eps_rel;
+  BatchArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ bool tile_active(long) const { return true; }
+  __device__ void begin_tile(long) {}
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    if (x0_mode == CELG_X0_REF_ONES) x[i] = 1.0;
+    else if (x0_mode == CELG_X0_ZERO) x[i] = 0.0;
+    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    a.bnorm[s] = sqrt(tot[0]);
+    double e = eps_abs;
+    if (eps_rel > 0.0 && eps_rel * a.bnorm[s] > e) e = eps_rel * a.bnorm[s];
+    a.eps[s] = e;
+    a.err[s] = 0;
+    a.iter[s] = 0;
+    a.active[s] = 1;
+    a.vres[s] = 0.0;
+  }
+  __device__ void finish_global() const { *a.n_active = a.nlive; }
+};
+
+// r = b - (0 + A x); p = J r; alpha = r.p; ||r||
+struct BEpiInit {
+  static constexpr int NRED = 2;
+  static constexpr bool kBatched = true;
+  const double* b;
+  double* r;
+  double* p;
+  const double* J;
+  BatchArgs a;
+  __device__ bool active() const { return true; }
+  __device__ bool tile_active(long) const { return true; }
+  __device__ void begin_tile(long) {}
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    r[i] = ri;
+    const double z = dmul(ri, J[i]);
+    p[i] = z;
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    a.alpha[s] = tot[0];
+    a.norm[s] = sqrt(tot[1]);
+    a.iter[s] = 0;
+    a.settle(s);
+  }
+  __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
+};
+
+// K1: v = 0 + A p; pv = v.p; sigma = alpha / pv
+struct BEpiAp {
+  static constexpr int NRED = 1;
+  static constexpr bool kBatched = true;
+  double* v;
+  const double* p;
+  BatchArgs a;
+  __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
+  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
+  __device__ void begin_tile(long) {}
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double vi = dadd(0.0, s);
+    v[i] = vi;
+    acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    const double sg = a.alpha[s] / tot[0];
+    a.sigma[s] = sg;
+    if (!isfinite(sg)) {
+      a.err[s] = kErrBreakdown;
+      a.active[s] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {}
+};
+
+// K2: x += sigma p; r += (-sigma) v; rz, rr; scalars and per-system test
+struct BOpUpdate {
+  static constexpr int NRED = 2;
+  static constexpr bool kBatched = true;
+  struct Regs { double x, r, p, v, J; };
+  double* x;
+  double* r;
+  const double* p;
+  const double* v;
+  const double* J;
+  BatchArgs a;
+  double sg;
+  __device__ bool prepare() { return true; }
+  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
+  __device__ void begin_tile(long t) { sg = a.sigma[a.sys_of(t)]; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const {
+    g.x = x[i];
+    g.r = r[i];
+    g.p = __ldg(p + i);
+    g.v = __ldg(v + i);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    x[i] = dadd(g.x, dmul(sg, g.p));
+    const double ri = dadd(g.r, dmul(-sg, g.v));
+    r[i] = ri;
+    const double z = dmul(ri, g.J);
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    a.beta[s] = tot[0] / a.alpha[s];
+    a.alpha[s] = tot[0];
+    a.norm[s] = sqrt(tot[1]);
+    a.iter[s] += 1;
+    a.settle(s);
+  }
+  __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
+};
+
+// K3: p = beta p + J r
+struct BOpDirection {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { double p, r, J; };
+  double* p;
+  const double* r;
+  const double* J;
+  BatchArgs a;
+  double bt;
+  __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
+  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
+  __device__ void begin_tile(long t) { bt = a.beta[a.sys_of(t)]; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  __device__ void compute(long i, Regs& g, double*) const {
+    p[i] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
+  }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// ||b - A x|| / ||b|| per system
+struct BEpiVerify {
+  static constexpr int NRED = 1;
+  static constexpr bool kBatched = true;
+  const double* b;
+  BatchArgs a;
+  __device__ bool active() const { return true; }
+  __device__ bool tile_active(long) const { return true; }
+  __device__ void begin_tile(long) {}
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    a.vres[s] = a.bnorm[s] > 0.0 ? sqrt(tot[0]) / a.bnorm[s] : sqrt(tot[0]);
+  }
+  __device__ void finish_global() const {}
+};
+
+// ---- concatenation ------------------------------------------------------------
+
+__global__ void batch_rows_kernel(int n, int pad, const int* __restrict__ rp_s, const double* __restrict__ J_s,
+                                  int nnz_off, int nnz_s, int* __restrict__ rp_d, double* __restrict__ J_d) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < pad; i += (long)gridDim.x * blockDim.x) {
+    rp_d[i] = i <= n ? rp_s[i] + nnz_off : nnz_off + nnz_s;
+    J_d[i] = i < n ? J_s[i] : 0.0;
+  }
+}
+
+__global__ void batch_cols_kernel(long nnz, const int* __restrict__ ci_s, int row_off,
+                                  int* __restrict__ ci_d) {
+  for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < nnz; k += (long)gridDim.x * blockDim.x)
+    ci_d[k] = ci_s[k] + row_off;
+}
+
+__global__ void fill_int_kernel(long n, int v, int* __restrict__ a) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a[i] = v;
+}
+
+}  // namespace celg
+
+struct Batch {
+  std::string key;
+  int nsys = 0;
+  long N = 0, NT = 0;
+  celg::CsrDev A;
+  double* J = nullptr;
+  double *B = nullptr, *X = nullptr, *R = nullptr, *P = nullptr, *V = nullptr;
+  int* tile_arrays = nullptr;  // tile_sys[NT], sys_tile0[nsys], sys_ntiles[nsys]
+  unsigned* sys_ticket = nullptr;
+  double* dstate = nullptr;    // 7 x nsys doubles
+  int* istate = nullptr;       // 3 x nsys ints + n_active
+  int nlive = 0;               // systems with at least one row
+  std::vector<long> row_off;
+  std::vector<int> n;
+};
+
+namespace celg {
+
+void batch_free(Batch* b) {
+  if (!b) return;
+  cudaFree(b->A.rp);
+  cudaFree(b->A.ci);
+  cudaFree(b->A.v);
+  cudaFree(b->J);
+  cudaFree(b->B);
+  cudaFree(b->tile_arrays);
+  cudaFree(b->sys_ticket);
+  cudaFree(b->dstate);
+  cudaFree(b->istate);
+  delete b;
+}
+
+static int ew(celg_handle* h, long n) {
+  return (int)std::max(1L, std::min((n + 255) / 256, (long)h->sms * 16));
+}
+
+static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const std::string& key,
+                       Batch** out) {
+  Batch* bt = new Batch();
+  bt->key = key;
+  bt->nsys = count;
+  bt->row_off.resize(count);
+  bt->n.resize(count);
+  long N = 0, NNZ = 0;
+  std::vector<long> nnz_off(count);
+  for (int s = 0; s < count; ++s) {
+    bt->row_off[s] = N;
+    nnz_off[s] = NNZ;
+    bt->n[s] = mats[s]->csr.n;
+    N += ((long)mats[s]->csr.n + kTile - 1) / kTile * kTile;
+    NNZ += mats[s]->csr.nnz;
+    if (mats[s]->csr.n > 0) bt->nlive++;
+  }
+  if (N >= (1L << 31) || NNZ >= (1L << 31)) {
+    delete bt;
+    return CELG_ERR_ARG;
+  }
+  bt->N = N;
+  bt->NT = N / kTile;
+  CsrDev& A = bt->A;
+  A.n = (int)N;
+  A.nnz = (int)NNZ;
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
+  ok(cudaMalloc(&A.rp, sizeof(int) * ((size_t)N + 1 + 8)));
+  ok(cudaMalloc(&A.ci, sizeof(int) * ((size_t)NNZ + 8)));
+  ok(cudaMalloc(&A.v, sizeof(double) * ((size_t)NNZ + 8)));
+  ok(cudaMalloc(&bt->J, sizeof(double) * std::max<size_t>(N, 1)));
+  ok(cudaMalloc(&bt->B, sizeof(double) * std::max<size_t>(N, 1) * 5));
+  ok(cudaMalloc(&bt->tile_arrays, sizeof(int) * ((size_t)bt->NT + 2 * (size_t)count + 1)));
+  ok(cudaMalloc(&bt->sys_ticket, sizeof(unsigned) * (size_t)count));
+  ok(cudaMalloc(&bt->dstate, sizeof(double) * 7 * (size_t)count));
+  ok(cudaMalloc(&bt->istate, sizeof(int) * (3 * (size_t)count + 1)));
+  if (e != cudaSuccess) {
+    batch_free(bt);
+    return cuda_status(e, "batch allocation");
+  }
+  bt->X = bt->B + N;
+  bt->R = bt->X + N;
+  bt->P = bt->R + N;
+  bt->V = bt->P + N;
+  ok(cudaMemsetAsync(bt->B, 0, sizeof(double) * (size_t)N * 5, h->stream));
+  ok(cudaMemsetAsync(A.ci + NNZ, 0, sizeof(int) * 8, h->stream));
+  ok(cudaMemsetAsync(A.v + NNZ, 0, sizeof(double) * 8, h->stream));
+  ok(cudaMemsetAsync(bt->sys_ticket, 0, sizeof(unsigned) * (size_t)count, h->stream));
+  for (int s = 0; s < count && e == cudaSuccess; ++s) {
+    const celg_mat* m = mats[s];
+    const long pad = ((long)m->csr.n + kTile - 1) / kTile * kTile;
+    if (pad > 0)
+      batch_rows_kernel<<<ew(h, pad), 256, 0, h->stream>>>(m->csr.n, (int)pad, m->csr.rp, m->jacobi,
+                                                           (int)nnz_off[s], m->csr.nnz,
+                                                           A.rp + bt->row_off[s], bt->J + bt->row_off[s]);
+    if (m->csr.nnz > 0) {
+      batch_cols_kernel<<<ew(h, m->csr.nnz), 256, 0, h->stream>>>(m->csr.nnz, m->csr.ci,
+                                                                 (int)bt->row_off[s], A.ci + nnz_off[s]);
+      ok(cudaMemcpyAsync(A.v + nnz_off[s], m->csr.v, sizeof(double) * (size_t)m->csr.nnz,
+                         cudaMemcpyDeviceToDevice, h->stream));
+    }
+    ok(cudaGetLastError());
+  }
+  fill_int_kernel<<<1, 32, 0, h->stream>>>(9, (int)NNZ, A.rp + N);  // rp[N] and the padded tail
+  std::vector<int> tiles((size_t)bt->NT + 2 * (size_t)count);
+  long t = 0;
+  for (int s = 0; s < count; ++s) {
+    const long nt = ((long)mats[s]->csr.n + kTile - 1) / kTile;
+    tiles[(size_t)bt->NT + s] = (int)t;
+    tiles[(size_t)bt->NT + count + s] = (int)nt;
+    for (long k = 0; k < nt; ++k) tiles[(size_t)(t + k)] = s;
+    t += nt;
+  }
+  ok(cudaMemcpyAsync(bt->tile_arrays, tiles.data(), sizeof(int) * tiles.size(), cudaMemcpyHostToDevice,
+                     h->stream));
+  ok(cudaStreamSynchronize(h->stream));
+  if (e != cudaSuccess) {
+    batch_free(bt);
+    return cuda_status(e, "batch assembly");
+  }
+  int st = csr_compute_cap(h, A);
+  if (st) {
+    batch_free(bt);
+    return st;
+  }
+  *out = bt;
+  return CELG_OK;
+}
+
+static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle cond, const int* errw) {
+  BatchArgs a;
+  const int c = bt->nsys;
+  a.alpha = bt->dstate;
+  a.sigma = a.alpha + c;
+  a.beta = a.sigma + c;
+  a.norm = a.beta + c;
+  a.bnorm = a.norm + c;
+  a.eps = a.bnorm + c;
+  a.vres = a.eps + c;
+  a.iter = bt->istate;
+  a.active = a.iter + c;
+  a.err = a.active + c;
+  a.n_active = a.err + c;
+  a.br.tile_sys = bt->tile_arrays;
+  a.br.sys_tile0 = bt->tile_arrays + bt->NT;
+  a.br.sys_ntiles = bt->tile_arrays + bt->NT + c;
+  a.br.sys_ticket = bt->sys_ticket;
+  a.nsys = c;
+  a.nlive = bt->nlive;
+  a.iter_max = iter_max;
+  a.cond = cond;
+  a.errw = errw;
+  return a;
+}
+
+static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
+                          const celg_params* p, BatchArgs a) {
+  const long N = bt->N;
+  for (int s = 0; s < bt->nsys; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(bt->B + bt->row_off[s], b_d[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+    if (p->x0_mode == CELG_X0_USER)
+      CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
+                                cudaMemcpyDeviceToDevice, h->stream));
+  }
+  int st = launch_tile(h, N, BOpPre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a});
+  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiInit{bt->B, bt->R, bt->P, bt->J, a});
+  if (!st)
+    st = capture_while(h, a.cond, [&]() -> int {
+      int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, BEpiAp{bt->V, bt->P, a});
+      if (!s2) s2 = launch_tile(h, N, BOpUpdate{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0});
+      if (!s2) s2 = launch_tile(h, N, BOpDirection{bt->P, bt->R, bt->J, a, 0.0});
+      return s2;
+    });
+  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiVerify{bt->B, a});
+  if (st) return st;
+  for (int s = 0; s < bt->nsys; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(x_d[s], bt->X + bt->row_off[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return CELG_OK;
+}
+
+int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                double* const* x_d, const celg_params* p, celg_result* res) {
+  std::string mkey = "batch";
+  char buf[64];
+  for (int s = 0; s < count; ++s) {
+    if (!mats[s] || !mats[s]->jacobi || mats[s]->h != h) return CELG_ERR_ARG;
+    if (mats[s]->csr.n > 0 && (!b_d[s] || !x_d[s])) return CELG_ERR_ARG;
+    std::snprintf(buf, sizeof(buf), "|%p", (const void*)mats[s]);
+    mkey += buf;
+  }
+  Batch* bt = h->batch;
+  if (!bt || bt->key != mkey) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    batch_free(h->batch);
+    h->batch = nullptr;
+    int st = batch_build(h, count, mats, mkey, &bt);
+    if (st) return st;
+    h->batch = bt;
+  }
+  int st = ensure_partials(h, bt->NT, 2);
+  if (st) return st;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  std::string gkey = mkey;
+  for (int s = 0; s < count; ++s) {
+    std::snprintf(buf, sizeof(buf), "|%p|%p", (const void*)b_d[s], (const void*)x_d[s]);
+    gkey += buf;
+  }
+  std::snprintf(buf, sizeof(buf), "|%d|%.17g|%.17g|%d", p->x0_mode, p->eps_abs, p->eps_rel, p->iter_max);
+  gkey += buf;
+  GraphEntry* ge = graph_cache_find(h, gkey);
+  if (!ge) {
+    st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
+      return record_batched(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, cond, h->err_d));
+    }, &ge);
+    if (st) return st;
+  }
+  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  std::vector<double> ds(7 * (size_t)count);
+  std::vector<int> is(3 * (size_t)count + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), bt->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), bt->istate, sizeof(int) * is.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, iters = 0;
+  for (int s = 0; s < count; ++s) {
+    const double alpha = ds[(size_t)s], norm = ds[3 * (size_t)count + s];
+    const double eps = ds[5 * (size_t)count + s];
+    const int it = is[(size_t)s], err = is[2 * (size_t)count + s];
+    int rs = CELG_OK;
+    if (bt->n[s] == 0) {
+      if (res) {
+        std::memset(&res[s], 0, offsetof(celg_result, history));
+        res[s].history_len = 0;
+      }
+      continue;
+    }
+    if (err) rs = err;
+    else if (!(norm <= eps) && it >= p->iter_max && std::fabs(alpha) > kRealSmall) rs = CELG_ERR_NOCONV;
+    if (rs && !ret) ret = rs;
+    iters = std::max(iters, it);
+    if (res) {
+      res[s].iter_done = it;
+      res[s].final_norm2 = norm;
+      res[s].bnorm = ds[4 * (size_t)count + s];
+      res[s].verified_relres = ds[6 * (size_t)count + s];
+      res[s].err = rs;
+      res[s].arnoldi_steps = 0;
+      res[s].history_len = 0;
+    }
+  }
+  h->last_iters = iters;
+  return ret;
+}
+
+}  // namespace celg
+
+extern "C" int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats,
+                                const double* const* b_d, double* const* x_d, const celg_params* p,
+                                celg_result* res) {
+  if (!h || count <= 0 || !mats || !b_d || !x_d || !p) return CELG_ERR_ARG;
+  if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(h->device));
+  return celg::pcg_batched(h, count, mats, b_d, x_d, p, res);
+}

@@ -13,6 +13,8 @@
 //     j+256, ... then butterfly and warp order) by the last CTA to finish.
 #pragma once
 #include <cstdint>
+#include <type_traits>
+
 #include <cuda_runtime.h>
 
 namespace celg {
@@ -173,6 +175,80 @@ __device__ __forceinline__ bool grid_finish(const RedCtx& red, double (&tot)[NRE
   }
   if (tid == 0) *red.ticket = 0u;
   return tid == 0;
+}
+
+// ---- batched solves --------------------------------------------------------
+//
+// An epilogue/op with `static constexpr bool kBatched = true` runs over the
+// concatenated rows of many systems (each padded to whole tiles).  It provides
+//   bool tile_active(long t)      skip the tiles of finished systems
+//   void begin_tile(long t)       load the tile's system scalars
+//   void finish_sys(int s, tot)   per-system scalars (lane 0 of the CTA that
+//                                 completed the system's last tile)
+//   void finish_global()          lane 0 of the last CTA of the kernel
+//   const BatchRed& bred()
+// Each system's partials are reduced in the same order as a single solve.
+struct BatchRed {
+  const int* tile_sys;    // system of each tile
+  const int* sys_tile0;  // first tile of each system
+  const int* sys_ntiles;  // tiles of each system
+  unsigned* sys_ticket;   // per-system completion tickets (reset by the finisher)
+};
+
+template <class T, class = void>
+struct is_batched : std::false_type {};
+template <class T>
+struct is_batched<T, std::void_t<decltype(T::kBatched)>> : std::integral_constant<bool, T::kBatched> {};
+
+// After lane 0 wrote tile t's partials: count the tile for its system; the
+// CTA that completes the system reduces its partials and calls finish_sys.
+template <int NRED, class Epi>
+__device__ __forceinline__ void batch_tile_done(const RedCtx& red, Epi& epi, long t,
+                                                double* scratch, int* s_flag, int tid,
+                                                int bar_id) {
+  const BatchRed& br = epi.bred();
+  const int s = br.tile_sys[t];
+  if (tid == 0) {
+    __threadfence();
+    const unsigned tk = atomicAdd(&br.sys_ticket[s], 1u);
+    *s_flag = (tk == (unsigned)br.sys_ntiles[s] - 1u) ? 1 : 0;
+  }
+  named_bar_sync(bar_id, kLanes);
+  if (*s_flag) {
+    __threadfence();
+    double tot[NRED];
+    const long t0 = br.sys_tile0[s];
+    const long nt = br.sys_ntiles[s];
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) {
+      double acc = 0.0;
+      const double* p = red.partials + (long)r * red.ntiles + t0;
+      for (long k = tid; k < nt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
+      tot[r] = group_fold256(acc, scratch, tid, bar_id);
+    }
+    if (tid == 0) {
+      epi.finish_sys(s, tot);
+      br.sys_ticket[s] = 0u;
+    }
+  }
+  named_bar_sync(bar_id, kLanes);
+}
+
+// All CTAs arrive once; lane 0 of the last one calls finish_global.
+template <class Epi>
+__device__ __forceinline__ void batch_grid_done(const RedCtx& red, Epi& epi, int* s_flag, int tid,
+                                                int bar_id) {
+  if (tid == 0) {
+    __threadfence();
+    const unsigned tk = atomicAdd(red.ticket, 1u);
+    *s_flag = (tk == gridDim.x - 1) ? 1 : 0;
+  }
+  named_bar_sync(bar_id, kLanes);
+  if (*s_flag && tid == 0) {
+    __threadfence();
+    epi.finish_global();
+    *red.ticket = 0u;
+  }
 }
 
 }  // namespace celg

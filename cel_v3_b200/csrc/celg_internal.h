@@ -80,6 +80,8 @@ struct celg_handle {
   size_t ircap = 0;
   // ELM assembly state
   struct Elm* elm = nullptr;
+  // concatenated systems of the last batched solve
+  struct Batch* batch = nullptr;
   // last solve timing
   float last_ms = 0.f;
   int last_iters = 0;
@@ -144,5 +146,6 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
              celg_result* res);
 int ensure_f32(celg_handle* h, size_t n);
+void batch_free(::Batch* b);
 
 }  // namespace celg

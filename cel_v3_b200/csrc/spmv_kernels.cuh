@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(kCsrThreads, 2)
                    const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
                    RedCtx red, int* err) {
   constexpr int NR = Epi::NRED;
+  constexpr bool kB = is_batched<Epi>::value;
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kStages;
@@ -80,6 +81,9 @@ __global__ void __launch_bounds__(kCsrThreads, 2)
       const long tn = t + gridDim.x;
       if (tn < ntiles && lane <= kSubPerTile)
         bnd = __ldg(rp + min(tn * kTile + (long)lane * kSub, (long)n));
+      if constexpr (kB) {
+        if (!epi.tile_active(t)) continue;
+      }
       for (int q = 0; q < kSubPerTile; ++q) {
         const long s = t * kSubPerTile + q;
         if (s >= nsub) break;
@@ -122,7 +126,12 @@ __global__ void __launch_bounds__(kCsrThreads, 2)
   // ---------------- consumer warps (256 threads, lane j = row in sub-tile) ----
   const int j = threadIdx.x;
   int it = 0;
+  Epi ep = epi;
   for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if constexpr (kB) {
+      if (!ep.tile_active(t)) continue;
+      ep.begin_tile(t);
+    }
     Acc<NR> acc;
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
@@ -142,23 +151,26 @@ __global__ void __launch_bounds__(kCsrThreads, 2)
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
         if (!fb) {
-          int k = b - a0;
-          const int ke = e - a0;
-          for (; k + 4 <= ke; k += 4) {
-            const int c0 = cis[k], c1 = cis[k + 1], c2 = cis[k + 2], c3 = cis[k + 3];
-            const VT v0 = vs[k], v1 = vs[k + 1], v2 = vs[k + 2], v3 = vs[k + 3];
-            const VT x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2),
-                     x3 = __ldg(x + c3);
-            sum = vadd(sum, vmul(v0, x0));
-            sum = vadd(sum, vmul(v1, x1));
-            sum = vadd(sum, vmul(v2, x2));
-            sum = vadd(sum, vmul(v3, x3));
+          // chunks of 8 entries: all gathers of a chunk are issued before the
+          // first add, so a row of up to 8 entries costs one memory round trip;
+          // the adds stay in stored order
+          for (int k = b - a0, ke = e - a0; k < ke; k += 8) {
+            VT xv[8], vv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              if (k + u < ke) {
+                vv[u] = vs[k + u];
+                xv[u] = __ldg(x + cis[k + u]);
+              }
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (k + u < ke) sum = vadd(sum, vmul(vv[u], xv[u]));
           }
-          for (; k < ke; ++k) sum = vadd(sum, vmul(vs[k], __ldg(x + cis[k])));
         } else {
           for (int k = b; k < e; ++k) sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + __ldg(ci + k))));
         }
-        epi.row(row, sum, acc.a);
+        ep.row(row, sum, acc.a);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
@@ -170,11 +182,14 @@ __global__ void __launch_bounds__(kCsrThreads, 2)
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
         if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
       }
+      if constexpr (kB) batch_tile_done<(NR > 0 ? NR : 1)>(red, ep, t, scratch, s_flag, j, 1);
     }
   }
-  if (NR > 0) {
+  if constexpr (kB) {
+    batch_grid_done(red, ep, s_flag, j, 1);
+  } else if (NR > 0) {
     double tot[NR > 0 ? NR : 1];
-    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) epi.finish(tot);
+    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);
   }
 }
 

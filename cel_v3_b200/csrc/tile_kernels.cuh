@@ -22,6 +22,7 @@ namespace celg {
 template <class Op>
 __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx red) {
   constexpr int NR = Op::NRED;
+  constexpr bool kB = is_batched<Op>::value;
   __shared__ double scratch[8];
   __shared__ int s_flag;
   Op op = op_in;
@@ -29,6 +30,10 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   const int j = threadIdx.x;
   const long ntiles = (n + kTile - 1) / kTile;
   for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    if constexpr (kB) {
+      if (!op.tile_active(t)) continue;
+      op.begin_tile(t);
+    }
     Acc<NR> acc;
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
@@ -46,9 +51,12 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
         if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
       }
+      if constexpr (kB) batch_tile_done<(NR > 0 ? NR : 1)>(red, op, t, scratch, &s_flag, j, 1);
     }
   }
-  if (NR > 0) {
+  if constexpr (kB) {
+    batch_grid_done(red, op, &s_flag, j, 1);
+  } else if (NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, &s_flag, j, 1)) op.finish(tot);
   }

@@ -173,6 +173,18 @@ int celg_gmres_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_
 int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_host,
                     double* x_host, const celg_params* p, celg_result* res);
 
+/* ---- batched form -------------------------------------------------------------- */
+/* Jacobi-PCG on `count` independent systems of uneven size in one device-driven
+ * loop (one CUDA graph launch for the whole batch).  mats[k] must have Jacobi
+ * set; b_d[k], x_d[k] are device vectors of mats[k]'s size.  p applies to every
+ * system (eps_rel relative to each system's own ||b||).  res (count entries,
+ * nullable) receives the per-system reports; history is not recorded.  Each
+ * system's result is bit-identical to celg_pcg_jacobi on it alone.  The
+ * concatenated copy of the matrices is cached on the handle until another
+ * batch or a celg_mat_destroy. */
+int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                     double* const* x_d, const celg_params* p, celg_result* res);
+
 /* ---- allocation-free entry point ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (their device memory belongs to their own pool or to another

@@ -1,0 +1,75 @@
+"""Batched Jacobi-PCG (celg_pcg_batched): every system of the batch must give
+the same bits as solving it alone with celg_pcg_jacobi (same reduction order
+per system), whatever the mix of sizes, including systems whose row count is
+not a multiple of the 1024-row tile and an empty one."""
+import numpy as np
+import pytest
+
+from cel_v3_b200 import synth
+from oracle import celref as R
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def systems():
+    rng = np.random.default_rng(4)
+    out = []
+    for side in (16, 5, 23, 31, 9, 40, 12):
+        _, (kx, ky, kz) = synth.lognormal_faces(rng, side, side + 1, side, 0.5)
+        rp, ci, v = synth.diffusion7(side, side + 1, side, kx, ky, kz)
+        out.append((rp, ci, v, rng.uniform(-1.0, 1.0, rp.size - 1)))
+    return out
+
+
+@pytest.mark.parametrize("x0", ["zero", "ones"])
+def test_batched_matches_single_solves_bitwise(gpu, x0):
+    celgpu, h, torch = gpu
+    sy = systems()
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+    bs = [dev(torch, b) for *_, b in sy]
+    xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    mode = celgpu.X0_ZERO if x0 == "zero" else celgpu.X0_REF_ONES
+    kw = dict(eps_rel=1e-9, iter_max=3000, x0_mode=mode)
+    infos = h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], **kw)
+    for s, ((rp, ci, v, b), m) in enumerate(zip(sy, mats)):
+        xo = dev(torch, np.zeros(b.size))
+        one = h.pcg_jacobi(m, bs[s].data_ptr(), xo.data_ptr(), **kw)
+        assert infos[s].status == celgpu.OK and one.status == celgpu.OK
+        assert infos[s].iter_done == one.iter_done
+        assert infos[s].final_norm2 == one.final_norm2
+        assert infos[s].verified_relres == one.verified_relres
+        assert np.array_equal(xs[s].cpu().numpy(), xo.cpu().numpy())
+    # and against the oracle in tree order for one of them
+    rp, ci, v, b = sy[3]
+    xr, ir = R.pcg_jacobi(R.Matrix(rp, ci, v), R.jacobi(R.diag(rp, ci, v)), b, eps_rel=1e-9,
+                          iter_max=3000, red=R.RED_TREE,
+                          x0_mode=R.X0_ZERO if x0 == "zero" else R.X0_ONES)
+    assert np.array_equal(xs[3].cpu().numpy(), xr) and ir["iter_done"] == infos[3].iter_done
+    # a second launch of the cached batch graph gives the same bits
+    xs2 = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    infos2 = h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs2], **kw)
+    for s in range(len(sy)):
+        assert np.array_equal(xs2[s].cpu().numpy(), xs[s].cpu().numpy())
+        assert infos2[s].iter_done == infos[s].iter_done
+    for m in mats:
+        m.destroy()
+
+
+def test_batched_with_empty_system_and_cap(gpu):
+    celgpu, h, torch = gpu
+    sy = systems()[:3]
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+    empty = h.matrix_from_csr(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)).jacobi()
+    bs = [dev(torch, b) for *_, b in sy]
+    xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    infos = h.pcg_batched(mats + [empty], [b.data_ptr() for b in bs] + [0],
+                          [x.data_ptr() for x in xs] + [0], eps_rel=1e-12, iter_max=5)
+    for s in range(3):
+        assert infos[s].iter_done == 5 and infos[s].status == celgpu.ERR_NOCONV
+    assert infos[3].iter_done == 0 and infos[3].status == celgpu.OK
+    for m in mats + [empty]:
+        m.destroy()
