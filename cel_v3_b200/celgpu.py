@@ -125,6 +125,8 @@ def _load():
         "celg_elm_destroy": (i, [vp]),
         "celg_dot_noalloc": (i, [i, vp, vp, vp, vp]),
         "celg_pcg_batched": (i, [vp, i, vp, vp, vp, ctypes.POINTER(Params), vp]),
+        "celg_check_bounded_wait": (i, [vp, i, ip]),
+        "celg_pcg_multirhs": (i, [vp, vp, i, vp, vp, ctypes.POINTER(Params), vp]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -388,6 +390,23 @@ class Handle:
         st = lib.celg_pcg_batched(self.ptr, k, M, B, X, ctypes.byref(p), res)
         _check(st, "celg_pcg_batched", allow=(ERR_NOCONV, ERR_BREAKDOWN))
         return [_info(r, None, r.err) for r in res]
+
+    def pcg_multirhs(self, mat, k, B_d, X_d, p=None, **kw):
+        """Jacobi-PCG on k right-hand sides (n x k row-major device arrays);
+        returns a list of per-column SolveInfo."""
+        p = p or params(**kw)
+        res = (Result * k)()
+        st = lib.celg_pcg_multirhs(self.ptr, mat.ptr, int(k), ctypes.c_void_p(B_d),
+                                   ctypes.c_void_p(X_d), ctypes.byref(p), res)
+        _check(st, "celg_pcg_multirhs", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return [_info(r, None, r.err) for r in res]
+
+    def check_bounded_wait(self, limit_ms=200):
+        """Status reported by a bounded device wait that is never satisfied."""
+        s = ctypes.c_int()
+        _check(lib.celg_check_bounded_wait(self.ptr, int(limit_ms), ctypes.byref(s)),
+               "celg_check_bounded_wait")
+        return s.value
 
     def solve_host(self, mat, b, x=None, solver=SOLVER_PCG, p=None, **kw):
         """Solve from host arrays (the copies are part of the call)."""

@@ -289,6 +289,8 @@ extern "C" int celg_destroy(celg_handle* h) {
   if (h->elm) celg_elm_destroy(h);
   batch_free(h->batch);
   h->batch = nullptr;
+  multi_free(h->multi);
+  h->multi = nullptr;
   graph_cache_clear(h);
   cudaFree(h->partials);
   cudaFree(h->sb);

@@ -82,6 +82,8 @@ struct celg_handle {
   struct Elm* elm = nullptr;
   // concatenated systems of the last batched solve
   struct Batch* batch = nullptr;
+  // work vectors and per-column state of multi-right-hand-side solves
+  struct Multi* multi = nullptr;
   // last solve timing
   float last_ms = 0.f;
   int last_iters = 0;
@@ -147,5 +149,6 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
              celg_result* res);
 int ensure_f32(celg_handle* h, size_t n);
 void batch_free(::Batch* b);
+void multi_free(::Multi* m);
 
 }  // namespace celg

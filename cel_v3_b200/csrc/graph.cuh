@@ -59,6 +59,53 @@ int capture_while(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
   return CELG_OK;
 }
 
+// Create a conditional handle on the graph being captured on h->stream
+// (used for an IF node inside a loop body).
+inline int capture_new_handle(celg_handle* h, unsigned default_value, cudaGraphConditionalHandle* out) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g;
+  CELG_CUDA(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &g, nullptr, nullptr));
+  CELG_CUDA(cudaGraphConditionalHandleCreate(out, g, default_value, cudaGraphCondAssignDefault));
+  return CELG_OK;
+}
+
+// Append an IF conditional node after the work captured so far on h->stream;
+// `body` records the work it guards.
+template <class Body>
+int capture_if(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cap_graph;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  CELG_CUDA(cudaStreamGetCaptureInfo(h->stream, &cs, nullptr, &cap_graph, &deps, &ndeps));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cnode;
+  CELG_CUDA(cudaGraphAddNode(&cnode, cap_graph, deps, ndeps, &cp));
+  cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+  CELG_CUDA(cudaStreamUpdateCaptureDependencies(h->stream, &cnode, 1,
+                                                cudaStreamSetCaptureDependencies));
+  cudaStream_t side;
+  CELG_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  cudaError_t e = cudaStreamBeginCaptureToGraph(side, bodyg, nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeRelaxed);
+  int st = CELG_OK;
+  if (e == cudaSuccess) {
+    cudaStream_t main_stream = h->stream;
+    h->stream = side;
+    st = body();
+    h->stream = main_stream;
+    cudaGraph_t out;
+    e = cudaStreamEndCapture(side, &out);
+  }
+  cudaStreamDestroy(side);
+  if (st) return st;
+  CELG_CUDA(e);
+  return CELG_OK;
+}
+
 // Capture `record(cond)` on the handle's private capture stream (the caller's
 // stream may be the legacy default stream, which cannot be captured),
 // instantiate it and add it to the cache under `key`.

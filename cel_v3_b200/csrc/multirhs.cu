@@ -1,0 +1,512 @@
+// multirhs.cu -- Jacobi-PCG on k <= 32 right-hand sides that share one matrix
+// (block SpMM-driven PCG): B and X are n x k row-major, every column runs its
+// own PCG recurrence (own alpha, sigma, beta, ||r||, iteration count), and
+// each iteration reads the matrix once for all k columns.
+//
+// Thread mapping: a 256-thread CTA works on 1024-row tiles; warp w handles
+// rows t*1024 + q*256 + w*32 + r (q = 0..3, r = 0..31) and lane c handles
+// column c, so a warp reads the k values of a row of X (k*8 contiguous bytes)
+// per non-zero.  Row sums run over the stored entries in order with separate
+// multiply/add roundings (each column's SpMV equals the single-vector SpMV).
+//
+// Reduction order (per column c; mirrored by the test-suite's oracle
+// composition): warp w sums its 128 rows of the tile in (q, r) order from
+// 0.0; the tile partial is warp 0 + warp 1 + ... + warp 7; the tile partials
+// are reduced with the single-vector order (lane j sums j, j+256, ...,
+// butterfly, warps in order).
+//
+// Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 104 n k.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "graph.cuh"
+#include "pcg_internal.cuh"
+
+namespace celg {
+
+constexpr int kMaxRhs = 32;
+
+struct MultiArgs {
+  double *alpha, *sigma, *beta, *norm, *bnorm, *eps, *vres;
+  int *iter, *active, *err, *n_active;
+  int k;
+  int iter_max;
+  cudaGraphConditionalHandle cond;
+  const int* errw;
+  __device__ int go(int c) const {
+    return (err[c] == 0 && *(volatile const int*)errw == 0 && iter[c] < iter_max &&
+            fabs(alpha[c]) > kRealSmall && norm[c] > eps[c])
+               ? 1
+               : 0;
+  }
+  __device__ void settle(int c) const {
+    const int g = go(c);
+    active[c] = g;
+    if (!g) atomicSub(n_active, 1);
+  }
+};
+
+// Per-column tile partials: after the warps accumulated their 128 rows,
+// combine warps in order and store partials[(r*k + c)*ntiles + t].
+template <int NRED>
+__device__ __forceinline__ void multi_tile_store(double (&acc)[NRED], double* s_w, int k, long t,
+                                                 long ntiles, double* partials, int warp, int lane) {
+  // s_w: [NRED][8][32]
+#pragma unroll
+  for (int r = 0; r < NRED; ++r) s_w[(r * 8 + warp) * 32 + lane] = acc[r];
+  named_bar_sync(1, kLanes);
+  if (threadIdx.x < NRED * 32) {
+    const int r = threadIdx.x / 32, c = threadIdx.x % 32;
+    if (c < k) {
+      double tot = s_w[(r * 8 + 0) * 32 + c];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) tot = dadd(tot, s_w[(r * 8 + w) * 32 + c]);
+      partials[((long)r * k + c) * ntiles + t] = tot;
+    }
+  }
+  named_bar_sync(1, kLanes);
+}
+
+// Last CTA: per (reduction, column) the single-vector tile reduction; then
+// op.finish_col(c, tot[]) for every column and op.finish_global().
+template <int NRED, class Op>
+__device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& op, int k,
+                                                  double* scratch, int* s_flag, double* s_tot) {
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned tk = atomicAdd(red.ticket, 1u);
+    *s_flag = (tk == gridDim.x - 1) ? 1 : 0;
+  }
+  named_bar_sync(1, kLanes);
+  if (!*s_flag) return;
+  __threadfence();
+  for (int rc = 0; rc < NRED * k; ++rc) {
+    const double* p = red.partials + (long)rc * red.ntiles;
+    double s = 0.0;
+    for (long q = tid; q < red.ntiles; q += kLanes) s = dadd(s, __ldcg(p + q));
+    const double tot = group_fold256(s, scratch, tid, 1);
+    if (tid == 0) s_tot[rc] = tot;
+  }
+  named_bar_sync(1, kLanes);
+  if (tid < k) {
+    double tot[NRED];
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) tot[r] = s_tot[r * k + tid];
+    op.finish_col(tid, tot);
+  }
+  named_bar_sync(1, kLanes);
+  if (tid == 0) {
+    op.finish_global();
+    *red.ticket = 0u;
+  }
+}
+
+// ---- SpMM with a fused per-row epilogue (matrix read straight from global:
+// the k-wide gathers dominate the traffic, the matrix is 12 nnz bytes) ------
+template <class Epi>
+__global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp,
+                                                      const int* __restrict__ ci,
+                                                      const double* __restrict__ v, int n, int k,
+                                                      const double* __restrict__ X, Epi epi,
+                                                      RedCtx red) {
+  constexpr int NR = Epi::NRED;
+  __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[(NR > 0 ? NR : 1) * kMaxRhs];
+  __shared__ int s_flag;
+  if (!epi.active()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool on = lane < k && epi.col_active(lane);
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      for (int r = 0; r < 32; ++r) {
+        const long row = t * kTile + q * kSub + warp * 32 + r;
+        if (row >= n) break;
+        const int b = __ldg(rp + row), e = __ldg(rp + row + 1);
+        double sum = 0.0;
+        for (int kk = b; kk < e; kk += 8) {
+          double xv[8], vv[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            if (kk + u < e) {
+              vv[u] = __ldg(v + kk + u);
+              const int c = __ldg(ci + kk + u);
+              xv[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (kk + u < e) sum = dadd(sum, dmul(vv[u], xv[u]));
+        }
+        if (on) epi.row(row, lane, sum, acc);
+      }
+    }
+    if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<(NR > 0 ? NR : 1)>(red, epi, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
+}
+
+// ---- n x k vector sweeps with per-column scalars ------------------------------
+template <class Op>
+__global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, RedCtx red) {
+  constexpr int NR = Op::NRED;
+  __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[(NR > 0 ? NR : 1) * kMaxRhs];
+  __shared__ int s_flag;
+  Op op = op_in;
+  if (!op.prepare()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool on = lane < k && op.col_active(lane);
+  op.begin_col(lane < k ? lane : 0);
+  const long ntiles = (n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      for (int r4 = 0; r4 < 32; r4 += 4) {
+        typename Op::Regs g[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (on && row0 + r4 + u < n) op.load((row0 + r4 + u) * k + lane, row0 + r4 + u, g[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (on && row0 + r4 + u < n) op.compute((row0 + r4 + u) * k + lane, row0 + r4 + u, g[u], acc);
+      }
+    }
+    if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<(NR > 0 ? NR : 1)>(red, op, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, op, 0, scratch, &s_flag, s_tot);
+}
+
+// ---- the sweeps of the multi-column PCG ------------------------------------------
+
+// x0 and ||b|| per column
+struct MOpPre {
+  static constexpr int NRED = 1;
+  struct Regs { double b; };
+  const double* B;
+  double* X;
+  int x0_mode;
+  double eps_abs, eps_rel;
+  MultiArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ bool col_active(int) const { return true; }
+  __device__ void begin_col(int) {}
+  __device__ void load(long e, long, Regs& g) const { g.b = __ldg(B + e); }
+  __device__ void compute(long e, long, Regs& g, double* acc) const {
+    if (x0_mode == CELG_X0_REF_ONES) X[e] = 1.0;
+    else if (x0_mode == CELG_X0_ZERO) X[e] = 0.0;
+    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    a.bnorm[c] = sqrt(tot[0]);
+    double e = eps_abs;
+    if (eps_rel > 0.0 && eps_rel * a.bnorm[c] > e) e = eps_rel * a.bnorm[c];
+    a.eps[c] = e;
+    a.err[c] = 0;
+    a.iter[c] = 0;
+    a.active[c] = 1;
+    a.vres[c] = 0.0;
+  }
+  __device__ void finish_global() const { *a.n_active = a.k; }
+};
+
+// r = b - (0 + A x); p = J r; alpha = r.p; ||r||
+struct MEpiInit {
+  static constexpr int NRED = 2;
+  const double* B;
+  double* R;
+  double* P;
+  const double* J;
+  int k;
+  MultiArgs a;
+  __device__ bool active() const { return true; }
+  __device__ bool col_active(int) const { return true; }
+  __device__ void row(long i, int c, double s, double* acc) const {
+    const long e = i * k + c;
+    const double ri = __dsub_rn(B[e], dadd(0.0, s));
+    R[e] = ri;
+    const double z = dmul(ri, __ldg(J + i));
+    P[e] = z;
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    a.alpha[c] = tot[0];
+    a.norm[c] = sqrt(tot[1]);
+    a.iter[c] = 0;
+    a.settle(c);
+  }
+  __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
+};
+
+// K1: v = 0 + A p; pv per column; sigma = alpha / pv
+struct MEpiAp {
+  static constexpr int NRED = 1;
+  double* V;
+  const double* P;
+  int k;
+  MultiArgs a;
+  __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
+  __device__ void row(long i, int c, double s, double* acc) const {
+    const long e = i * k + c;
+    const double vi = dadd(0.0, s);
+    V[e] = vi;
+    acc[0] = dadd(acc[0], dmul(vi, __ldg(P + e)));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    if (!a.active[c]) return;
+    const double sg = a.alpha[c] / tot[0];
+    a.sigma[c] = sg;
+    if (!isfinite(sg)) {
+      a.err[c] = kErrBreakdown;
+      a.active[c] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {}
+};
+
+// K2: x += sigma p; r += (-sigma) v; rz, rr; per-column scalars and test
+struct MOpUpdate {
+  static constexpr int NRED = 2;
+  struct Regs { double x, r, p, v, J; };
+  double* X;
+  double* R;
+  const double* P;
+  const double* V;
+  const double* J;
+  MultiArgs a;
+  double sg;
+  __device__ bool prepare() { return true; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
+  __device__ void begin_col(int c) { sg = a.sigma[c]; }
+  __device__ void load(long e, long i, Regs& g) const {
+    g.x = X[e];
+    g.r = R[e];
+    g.p = __ldg(P + e);
+    g.v = __ldg(V + e);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long e, long, Regs& g, double* acc) const {
+    X[e] = dadd(g.x, dmul(sg, g.p));
+    const double ri = dadd(g.r, dmul(-sg, g.v));
+    R[e] = ri;
+    const double z = dmul(ri, g.J);
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    if (!a.active[c]) return;
+    a.beta[c] = tot[0] / a.alpha[c];
+    a.alpha[c] = tot[0];
+    a.norm[c] = sqrt(tot[1]);
+    a.iter[c] += 1;
+    a.settle(c);
+  }
+  __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
+};
+
+// K3: p = beta p + J r
+struct MOpDirection {
+  static constexpr int NRED = 0;
+  struct Regs { double p, r, J; };
+  double* P;
+  const double* R;
+  const double* J;
+  MultiArgs a;
+  double bt;
+  __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
+  __device__ void begin_col(int c) { bt = a.beta[c]; }
+  __device__ void load(long e, long i, Regs& g) const { g.p = P[e]; g.r = __ldg(R + e); g.J = __ldg(J + i); }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    P[e] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// ||b - A x|| / ||b|| per column
+struct MEpiVerify {
+  static constexpr int NRED = 1;
+  const double* B;
+  int k;
+  MultiArgs a;
+  __device__ bool active() const { return true; }
+  __device__ bool col_active(int) const { return true; }
+  __device__ void row(long i, int c, double s, double* acc) const {
+    const double ri = __dsub_rn(B[i * k + c], dadd(0.0, s));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    a.vres[c] = a.bnorm[c] > 0.0 ? sqrt(tot[0]) / a.bnorm[c] : sqrt(tot[0]);
+  }
+  __device__ void finish_global() const {}
+};
+
+template <class Epi>
+static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{h->partials, h->ticket, nt};
+  if (A.n == 0) return CELG_OK;
+  const int grid = grid_for_tiles(h, nt, 8);
+  spmm_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+template <class Op>
+static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
+  const long nt = ntiles_of(n);
+  RedCtx red{h->partials, h->ticket, nt};
+  const int grid = grid_for_tiles(h, nt, 8);
+  mtile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+}  // namespace celg
+
+struct Multi {
+  size_t cap = 0;        // n*k of the work vectors
+  double* work = nullptr;  // R, P, V
+  double* dstate = nullptr;
+  int* istate = nullptr;
+};
+
+namespace celg {
+
+void multi_free(Multi* m) {
+  if (!m) return;
+  cudaFree(m->work);
+  cudaFree(m->dstate);
+  cudaFree(m->istate);
+  delete m;
+}
+
+int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
+                 const celg_params* p, celg_result* res) {
+  const long n = m->csr.n;
+  const size_t nk = (size_t)n * (size_t)k;
+  if (!h->multi) h->multi = new Multi();
+  Multi* mu = h->multi;
+  if (nk > mu->cap || !mu->work) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->work);
+    mu->work = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
+    mu->cap = nk;
+  }
+  if (!mu->dstate) {
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 1)));
+  }
+  int st = ensure_partials(h, ntiles_of(n), 2 * k);
+  if (st) return st;
+  double* R = mu->work;
+  double* P = R + nk;
+  double* V = P + nk;
+  MultiArgs a;
+  a.alpha = mu->dstate;
+  a.sigma = a.alpha + kMaxRhs;
+  a.beta = a.sigma + kMaxRhs;
+  a.norm = a.beta + kMaxRhs;
+  a.bnorm = a.norm + kMaxRhs;
+  a.eps = a.bnorm + kMaxRhs;
+  a.vres = a.eps + kMaxRhs;
+  a.iter = mu->istate;
+  a.active = a.iter + kMaxRhs;
+  a.err = a.active + kMaxRhs;
+  a.n_active = a.err + kMaxRhs;
+  a.k = k;
+  a.iter_max = p->iter_max;
+  a.errw = h->err_d;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  auto record = [&](cudaGraphConditionalHandle cond) -> int {
+    MultiArgs ac = a;
+    ac.cond = cond;
+    int s2 = launch_mtile(h, n, k, MOpPre{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
+    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit{B, R, P, m->jacobi, k, ac});
+    if (!s2)
+      s2 = capture_while(h, cond, [&]() -> int {
+        int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac});
+        if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate{X, R, P, V, m->jacobi, ac, 0.0});
+        if (!s3) s3 = launch_mtile(h, n, k, MOpDirection{P, R, m->jacobi, ac, 0.0});
+        return s3;
+      });
+    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac});
+    return s2;
+  };
+  char kb[256];
+  std::snprintf(kb, sizeof(kb), "mrhs|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%d", (const void*)m, m->csr.n, k,
+                (const void*)B, (const void*)X, (const void*)R, p->x0_mode, p->eps_abs, p->eps_rel,
+                p->iter_max);
+  const std::string key(kb);
+  GraphEntry* ge = graph_cache_find(h, key);
+  if (!ge) {
+    st = graph_build(h, key, record, &ge);
+    if (st) return st;
+  }
+  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  std::vector<double> ds(7 * kMaxRhs);
+  std::vector<int> is(3 * kMaxRhs + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), mu->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), mu->istate, sizeof(int) * is.size(), cudaMemcpyDeviceToHost, h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, iters = 0;
+  for (int c = 0; c < k; ++c) {
+    const double alpha = ds[c], norm = ds[3 * kMaxRhs + c], eps = ds[5 * kMaxRhs + c];
+    const int it = is[c], err = is[2 * kMaxRhs + c];
+    int rs = CELG_OK;
+    if (err) rs = err;
+    else if (!(norm <= eps) && it >= p->iter_max && std::fabs(alpha) > kRealSmall) rs = CELG_ERR_NOCONV;
+    if (rs && !ret) ret = rs;
+    iters = std::max(iters, it);
+    if (res) {
+      res[c].iter_done = it;
+      res[c].final_norm2 = norm;
+      res[c].bnorm = ds[4 * kMaxRhs + c];
+      res[c].verified_relres = ds[6 * kMaxRhs + c];
+      res[c].err = rs;
+      res[c].arnoldi_steps = 0;
+      res[c].history_len = 0;
+    }
+  }
+  h->last_iters = iters;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 104.0 * (double)nk;
+  return ret;
+}
+
+}  // namespace celg
+
+extern "C" int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
+                                 const celg_params* p, celg_result* res) {
+  if (!h || !m || !p || k <= 0 || k > celg::kMaxRhs || m->h != h) return CELG_ERR_ARG;
+  if (m->csr.n > 0 && (!B_d || !X_d)) return CELG_ERR_ARG;
+  if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0) return CELG_ERR_ARG;
+  if (!m->jacobi) return CELG_ERR_STATE;
+  CELG_CUDA(cudaSetDevice(h->device));
+  return celg::pcg_multirhs(h, m, k, B_d, X_d, p, res);
+}

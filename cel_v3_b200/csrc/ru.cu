@@ -46,6 +46,7 @@ struct RuArgs {
   int iter_max;
   cudaGraphConditionalHandle cond;
   const int* errw;
+  cudaGraphConditionalHandle cond_update;  // IF node guarding the reliable update (0: none)
   PcgArgs pcg() const {
     return PcgArgs{&st->s, hist, hist_cap, iter_max, cond, errw};
   }
@@ -179,6 +180,7 @@ struct OpRuStep {
     const int upd = (st->s.norm < st->delta * st->maxr) || (st->s.norm <= st->s.eps) ||
                     (st->s.iter >= a.iter_max);
     st->update = upd;
+    set_cond(a.cond_update, upd);
     if (!upd) {
       // FP32 recurrence continues; stop only on the iteration cap or an error
       const int go = (st->s.err == 0 && *(volatile const int*)a.errw == 0 &&
@@ -244,16 +246,27 @@ static int ru_setup(celg_handle* h, celg_mat* m, const double* b, double* x, con
   return st;
 }
 
+// One iteration: K1, K2, then (only when K2 asked for it) the reliable
+// update -- inside an IF conditional node when recorded into a graph, as
+// self-skipping kernels otherwise -- then K3.
 static int ru_body(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* r,
-                   float* pv, float* v, float* d) {
+                   float* pv, float* v, float* d, bool in_graph) {
   const long n = m->csr.n;
+  if (in_graph) {
+    int st = capture_new_handle(h, 0, &a.cond_update);
+    if (st) return st;
+  }
   PcgArgs pa = a.pcg();
   int st = launch_csr<float>(h, m->csr, m->csr.v32, pv, EpiAp<float>{v, pv, pa});
   if (!st) st = launch_tile(h, n, OpRuStep{d, r, pv, v, m->jacobi32, a, 0.0});
-  if (!st) st = launch_tile(h, n, OpRuFlush{x, d, a, 0});
-  if (!st)
-    st = launch_csr<double>(h, m->csr, m->csr.v, x,
-                            EpiRuResidual{b, r, nullptr, m->jacobi32, a, 0});
+  auto update = [&]() -> int {
+    int s2 = launch_tile(h, n, OpRuFlush{x, d, a, 0});
+    if (!s2)
+      s2 = launch_csr<double>(h, m->csr, m->csr.v, x,
+                              EpiRuResidual{b, r, nullptr, m->jacobi32, a, 0});
+    return s2;
+  };
+  if (!st) st = in_graph ? capture_if(h, a.cond_update, update) : update();
   if (!st) st = launch_tile(h, n, OpDirection<float>{pv, r, m->jacobi32, pa, 0.0});
   return st;
 }
@@ -296,12 +309,12 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
                 m->csr.n, (const void*)b, (const void*)x, (const void*)r, p->x0_mode, p->eps_abs,
                 p->eps_rel, p->inner_eps_rel, p->iter_max);
   const std::string key(kb);
-  RuArgs a0{sd, h->hist_d, hist_cap, p->iter_max, 0, h->err_d};
+  RuArgs a0{sd, h->hist_d, hist_cap, p->iter_max, 0, h->err_d, 0};
   if (!graphs_enabled()) {
     CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
     st = ru_setup(h, m, b, x, p, a0, r, pv, d);
     for (int it = 0; !st && it < p->iter_max; it += 8) {
-      for (int k = 0; k < 8 && !st; ++k) st = ru_body(h, m, b, x, a0, r, pv, v, d);
+      for (int k = 0; k < 8 && !st; ++k) st = ru_body(h, m, b, x, a0, r, pv, v, d, false);
       if (st) break;
       CELG_CUDA(cudaMemcpyAsync(sh, sd, sizeof(RuState), cudaMemcpyDeviceToHost, h->stream));
       CELG_CUDA(cudaStreamSynchronize(h->stream));
@@ -314,9 +327,10 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
     GraphEntry* ge = graph_cache_find(h, key);
     if (!ge) {
       st = graph_build(h, key, [&](cudaGraphConditionalHandle cond) -> int {
-        RuArgs a{sd, h->hist_d, hist_cap, p->iter_max, cond, h->err_d};
+        RuArgs a{sd, h->hist_d, hist_cap, p->iter_max, cond, h->err_d, 0};
         int s2 = ru_setup(h, m, b, x, p, a, r, pv, d);
-        if (!s2) s2 = capture_while(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d); });
+        if (!s2)
+          s2 = capture_while(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d, true); });
         if (!s2) s2 = ru_tail(h, m, b, x, a, d);
         return s2;
       }, &ge);

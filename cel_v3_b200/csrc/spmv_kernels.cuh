@@ -40,7 +40,7 @@ struct Acc {
 };
 
 template <typename VT, class Epi>
-__global__ void __launch_bounds__(kCsrThreads, 2)
+__global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
     csr_tma_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
                    const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
                    RedCtx red, int* err) {

@@ -185,6 +185,24 @@ int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_hos
 int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
                      double* const* x_d, const celg_params* p, celg_result* res);
 
+/* ---- diagnostics --------------------------------------------------------------- */
+/* Runs the library's bounded device wait on an mbarrier that nothing arrives
+ * on, with a limit of limit_ms (1..10000) milliseconds, and stores the status
+ * the kernel reported (CELG_ERR_TIMEOUT when the bound works).  The handle and
+ * its context remain usable.  No counterpart in the reference, whose waits
+ * (MPI_Test polling, src/felmsolver/cel_elmsolver_module.f90:637-644) have no
+ * limit. */
+int celg_check_bounded_wait(celg_handle* h, int limit_ms, int* status);
+
+/* Jacobi-PCG on k (1..32) right-hand sides sharing one matrix: B_d and X_d
+ * are n x k row-major (entry (i,c) at i*k + c).  Every column runs its own
+ * recurrence (own scalars, own convergence); each iteration reads the matrix
+ * once for all columns (block SpMM).  res (k entries, nullable) receives the
+ * per-column reports.  Per-column SpMVs are bit-identical to celg_spmv; the
+ * column dot products use a warp-ordered tile reduction (see multirhs.cu). */
+int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
+                      const celg_params* p, celg_result* res);
+
 /* ---- allocation-free entry point ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device
  * memory (their device memory belongs to their own pool or to another
