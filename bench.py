@@ -172,6 +172,41 @@ def batch_form(h, celgpu, torch, stream):
     return out
 
 
+def multirhs_form(h, celgpu, torch, stream):
+    """128^3 Poisson with 32 right-hand sides ~ U[-1,1) (seed 5) to rel-res 1e-8:
+    one multi-RHS solve against 32 single solves."""
+    from cel_v3_b200 import synth
+    rp, ci, v, B = synth.multirhs_problem()
+    n, k = B.shape
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd = torch.from_numpy(B).cuda()
+    Xd = torch.zeros_like(Bd)
+    cols = [Bd[:, c].contiguous() for c in range(k)]
+    xs = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(k)]
+    p = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    runs = (("one_by_one", lambda: [h.pcg_jacobi(m, c.data_ptr(), x.data_ptr(), p) for c, x in zip(cols, xs)]),
+            ("multirhs", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p)))
+    for name, fn in runs:
+        fn()
+        torch.cuda.synchronize()
+        reps = 2
+        e0.record(stream)
+        for _ in range(reps):
+            infos = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "solves_per_s": k * 1e3 / ms,
+                     "max_iters": max(i.iter_done for i in infos),
+                     "worst_verified_relres": max(i.verified_relres for i in infos),
+                     "all_ok": all(i.status == celgpu.OK for i in infos)}
+    out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
+    m.destroy()
+    return out
+
+
 def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
     """Time the oracle's reference-order PCG on the host cores for a bounded
     number of iterations and scale to solves/s."""
@@ -351,6 +386,7 @@ def run_gpu(args):
         for k in ("fp32_ir_1e-10", "fp32_ru_1e-10"):
             forms[k]["speedup_vs_fp64_at_1e-10"] = forms[k]["solves_per_s"] / base
         forms["batched_64"] = batch_form(h, celgpu, torch, stream)
+        forms["multirhs_128_k32"] = multirhs_form(h, celgpu, torch, stream)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))
