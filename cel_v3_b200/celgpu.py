@@ -127,6 +127,8 @@ def _load():
         "celg_pcg_batched": (i, [vp, i, vp, vp, vp, ctypes.POINTER(Params), vp]),
         "celg_check_bounded_wait": (i, [vp, i, ip]),
         "celg_pcg_multirhs": (i, [vp, vp, i, vp, vp, ctypes.POINTER(Params), vp]),
+        "celg_pcg_adjoint": (i, [vp, vp, vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
+        "celg_diffusion7_face_grad": (i, [vp, i, i, i, vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -400,6 +402,23 @@ class Handle:
                                    ctypes.c_void_p(X_d), ctypes.byref(p), res)
         _check(st, "celg_pcg_multirhs", allow=(ERR_NOCONV, ERR_BREAKDOWN))
         return [_info(r, None, r.err) for r in res]
+
+    def pcg_adjoint(self, mat, x_d, g_d, lambda_d, grad_vals_d=None, p=None, **kw):
+        """lambda = A^{-1} g (dL/db) and optionally dL/dA on the pattern."""
+        p = p or params(**kw)
+        res = Result()
+        st = lib.celg_pcg_adjoint(self.ptr, mat.ptr, ctypes.c_void_p(x_d), ctypes.c_void_p(g_d),
+                                  ctypes.c_void_p(lambda_d),
+                                  ctypes.c_void_p(grad_vals_d) if grad_vals_d else None,
+                                  ctypes.byref(p), ctypes.byref(res))
+        _check(st, "celg_pcg_adjoint", allow=(ERR_NOCONV,))
+        return _info(res, None, st)
+
+    def diffusion7_face_grad(self, nx, ny, nz, lambda_d, x_d, gkx_d, gky_d, gkz_d):
+        _check(lib.celg_diffusion7_face_grad(self.ptr, int(nx), int(ny), int(nz),
+                                             ctypes.c_void_p(lambda_d), ctypes.c_void_p(x_d),
+                                             ctypes.c_void_p(gkx_d), ctypes.c_void_p(gky_d),
+                                             ctypes.c_void_p(gkz_d)), "celg_diffusion7_face_grad")
 
     def check_bounded_wait(self, limit_ms=200):
         """Status reported by a bounded device wait that is never satisfied."""

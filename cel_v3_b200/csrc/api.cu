@@ -4,6 +4,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -92,11 +93,101 @@ static int ew_grid(celg_handle* h, long n) {
   return (int)std::max(1L, std::min((n + 255) / 256, (long)h->sms * 16));
 }
 
+// ---- column-offset dictionary of the FP32 copy --------------------------------
+
+constexpr int kOffSlots = 1024;
+constexpr int kOffEmpty = INT_MIN;
+
+// distinct column offsets (col - row) into an open-addressed set; gives up
+// (overflow) beyond kDictMax distinct offsets
+__global__ void offset_set_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                  int* table, int* count, int* overflow) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      if (*(volatile int*)overflow) return;
+      const int off = ci[k] - (int)i;
+      unsigned hsh = ((unsigned)off * 2654435761u) & (kOffSlots - 1);
+      for (int probe = 0; probe < kOffSlots; ++probe) {
+        const int cur = *(volatile int*)&table[hsh];
+        if (cur == off) break;
+        if (cur == kOffEmpty) {
+          const int prev = atomicCAS(&table[hsh], kOffEmpty, off);
+          if (prev == kOffEmpty) {
+            if (atomicAdd(count, 1) >= kDictMax) atomicExch(overflow, 1);
+            break;
+          }
+          if (prev == off) break;
+        }
+        hsh = (hsh + 1) & (kOffSlots - 1);
+      }
+    }
+  }
+}
+
+__global__ void offset_index_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                    const int* __restrict__ dict, int ndict, uint8_t* __restrict__ ci8) {
+  __shared__ int s_dict[kDictMax];
+  for (int q = threadIdx.x; q < ndict; q += blockDim.x) s_dict[q] = dict[q];
+  __syncthreads();
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    for (int k = rp[i]; k < rp[i + 1]; ++k) {
+      const int off = ci[k] - (int)i;
+      int lo = 0, hi = ndict - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_dict[mid] < off) lo = mid + 1; else hi = mid;
+      }
+      ci8[k] = (uint8_t)lo;
+    }
+  }
+}
+
+// Build ci8/dict for the FP32 copy; leaves them unset when the matrix has
+// more than kDictMax distinct offsets.
+static int build_offset_dict(celg_handle* h, celg_mat* m) {
+  CsrDev& A = m->csr;
+  cudaFree(A.ci8);
+  cudaFree(A.dict);
+  A.ci8 = nullptr;
+  A.dict = nullptr;
+  A.ndict = 0;
+  if (A.n == 0 || A.nnz == 0) return CELG_OK;
+  int* table = nullptr;
+  CELG_CUDA(cudaMalloc(&table, sizeof(int) * (kOffSlots + 2)));
+  std::vector<int> init(kOffSlots + 2, kOffEmpty);
+  init[kOffSlots] = 0;
+  init[kOffSlots + 1] = 0;
+  CELG_CUDA(cudaMemcpyAsync(table, init.data(), sizeof(int) * init.size(), cudaMemcpyHostToDevice, h->stream));
+  offset_set_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci, table, table + kOffSlots,
+                                                           table + kOffSlots + 1);
+  std::vector<int> out(kOffSlots + 2);
+  cudaError_t e = cudaMemcpyAsync(out.data(), table, sizeof(int) * out.size(), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(table);
+  if (e != cudaSuccess) return cuda_status(e, "offset dictionary");
+  if (out[kOffSlots + 1] || out[kOffSlots] > kDictMax) return CELG_OK;  // too many offsets
+  std::vector<int> dict;
+  for (int q = 0; q < kOffSlots; ++q)
+    if (out[q] != kOffEmpty) dict.push_back(out[q]);
+  std::sort(dict.begin(), dict.end());
+  CELG_CUDA(cudaMalloc(&A.dict, sizeof(int) * dict.size()));
+  CELG_CUDA(cudaMalloc(&A.ci8, (size_t)A.nnz + 32));
+  CELG_CUDA(cudaMemsetAsync(A.ci8 + A.nnz, 0, 32, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(A.dict, dict.data(), sizeof(int) * dict.size(), cudaMemcpyHostToDevice, h->stream));
+  A.ndict = (int)dict.size();
+  offset_index_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci, A.dict, A.ndict, A.ci8);
+  CELG_CUDA(cudaGetLastError());
+  A.cap_dict = (A.cap + 24 + 15) & ~15;  // 16-entry aligned spans are at most 24 entries wider
+  return CELG_OK;
+}
+
 static void free_mat_arrays(celg_mat* m) {
   cudaFree(m->csr.rp);
   cudaFree(m->csr.ci);
   cudaFree(m->csr.v);
   cudaFree(m->csr.v32);
+  cudaFree(m->csr.ci8);
+  cudaFree(m->csr.dict);
   cudaFree(m->jad.begin);
   cudaFree(m->jad.ci);
   cudaFree(m->jad.v);
@@ -488,10 +579,11 @@ extern "C" int celg_mat_make_fp32(celg_mat* m) {
   if (!m) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(m->h->device));
   if (!m->csr.v32) {
-    CELG_CUDA(cudaMalloc(&m->csr.v32, sizeof(float) * ((size_t)m->csr.nnz + 8)));
-    CELG_CUDA(cudaMemsetAsync(m->csr.v32 + m->csr.nnz, 0, sizeof(float) * 8, m->h->stream));
+    CELG_CUDA(cudaMalloc(&m->csr.v32, sizeof(float) * ((size_t)m->csr.nnz + 32)));
+    CELG_CUDA(cudaMemsetAsync(m->csr.v32 + m->csr.nnz, 0, sizeof(float) * 32, m->h->stream));
   }
   int st = launch_to_f32(m->h, m->csr.nnz, m->csr.v, m->csr.v32);
+  if (!st && !m->csr.ci8) st = build_offset_dict(m->h, m);
   if (!st && m->jacobi) {
     if (!m->jacobi32) CELG_CUDA(cudaMalloc(&m->jacobi32, sizeof(float) * std::max(1, m->csr.n)));
     st = launch_to_f32(m->h, m->csr.n, m->jacobi, m->jacobi32);

@@ -151,6 +151,25 @@ __device__ __forceinline__ double group_fold256(double v, double* scratch, int t
   return tot;
 }
 
+// The 256-lane order computed by one warp: lane l plays the virtual lanes
+// l + 32 g (g = 0..7) -- virtual lane j sums p[j], p[j+256], ... from 0.0;
+// each group of 32 virtual lanes folds with the butterfly; the 8 group sums
+// are added in order.  Bit-identical to group_fold256 over 256 threads, and
+// lets independent reductions run in parallel warps.  Result in all lanes.
+__device__ __forceinline__ double warp_reduce256(const double* p, long cnt, int lane) {
+  double s[8];
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    double acc = 0.0;
+    for (long k = lane + 32 * g; k < cnt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
+    s[g] = warp_fold(acc);
+  }
+  double tot = s[0];
+#pragma unroll
+  for (int g = 1; g < 8; ++g) tot = dadd(tot, s[g]);
+  return tot;
+}
+
 // Last-block-done completion for NRED reductions whose tile partials are in
 // red.partials[r * ntiles + t].  Called by the 256 lanes of each CTA after
 // all of its partials were written (by lane 0).  Returns true in lane 0 of
@@ -166,13 +185,16 @@ __device__ __forceinline__ bool grid_finish(const RedCtx& red, double (&tot)[NRE
   named_bar_sync(bar_id, kLanes);
   if (*s_flag == 0) return false;
   __threadfence();
-#pragma unroll
-  for (int r = 0; r < NRED; ++r) {
-    double s = 0.0;
-    const double* p = red.partials + (long)r * red.ntiles;
-    for (long k = tid; k < red.ntiles; k += kLanes) s = dadd(s, __ldcg(p + k));
-    tot[r] = group_fold256(s, scratch, tid, bar_id);
+  // reduction r by warp r, in parallel
+  if ((tid >> 5) < NRED) {
+    const int r = tid >> 5;
+    const double v = warp_reduce256(red.partials + (long)r * red.ntiles, red.ntiles, tid & 31);
+    if ((tid & 31) == 0) scratch[r] = v;
   }
+  named_bar_sync(bar_id, kLanes);
+#pragma unroll
+  for (int r = 0; r < NRED; ++r) tot[r] = scratch[r];
+  named_bar_sync(bar_id, kLanes);
   if (tid == 0) *red.ticket = 0u;
   return tid == 0;
 }
@@ -216,17 +238,18 @@ __device__ __forceinline__ void batch_tile_done(const RedCtx& red, Epi& epi, lon
   named_bar_sync(bar_id, kLanes);
   if (*s_flag) {
     __threadfence();
-    double tot[NRED];
     const long t0 = br.sys_tile0[s];
     const long nt = br.sys_ntiles[s];
-#pragma unroll
-    for (int r = 0; r < NRED; ++r) {
-      double acc = 0.0;
-      const double* p = red.partials + (long)r * red.ntiles + t0;
-      for (long k = tid; k < nt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
-      tot[r] = group_fold256(acc, scratch, tid, bar_id);
+    if ((tid >> 5) < NRED) {
+      const int r = tid >> 5;
+      const double v = warp_reduce256(red.partials + (long)r * red.ntiles + t0, nt, tid & 31);
+      if ((tid & 31) == 0) scratch[r] = v;
     }
+    named_bar_sync(bar_id, kLanes);
     if (tid == 0) {
+      double tot[NRED];
+#pragma unroll
+      for (int r = 0; r < NRED; ++r) tot[r] = scratch[r];
       epi.finish_sys(s, tot);
       br.sys_ticket[s] = 0u;
     }

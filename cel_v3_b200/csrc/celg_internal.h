@@ -21,8 +21,14 @@ struct CsrDev {
   int* rp = nullptr;
   int* ci = nullptr;
   double* v = nullptr;
-  float* v32 = nullptr;   // FP32 copy (refinement inner solve)
+  float* v32 = nullptr;   // FP32 copy (refinement inner solve), nnz+32
   int cap = 0;            // staged entries per 256-row sub-tile
+  // FP32 copy's column indices as 1-byte indices into a dictionary of
+  // column offsets (col - row), when the matrix has at most 256 of them
+  uint8_t* ci8 = nullptr; // nnz+32
+  int* dict = nullptr;    // ndict offsets, ascending
+  int ndict = 0;
+  int cap_dict = 0;       // staging capacity with 16-entry alignment
 };
 
 struct JadDev {

@@ -84,12 +84,10 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
   named_bar_sync(1, kLanes);
   if (!*s_flag) return;
   __threadfence();
-  for (int rc = 0; rc < NRED * k; ++rc) {
-    const double* p = red.partials + (long)rc * red.ntiles;
-    double s = 0.0;
-    for (long q = tid; q < red.ntiles; q += kLanes) s = dadd(s, __ldcg(p + q));
-    const double tot = group_fold256(s, scratch, tid, 1);
-    if (tid == 0) s_tot[rc] = tot;
+  // (reduction, column) pairs spread over the 8 warps, each in the 256-lane order
+  for (int rc = tid >> 5; rc < NRED * k; rc += 8) {
+    const double v = warp_reduce256(red.partials + (long)rc * red.ntiles, red.ntiles, tid & 31);
+    if ((tid & 31) == 0) s_tot[rc] = v;
   }
   named_bar_sync(1, kLanes);
   if (tid < k) {

@@ -6,9 +6,9 @@
 
 namespace celg {
 
-int csr_smem_bytes(int cap, int vt_size) {
-  StageLayout L(cap, vt_size);
-  return kCsrHeader + kStages * L.bytes;
+int csr_smem_bytes(int cap, int vt_size, int ct_size) {
+  StageLayout L(cap, vt_size, ct_size);
+  return kCsrHeader + (ct_size == 1 ? kDictMax * 4 : 0) + kStages * L.bytes;
 }
 
 // Largest 16-byte-rounded entry span of any 256-row sub-tile.

@@ -22,16 +22,26 @@
 
 namespace celg {
 
-// Shared-memory layout of one pipeline stage for `cap` staged entries.
+// Shared-memory layout of one pipeline stage for `cap` staged entries with
+// column indices of ct_size bytes (4: int32 columns; 1: offset-dictionary
+// indices) and values of vt_size bytes.
 struct StageLayout {
   int ci_off, v_off, bytes;
-  __host__ __device__ StageLayout(int cap, int vt_size) {
-    ci_off = (kSub + 4) * 4;                                   // 1040, 16B multiple
-    v_off = ci_off + (cap + 8) * 4;                            // cap % 4 == 0
-    int end = v_off + (cap + 8) * vt_size;
+  __host__ __device__ StageLayout(int cap, int vt_size, int ct_size = 4) {
+    ci_off = (kSub + 4) * 4;                                          // 1040, 16B multiple
+    v_off = ci_off + (((cap + 32) * ct_size + 15) & ~15);
+    int end = v_off + (cap + 32) * vt_size;
     bytes = (end + 127) & ~127;
   }
 };
+constexpr int kDictMax = 256;  // offset-dictionary entries (uint8 indices)
+
+// column of stored entry k of row `row`: int32 columns are absolute, uint8
+// indices select an offset col - row from the matrix's dictionary
+__device__ __forceinline__ int entry_col(int c, long, const int*) { return c; }
+__device__ __forceinline__ int entry_col(uint8_t c, long row, const int* dict) {
+  return (int)row + dict[c];
+}
 constexpr int kCsrHeader = 256;  // mbarriers, stage meta, fold scratch
 
 template <int N>
@@ -39,21 +49,24 @@ struct Acc {
   double a[N > 0 ? N : 1];
 };
 
-template <typename VT, class Epi>
+template <typename VT, class Epi, typename CT = int>
 __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
-    csr_tma_kernel(const int* __restrict__ rp, const int* __restrict__ ci,
+    csr_tma_kernel(const int* __restrict__ rp, const CT* __restrict__ ci,
                    const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
-                   RedCtx red, int* err) {
+                   RedCtx red, int* err, const int* __restrict__ dict, int ndict) {
   constexpr int NR = Epi::NRED;
   constexpr bool kB = is_batched<Epi>::value;
+  constexpr bool kDict = sizeof(CT) == 1;
+  constexpr int kAlign = kDict ? 16 : 4;  // entries per 16 bytes of the narrowest array
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kStages;
   int* meta = reinterpret_cast<int*>(empty + kStages);        // a0, fallback per stage
   double* scratch = reinterpret_cast<double*>(smem + 128);    // 8 doubles
   int* s_flag = reinterpret_cast<int*>(smem + 192);
-  unsigned char* stages = smem + kCsrHeader;
-  const StageLayout L(cap, (int)sizeof(VT));
+  int* s_dict = reinterpret_cast<int*>(smem + kCsrHeader);    // offset dictionary (kDict)
+  unsigned char* stages = smem + kCsrHeader + (kDict ? kDictMax * 4 : 0);
+  const StageLayout L(cap, (int)sizeof(VT), (int)sizeof(CT));
 
   if (!epi.active()) return;
   const long nsub = ((long)n + kSub - 1) / kSub;
@@ -66,6 +79,9 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
       mbar_init(&empty[s], kConsumerWarps);
     }
     fence_mbar_init();
+  }
+  if constexpr (kDict) {
+    for (int q = threadIdx.x; q < ndict; q += blockDim.x) s_dict[q] = dict[q];
   }
   __syncthreads();
 
@@ -98,19 +114,19 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
           } else {
             const long row0 = s * kSub;
             const int rows = (int)min((long)kSub, (long)n - row0);
-            const int a0 = e0 & ~3;
-            const int a1 = (e1 + 3) & ~3;
+            const int a0 = e0 & ~(kAlign - 1);
+            const int a1 = (e1 + kAlign - 1) & ~(kAlign - 1);
             const int cnt = a1 - a0;
             const int fb = cnt > cap ? 1 : 0;
             meta[2 * st] = a0;
             meta[2 * st + 1] = fb;
             const uint32_t rpb = (uint32_t)(((rows + 1 + 3) & ~3) * 4);
-            const uint32_t mb = fb ? 0u : (uint32_t)cnt * (uint32_t)(4 + sizeof(VT));
+            const uint32_t mb = fb ? 0u : (uint32_t)cnt * (uint32_t)(sizeof(CT) + sizeof(VT));
             unsigned char* sb = stages + (size_t)st * L.bytes;
             mbar_arrive_expect_tx(&full[st], rpb + mb);
             bulk_g2s(sb, rp + row0, rpb, &full[st]);
             if (!fb && cnt > 0) {
-              bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * 4u, &full[st]);
+              bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT), &full[st]);
               bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
             }
           }
@@ -142,7 +158,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
       if (!mbar_wait_bounded(&full[st], (uint32_t)((it / kStages) & 1), err)) return;
       const unsigned char* sb = stages + (size_t)st * L.bytes;
       const int* rps = reinterpret_cast<const int*>(sb);
-      const int* cis = reinterpret_cast<const int*>(sb + L.ci_off);
+      const CT* cis = reinterpret_cast<const CT*>(sb + L.ci_off);
       const VT* vs = reinterpret_cast<const VT*>(sb + L.v_off);
       const int a0 = meta[2 * st];
       const int fb = meta[2 * st + 1];
@@ -160,7 +176,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
             for (int u = 0; u < 8; ++u) {
               if (k + u < ke) {
                 vv[u] = vs[k + u];
-                xv[u] = __ldg(x + cis[k + u]);
+                xv[u] = __ldg(x + entry_col(cis[k + u], row, s_dict));
               }
             }
 #pragma unroll
@@ -168,7 +184,8 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
               if (k + u < ke) sum = vadd(sum, vmul(vv[u], xv[u]));
           }
         } else {
-          for (int k = b; k < e; ++k) sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + __ldg(ci + k))));
+          for (int k = b; k < e; ++k)
+            sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + entry_col(__ldg(ci + k), row, s_dict))));
         }
         ep.row(row, sum, acc.a);
       }
@@ -276,6 +293,6 @@ struct EpiResidual {
 };
 
 // Host helpers (spmv.cu)
-int csr_smem_bytes(int cap, int vt_size);
+int csr_smem_bytes(int cap, int vt_size, int ct_size = 4);
 
 }  // namespace celg

@@ -77,8 +77,9 @@ int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
   return CELG_OK;
 }
 
-template <typename VT, class Epi>
-int launch_csr(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, const Epi& epi) {
+template <typename VT, typename CT, class Epi>
+int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* cols, int cap,
+                  const VT* x, const Epi& epi) {
   const long nt = ntiles_of(A.n);
   RedCtx red{nullptr, h->ticket, nt};
   if (Epi::NRED > 0) {
@@ -87,17 +88,28 @@ int launch_csr(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, con
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
-  const int smem = csr_smem_bytes(A.cap, (int)sizeof(VT));
-  auto kern = csr_tma_kernel<VT, Epi>;
+  const int smem = csr_smem_bytes(cap, (int)sizeof(VT), (int)sizeof(CT));
+  auto kern = csr_tma_kernel<VT, Epi, CT>;
   CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
   per_sm = std::max(1, per_sm);
   const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * per_sm));
-  kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, A.ci, vals, A.n, A.cap, x, epi, red,
-                                               h->err_d);
+  kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, cols, vals, A.n, cap, x, epi, red, h->err_d,
+                                               sizeof(CT) == 1 ? A.dict : nullptr,
+                                               sizeof(CT) == 1 ? A.ndict : 0);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
+}
+
+// CSR sweep with the matrix's own column indices; the FP32 copy uses the
+// 1-byte offset dictionary when the matrix has one.
+template <typename VT, class Epi>
+int launch_csr(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, const Epi& epi) {
+  if constexpr (sizeof(VT) == 4) {
+    if (A.ci8) return launch_csr_ct<VT, uint8_t>(h, A, vals, A.ci8, A.cap_dict, x, epi);
+  }
+  return launch_csr_ct<VT, int>(h, A, vals, A.ci, A.cap, x, epi);
 }
 
 template <class Epi>

@@ -157,6 +157,11 @@ int celg_jacobi_apply(celg_handle* h, const celg_mat* m, const double* r_d, doub
 
 /* ---- solvers (b_d, x_d device vectors of length n) ---------------------------- */
 /* Jacobi-PCG, cel_cgalg_jacobi (src/fcgalg/cel_cgalg_module.f90:178-305).
+ * The loop runs while iter < iter_max, ||r|| > eps and |r.z| > 1.1 eps_mach:
+ * the last test is the reference's absolute guard (:248), so a solve whose
+ * residual is already tiny in absolute terms (small ||b||, tight eps_rel) can
+ * end with CELG_OK before ||r|| <= eps; final_norm2 and verified_relres say
+ * where it ended.
  * precision CELG_PREC_FP32_IR runs FP32-storage PCG sweeps inside FP64
  * iterative refinement; the outer residual, update and test stay FP64. */
 int celg_pcg_jacobi(celg_handle* h, celg_mat* m, const double* b_d, double* x_d,
@@ -202,6 +207,22 @@ int celg_check_bounded_wait(celg_handle* h, int limit_ms, int* status);
  * column dot products use a warp-ordered tile reduction (see multirhs.cu). */
 int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
                       const celg_params* p, celg_result* res);
+
+/* ---- differentiation --------------------------------------------------------- */
+/* Adjoint of a Jacobi-PCG solve x = A^{-1} b (A symmetric): given x_d and
+ * g_d = dL/dx, solves A lambda = g with Jacobi-PCG under p (the precision
+ * field is ignored: FP64), writes lambda_d = dL/db and, when grad_vals_d is
+ * not NULL, dL/dA on the sparsity pattern: grad_vals_d[k] = -lambda_i x_j for
+ * stored entry k = (i, j).  res reports the adjoint solve. */
+int celg_pcg_adjoint(celg_handle* h, celg_mat* m, const double* x_d, const double* g_d,
+                     double* lambda_d, double* grad_vals_d, const celg_params* p, celg_result* res);
+/* Face-coefficient gradient of a 7-point diffusion operator on an nx x ny x nz
+ * grid (A_ii = sum of the cell's six face coefficients, A_ij = -k_f):
+ * dL/dk_f = -(lambda_i - lambda_j)(x_i - x_j) for the face between cells i, j
+ * and -(lambda_i x_i) for a Dirichlet face of cell i.  Face arrays are x-fastest
+ * with shapes (nz, ny, nx+1), (nz, ny+1, nx), (nz+1, ny, nx). */
+int celg_diffusion7_face_grad(celg_handle* h, int nx, int ny, int nz, const double* lambda_d,
+                              const double* x_d, double* gkx_d, double* gky_d, double* gkz_d);
 
 /* ---- allocation-free entry point ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

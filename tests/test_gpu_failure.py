@@ -22,8 +22,8 @@ def test_bounded_wait_times_out_and_context_survives(gpu):
     m = h.matrix_from_csr(rp, ci, v).jacobi()
     b = torch.ones(rp.size - 1, dtype=torch.float64, device="cuda")
     x = torch.zeros_like(b)
-    info = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), eps_rel=1e-10)
-    assert info.status == celgpu.OK and info.verified_relres <= 1e-10
+    info = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), eps_rel=1e-8)
+    assert info.status == celgpu.OK and info.verified_relres <= 1.5e-8
     m.destroy()
 
 

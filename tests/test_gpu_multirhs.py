@@ -90,7 +90,9 @@ def test_multirhs_bitexact_and_close_to_single(gpu, case):
     X = Xd.cpu().numpy()
     assert np.array_equal(X, Xo)
     assert [i.iter_done for i in infos] == list(ito)
-    assert all(i.status == celgpu.OK and i.verified_relres <= 1e-10 for i in infos)
+    # the loop may also end on the reference's absolute |r.z| guard
+    # (cel_cgalg_module.f90:248) once ||r|| is tiny: the true residual stays small
+    assert all(i.status == celgpu.OK and i.verified_relres <= 1e-8 for i in infos)
     for c in range(k):
         xs = dev(torch, np.zeros(n))
         one = h.pcg_jacobi(m, dev(torch, B[:, c]).data_ptr(), xs.data_ptr(), eps_rel=1e-10, iter_max=2000)
