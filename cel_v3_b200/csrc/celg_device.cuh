@@ -159,14 +159,30 @@ __device__ __forceinline__ double group_fold256(double v, double* scratch, int t
 __device__ __forceinline__ double warp_reduce256(const double* p, long cnt, int lane) {
   double s[8];
 #pragma unroll
-  for (int g = 0; g < 8; ++g) {
-    double acc = 0.0;
-    for (long k = lane + 32 * g; k < cnt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
-    s[g] = warp_fold(acc);
-  }
-  double tot = s[0];
+  for (int g = 0; g < 8; ++g) s[g] = 0.0;
+  // rounds of 4 x 256 elements: the 32 loads of a lane are issued before
+  // its adds, which stay in element order within each virtual lane
+  for (long base = 0; base < cnt; base += 4 * kLanes) {
+    double v[4][8];
 #pragma unroll
-  for (int g = 1; g < 8; ++g) tot = dadd(tot, s[g]);
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {
+        const long k = base + (long)u * kLanes + 32 * g + lane;
+        v[u][g] = k < cnt ? __ldcg(p + k) : 0.0;
+      }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int g = 0; g < 8; ++g)
+        if (base + (long)u * kLanes + 32 * g + lane < cnt) s[g] = dadd(s[g], v[u][g]);
+  }
+  double tot = 0.0;
+#pragma unroll
+  for (int g = 0; g < 8; ++g) {
+    const double f = warp_fold(s[g]);
+    tot = g == 0 ? f : dadd(tot, f);
+  }
   return tot;
 }
 
@@ -185,16 +201,13 @@ __device__ __forceinline__ bool grid_finish(const RedCtx& red, double (&tot)[NRE
   named_bar_sync(bar_id, kLanes);
   if (*s_flag == 0) return false;
   __threadfence();
-  // reduction r by warp r, in parallel
-  if ((tid >> 5) < NRED) {
-    const int r = tid >> 5;
-    const double v = warp_reduce256(red.partials + (long)r * red.ntiles, red.ntiles, tid & 31);
-    if ((tid & 31) == 0) scratch[r] = v;
-  }
-  named_bar_sync(bar_id, kLanes);
 #pragma unroll
-  for (int r = 0; r < NRED; ++r) tot[r] = scratch[r];
-  named_bar_sync(bar_id, kLanes);
+  for (int r = 0; r < NRED; ++r) {
+    double s = 0.0;
+    const double* p = red.partials + (long)r * red.ntiles;
+    for (long k = tid; k < red.ntiles; k += kLanes) s = dadd(s, __ldcg(p + k));
+    tot[r] = group_fold256(s, scratch, tid, bar_id);
+  }
   if (tid == 0) *red.ticket = 0u;
   return tid == 0;
 }
@@ -238,18 +251,17 @@ __device__ __forceinline__ void batch_tile_done(const RedCtx& red, Epi& epi, lon
   named_bar_sync(bar_id, kLanes);
   if (*s_flag) {
     __threadfence();
+    double tot[NRED];
     const long t0 = br.sys_tile0[s];
     const long nt = br.sys_ntiles[s];
-    if ((tid >> 5) < NRED) {
-      const int r = tid >> 5;
-      const double v = warp_reduce256(red.partials + (long)r * red.ntiles + t0, nt, tid & 31);
-      if ((tid & 31) == 0) scratch[r] = v;
-    }
-    named_bar_sync(bar_id, kLanes);
-    if (tid == 0) {
-      double tot[NRED];
 #pragma unroll
-      for (int r = 0; r < NRED; ++r) tot[r] = scratch[r];
+    for (int r = 0; r < NRED; ++r) {
+      double acc = 0.0;
+      const double* p = red.partials + (long)r * red.ntiles + t0;
+      for (long k = tid; k < nt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
+      tot[r] = group_fold256(acc, scratch, tid, bar_id);
+    }
+    if (tid == 0) {
       epi.finish_sys(s, tot);
       br.sys_ticket[s] = 0u;
     }

@@ -435,35 +435,62 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   a.k = k;
   a.iter_max = p->iter_max;
   a.errw = h->err_d;
+  a.cond = 0;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
-  auto record = [&](cudaGraphConditionalHandle cond) -> int {
-    MultiArgs ac = a;
-    ac.cond = cond;
+  auto setup = [&](const MultiArgs& ac) -> int {
     int s2 = launch_mtile(h, n, k, MOpPre{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
     if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit{B, R, P, m->jacobi, k, ac});
-    if (!s2)
-      s2 = capture_while(h, cond, [&]() -> int {
-        int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac});
-        if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate{X, R, P, V, m->jacobi, ac, 0.0});
-        if (!s3) s3 = launch_mtile(h, n, k, MOpDirection{P, R, m->jacobi, ac, 0.0});
-        return s3;
-      });
-    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac});
     return s2;
   };
-  char kb[256];
-  std::snprintf(kb, sizeof(kb), "mrhs|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%d", (const void*)m, m->csr.n, k,
-                (const void*)B, (const void*)X, (const void*)R, p->x0_mode, p->eps_abs, p->eps_rel,
-                p->iter_max);
-  const std::string key(kb);
-  GraphEntry* ge = graph_cache_find(h, key);
-  if (!ge) {
-    st = graph_build(h, key, record, &ge);
+  auto body = [&](const MultiArgs& ac) -> int {
+    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate{X, R, P, V, m->jacobi, ac, 0.0});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection{P, R, m->jacobi, ac, 0.0});
+    return s3;
+  };
+  auto tail = [&](const MultiArgs& ac) -> int {
+    return launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac});
+  };
+  if (!graphs_enabled()) {
+    // profiling mode: the same kernels from a host loop (see graph.cuh)
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    a.cond = 0;
+    st = setup(a);
+    for (int it = 0; !st && it < p->iter_max; it += 8) {
+      for (int q = 0; q < 8 && !st; ++q) st = body(a);
+      int act = 0;
+      if (!st) {
+        CELG_CUDA(cudaMemcpyAsync(&act, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CELG_CUDA(cudaStreamSynchronize(h->stream));
+      }
+      if (!act) break;
+    }
+    if (!st) st = tail(a);
     if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    auto record = [&](cudaGraphConditionalHandle cond) -> int {
+      MultiArgs ac = a;
+      ac.cond = cond;
+      int s2 = setup(ac);
+      if (!s2) s2 = capture_while(h, cond, [&]() -> int { return body(ac); });
+      if (!s2) s2 = tail(ac);
+      return s2;
+    };
+    char kb[256];
+    std::snprintf(kb, sizeof(kb), "mrhs|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%d", (const void*)m, m->csr.n, k,
+                  (const void*)B, (const void*)X, (const void*)R, p->x0_mode, p->eps_abs, p->eps_rel,
+                  p->iter_max);
+    const std::string key(kb);
+    GraphEntry* ge = graph_cache_find(h, key);
+    if (!ge) {
+      st = graph_build(h, key, record, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   }
-  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
-  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
-  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   std::vector<double> ds(7 * kMaxRhs);
   std::vector<int> is(3 * kMaxRhs + 1);
   CELG_CUDA(cudaMemcpyAsync(ds.data(), mu->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost, h->stream));

@@ -3,6 +3,7 @@
   python -m cel_v3_b200.drive spmv SIDE [REPS]          REPS CSR SpMVs, SIDE^3 Poisson
   python -m cel_v3_b200.drive pcg SIDE ITERS [fp64|ru|ir]
                                                         one solve capped at ITERS iterations
+  python -m cel_v3_b200.drive mrhs SIDE ITERS K         K right-hand sides, capped at ITERS
 
 Set CELG_GRAPH=0 to launch the solver kernels from a host loop instead of
 one CUDA graph, so that a kernel profiler can attribute time to each kernel.
@@ -40,6 +41,13 @@ def main(argv):
                             iter_max=iters, **kw)
         torch.cuda.synchronize()
         print("pcg", side, mode, info.iter_done, info.status)
+    elif what == "mrhs":
+        iters, k = int(argv[2]), int(argv[3])
+        B = torch.rand((n, k), dtype=torch.float64, device="cuda")
+        X = torch.zeros_like(B)
+        infos = h.pcg_multirhs(m, k, B.data_ptr(), X.data_ptr(), eps_rel=1e-12, iter_max=iters)
+        torch.cuda.synchronize()
+        print("mrhs", side, k, max(i.iter_done for i in infos))
     else:
         raise SystemExit(__doc__)
     h.close()
