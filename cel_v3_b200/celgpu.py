@@ -129,6 +129,19 @@ def _load():
         "celg_pcg_multirhs": (i, [vp, vp, i, vp, vp, ctypes.POINTER(Params), vp]),
         "celg_pcg_adjoint": (i, [vp, vp, vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
         "celg_diffusion7_face_grad": (i, [vp, i, i, i, vp, vp, vp, vp, vp]),
+        "celg_mat_from_csr_ext": (i, [vp, i, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_dist_create": (i, [vp, vp, ctypes.POINTER(Params), vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_dist_destroy": (i, [vp]),
+        "celg_dist_exchange_buffer": (i, [vp, ctypes.POINTER(vp)]),
+        "celg_dist_pcg_begin": (i, [vp, vp, vp]),
+        "celg_dist_pcg_init": (i, [vp, vp, vp, vp, vp]),
+        "celg_dist_pcg_start": (i, [vp]),
+        "celg_dist_pcg_ap": (i, [vp, vp, vp]),
+        "celg_dist_pcg_update": (i, [vp, vp, vp, vp, vp]),
+        "celg_dist_pcg_direction": (i, [vp, vp, vp]),
+        "celg_dist_pcg_poll": (i, [vp, ip, ip]),
+        "celg_dist_pcg_verify": (i, [vp, vp, vp]),
+        "celg_dist_pcg_result": (i, [vp, ctypes.POINTER(Result)]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -174,6 +187,74 @@ def dot_noalloc(n, a_d, b_d, out_d, stream=0):
     include/celgpu.h); returns the status code."""
     return lib.celg_dot_noalloc(int(n), ctypes.c_void_p(a_d), ctypes.c_void_p(b_d),
                                 ctypes.c_void_p(out_d), ctypes.c_void_p(int(stream)) if stream else None)
+
+
+DIST_NEXCH = 5
+DIST_STATE_BYTES = 256
+
+
+class Dist:
+    """celg_dist: the phases of a distributed Jacobi-PCG on one rank's row
+    block (device pointers; see include/celgpu.h for the sequence)."""
+
+    def __init__(self, handle, mat, p, state_d=0, hist_d=0, hist_cap=0):
+        self.handle = handle
+        self.ptr = ctypes.c_void_p()
+        _check(lib.celg_dist_create(handle.ptr, mat.ptr, ctypes.byref(p),
+                                    ctypes.c_void_p(state_d) if state_d else None,
+                                    ctypes.c_void_p(hist_d) if hist_d else None, int(hist_cap),
+                                    ctypes.byref(self.ptr)), "celg_dist_create")
+        self.iter_max = p.iter_max
+
+    def _call(self, name, *ptrs):
+        _check(getattr(lib, name)(self.ptr, *[ctypes.c_void_p(q) for q in ptrs]), name)
+
+    def exchange_buffer(self):
+        out = ctypes.c_void_p()
+        _check(lib.celg_dist_exchange_buffer(self.ptr, ctypes.byref(out)), "celg_dist_exchange_buffer")
+        return out.value
+
+    def begin(self, b_d, x_ext_d):
+        self._call("celg_dist_pcg_begin", b_d, x_ext_d)
+
+    def init(self, b_d, x_ext_d, r_d, p_ext_d):
+        self._call("celg_dist_pcg_init", b_d, x_ext_d, r_d, p_ext_d)
+
+    def start(self):
+        self._call("celg_dist_pcg_start")
+
+    def ap(self, p_ext_d, v_d):
+        self._call("celg_dist_pcg_ap", p_ext_d, v_d)
+
+    def update(self, x_ext_d, r_d, p_ext_d, v_d):
+        self._call("celg_dist_pcg_update", x_ext_d, r_d, p_ext_d, v_d)
+
+    def direction(self, r_d, p_ext_d):
+        self._call("celg_dist_pcg_direction", r_d, p_ext_d)
+
+    def poll(self):
+        a, it = ctypes.c_int(), ctypes.c_int()
+        _check(lib.celg_dist_pcg_poll(self.ptr, ctypes.byref(a), ctypes.byref(it)), "celg_dist_pcg_poll")
+        return a.value, it.value
+
+    def verify(self, b_d, x_ext_d):
+        self._call("celg_dist_pcg_verify", b_d, x_ext_d)
+
+    def result(self, history=False):
+        res = Result()
+        hist = None
+        if history:
+            hist = np.zeros(self.iter_max + 1)
+            res.history = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            res.history_cap = hist.size
+        st = lib.celg_dist_pcg_result(self.ptr, ctypes.byref(res))
+        _check(st, "celg_dist_pcg_result", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return _info(res, hist, st)
+
+    def destroy(self):
+        if self.ptr:
+            lib.celg_dist_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
 
 
 class SolveInfo(dict):
@@ -308,6 +389,20 @@ class Handle:
         _check(lib.celg_mat_from_csr(self.ptr, n, int(ci.size), _host_ptr(rp), _host_ptr(ci),
                                      _host_ptr(v), int(index_base), ctypes.byref(m)),
                "celg_mat_from_csr")
+        mat = Matrix(self, m)
+        self.mats.append(mat)
+        return mat
+
+    def matrix_from_csr_ext(self, rp, ci, v, ncols, index_base=0):
+        """A row block with halo columns n..ncols-1 (celg_mat_from_csr_ext)."""
+        rp = np.ascontiguousarray(rp, np.int32)
+        ci = np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, np.float64)
+        m = ctypes.c_void_p()
+        _check(lib.celg_mat_from_csr_ext(self.ptr, rp.size - 1, int(ncols), int(ci.size),
+                                         _host_ptr(rp), _host_ptr(ci), _host_ptr(v),
+                                         int(index_base), ctypes.byref(m)),
+               "celg_mat_from_csr_ext")
         mat = Matrix(self, m)
         self.mats.append(mat)
         return mat

@@ -61,7 +61,7 @@ using namespace celg;
 extern "C" int celg_pcg_adjoint(celg_handle* h, celg_mat* m, const double* x_d, const double* g_d,
                                 double* lambda_d, double* grad_vals_d, const celg_params* p,
                                 celg_result* res) {
-  if (!h || !m || !p || m->h != h) return CELG_ERR_ARG;
+  if (!h || !m || !p || m->h != h || m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
   if (m->csr.n > 0 && (!x_d || !g_d || !lambda_d)) return CELG_ERR_ARG;
   if (!m->jacobi) return CELG_ERR_STATE;
   CELG_CUDA(cudaSetDevice(h->device));

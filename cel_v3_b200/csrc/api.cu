@@ -26,8 +26,8 @@ int cuda_status(cudaError_t e, const char* what) {
 // 0-based conversion, padding of the row-pointer tail and validation.
 // bad[0] is set when row_ptr is not monotone or its ends are wrong, bad[1]
 // when a column index is out of range.
-__global__ void csr_prepare_kernel(int n, int nnz, int base, int* rp, int* ci, int pad_rp,
-                                   int* bad) {
+__global__ void csr_prepare_kernel(int n, int ncols, int nnz, int base, int* rp, int* ci,
+                                   int pad_rp, int* bad) {
   const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long stride = (long)gridDim.x * blockDim.x;
   for (long i = tid; i <= n; i += stride) {
@@ -38,7 +38,7 @@ __global__ void csr_prepare_kernel(int n, int nnz, int base, int* rp, int* ci, i
   for (long k = tid; k < nnz; k += stride) {
     const int c = ci[k] - base;
     ci[k] = c;
-    if (c < 0 || c >= n) atomicExch(&bad[1], 1);
+    if (c < 0 || c >= ncols) atomicExch(&bad[1], 1);
   }
   for (long i = tid; i < pad_rp; i += stride) rp[n + 1 + i] = nnz;
 }
@@ -199,9 +199,10 @@ static void free_mat_arrays(celg_mat* m) {
 }
 
 // Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.
-static int alloc_csr(celg_mat* m, int n, int nnz) {
+static int alloc_csr(celg_mat* m, int n, int nnz, int ncols) {
   m->csr.n = n;
   m->csr.nnz = nnz;
+  m->csr.ncols = ncols;
   CELG_CUDA(cudaMalloc(&m->csr.rp, sizeof(int) * ((size_t)n + 1 + 8)));
   CELG_CUDA(cudaMalloc(&m->csr.ci, sizeof(int) * ((size_t)nnz + 8)));
   CELG_CUDA(cudaMalloc(&m->csr.v, sizeof(double) * ((size_t)nnz + 8)));
@@ -215,7 +216,7 @@ static int finish_csr(celg_handle* h, celg_mat* m, int base) {
   int* bad = h->err_d + 2;
   CELG_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int), h->stream));
   csr_prepare_kernel<<<ew_grid(h, std::max(n + 1, nnz)), 256, 0, h->stream>>>(
-      n, nnz, base, m->csr.rp, m->csr.ci, 8, bad);
+      n, m->csr.ncols, nnz, base, m->csr.rp, m->csr.ci, 8, bad);
   CELG_CUDA(cudaGetLastError());
   csr_check_rows_kernel<<<ew_grid(h, n + 1), 256, 0, h->stream>>>(n, nnz, m->csr.rp, bad);
   CELG_CUDA(cudaGetLastError());
@@ -431,17 +432,16 @@ extern "C" int celg_sm_count(celg_handle* h, int* sms) {
 // matrix
 // ---------------------------------------------------------------------------
 
-extern "C" int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr,
-                                 const int* cols, const double* vals, int index_base,
-                                 celg_mat** out) {
-  if (!h || !out || n < 0 || nnz < 0 || !row_ptr || (nnz > 0 && (!cols || !vals)) ||
+static int mat_upload(celg_handle* h, int n, int ncols, int nnz, const int* row_ptr,
+                      const int* cols, const double* vals, int index_base, celg_mat** out) {
+  if (!h || !out || n < 0 || ncols < n || nnz < 0 || !row_ptr || (nnz > 0 && (!cols || !vals)) ||
       (index_base != 0 && index_base != 1))
     return CELG_ERR_ARG;
   *out = nullptr;
   CELG_CUDA(cudaSetDevice(h->device));
   celg_mat* m = new celg_mat();
   m->h = h;
-  int st = alloc_csr(m, n, nnz);
+  int st = alloc_csr(m, n, nnz, ncols);
   if (!st) {
     cudaError_t e = cudaMemcpyAsync(m->csr.rp, row_ptr, sizeof(int) * ((size_t)n + 1),
                                     cudaMemcpyHostToDevice, h->stream);
@@ -462,6 +462,18 @@ extern "C" int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_
   return CELG_OK;
 }
 
+extern "C" int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr,
+                                 const int* cols, const double* vals, int index_base,
+                                 celg_mat** out) {
+  return mat_upload(h, n, n, nnz, row_ptr, cols, vals, index_base, out);
+}
+
+extern "C" int celg_mat_from_csr_ext(celg_handle* h, int n, int ncols, int nnz, const int* row_ptr,
+                                     const int* cols, const double* vals, int index_base,
+                                     celg_mat** out) {
+  return mat_upload(h, n, ncols, nnz, row_ptr, cols, vals, index_base, out);
+}
+
 extern "C" int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_d,
                                         const int* cols_d, const double* vals_d, celg_mat** out) {
   if (!h || !out || n < 0 || nnz < 0 || !row_ptr_d || (nnz > 0 && (!cols_d || !vals_d)))
@@ -470,7 +482,7 @@ extern "C" int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const in
   CELG_CUDA(cudaSetDevice(h->device));
   celg_mat* m = new celg_mat();
   m->h = h;
-  int st = alloc_csr(m, n, nnz);
+  int st = alloc_csr(m, n, nnz, n);
   if (!st) {
     cudaError_t e = cudaMemcpyAsync(m->csr.rp, row_ptr_d, sizeof(int) * ((size_t)n + 1),
                                     cudaMemcpyDeviceToDevice, h->stream);
@@ -519,7 +531,7 @@ extern "C" int celg_mat_info(const celg_mat* m, int* n, int* nnz, int* jad_mmax)
 }
 
 extern "C" int celg_mat_to_jad(celg_mat* m, int* perm_out) {
-  if (!m) return CELG_ERR_ARG;
+  if (!m || m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(m->h->device));
   int st = build_jad(m);
   if (st) return st;
@@ -558,7 +570,7 @@ extern "C" int celg_mat_get_jacobi(const celg_mat* m, double* jacobi_host) {
 }
 
 extern "C" int celg_mat_scale_diagonal(celg_mat* m) {
-  if (!m) return CELG_ERR_ARG;
+  if (!m || m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
   if (m->scaled) return CELG_OK;
   CELG_CUDA(cudaSetDevice(m->h->device));
   m->scaled = false;
@@ -576,7 +588,7 @@ extern "C" int celg_mat_scale_diagonal(celg_mat* m) {
 }
 
 extern "C" int celg_mat_make_fp32(celg_mat* m) {
-  if (!m) return CELG_ERR_ARG;
+  if (!m || m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(m->h->device));
   if (!m->csr.v32) {
     CELG_CUDA(cudaMalloc(&m->csr.v32, sizeof(float) * ((size_t)m->csr.nnz + 32)));
@@ -660,6 +672,7 @@ static int check_solve_args(celg_handle* h, celg_mat* m, const double* b, double
   if (p->fmt != CELG_FMT_CSR && p->fmt != CELG_FMT_JAD) return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER) return CELG_ERR_ARG;
   if (m->h != h) return CELG_ERR_ARG;
+  if (m->csr.ncols != m->csr.n) return CELG_ERR_ARG;  // row blocks: celg_dist_* only
   return CELG_OK;
 }
 

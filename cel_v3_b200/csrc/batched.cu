@@ -305,6 +305,7 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
   bt->NT = N / kTile;
   CsrDev& A = bt->A;
   A.n = (int)N;
+  A.ncols = (int)N;
   A.nnz = (int)NNZ;
   cudaError_t e = cudaSuccess;
   auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
@@ -515,6 +516,8 @@ extern "C" int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats
                                 celg_result* res) {
   if (!h || count <= 0 || !mats || !b_d || !x_d || !p) return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0) return CELG_ERR_ARG;
+  for (int s = 0; s < count; ++s)
+    if (mats[s] && mats[s]->csr.ncols != mats[s]->csr.n) return CELG_ERR_ARG;  // square systems only
   CELG_CUDA(cudaSetDevice(h->device));
   return celg::pcg_batched(h, count, mats, b_d, x_d, p, res);
 }

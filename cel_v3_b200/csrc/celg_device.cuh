@@ -212,6 +212,30 @@ __device__ __forceinline__ bool grid_finish(const RedCtx& red, double (&tot)[NRE
   return tid == 0;
 }
 
+// Last-block-done completion without partials (an op with no reduction that
+// still needs one thread to run after every CTA has read its inputs).
+// Returns true in lane 0 of the CTA that finished last.
+__device__ __forceinline__ bool grid_last(unsigned* ticket, int* s_flag, int tid, int bar_id) {
+  if (tid == 0) {
+    __threadfence();
+    unsigned tk = atomicAdd(ticket, 1u);
+    *s_flag = (tk == gridDim.x - 1) ? 1 : 0;
+  }
+  named_bar_sync(bar_id, kLanes);
+  if (*s_flag == 0) return false;
+  __threadfence();
+  if (tid == 0) *ticket = 0u;
+  return tid == 0;
+}
+
+// An op with NRED == 0 and `static constexpr bool kFinishAlways = true`
+// gets finish(nullptr) from the last CTA.
+template <class T, class = void>
+struct finishes_always : std::false_type {};
+template <class T>
+struct finishes_always<T, std::void_t<decltype(T::kFinishAlways)>>
+    : std::integral_constant<bool, T::kFinishAlways> {};
+
 // ---- batched solves --------------------------------------------------------
 //
 // An epilogue/op with `static constexpr bool kBatched = true` runs over the

@@ -18,6 +18,8 @@ namespace celg {
 struct CsrDev {
   int n = 0;
   int nnz = 0;
+  int ncols = 0;          // n, or more for a row block with halo columns
+
   int* rp = nullptr;
   int* ci = nullptr;
   double* v = nullptr;

@@ -1,0 +1,407 @@
+// dist.cu -- the local sweeps of a Jacobi-PCG solve whose rows are split into
+// blocks over ranks (one GPU each), with the caller running the exchange
+// steps between them.
+//
+// The multi-process path of cel_cgalg_jacobi (src/fcgalg/cel_cgalg_module.f90:
+// 178-305) does, per iteration, a halo exchange of p before the SpMV
+// (src/fspmtdistr/cel_sp_mat_distr_vec_module.f90:265-724) and one
+// MPI_Allreduce per global scalar (src/fop/cel_fop_vec_distr_module.f90:
+// 419-832).  Here each rank holds its rows with halo columns appended after
+// the local ones (celg_mat_from_csr_ext), and the phases below are stream-
+// ordered kernels that read the all-reduced scalars from a small device
+// buffer: no host synchronisation inside the loop, so a caller can queue the
+// collectives (NCCL, or MPI on device memory) on the same stream and capture
+// whole iterations in a CUDA graph.
+//
+// Exchange buffer: CELG_DIST_NEXCH doubles at the start of the state.  Every
+// phase that produces partial sums overwrites all of them (its own sums, 0
+// elsewhere; the last one is this rank's error flag), so the caller's rule is
+// uniform: after begin, init, ap, update and verify, sum-all-reduce the whole
+// buffer.  The scalars of the recurrence are computed from the reduced values
+// identically on every rank, so every rank takes the same number of steps.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "pcg_internal.cuh"
+
+namespace celg {
+
+struct DistState {
+  double xch[CELG_DIST_NEXCH];  // [b.b | r.z | r.r | p.v | error flag]
+  double alpha, sigma, beta, norm, bnorm, eps;
+  int iter, active, err, hist_len;
+};
+static_assert(sizeof(DistState) <= CELG_DIST_STATE_BYTES, "state buffer too small");
+
+enum { X_BB = 0, X_RZ = 1, X_RR = 2, X_PV = 3, X_ERR = 4 };
+
+struct DistArgs {
+  DistState* st;
+  double* hist;
+  int hist_cap;
+  int iter_max;
+  const int* errw;  // this rank's device error word (bounded waits)
+};
+
+__device__ __forceinline__ void xch_store(DistState* st, const DistArgs& a, double s0, double s1,
+                                          double s2, double s3) {
+  st->xch[X_BB] = s0;
+  st->xch[X_RZ] = s1;
+  st->xch[X_RR] = s2;
+  st->xch[X_PV] = s3;
+  st->xch[X_ERR] = (st->err != 0 || *(volatile const int*)a.errw != 0) ? 1.0 : 0.0;
+}
+
+__device__ __forceinline__ int dist_go(const DistState* st, int iter_max) {
+  return (st->err == 0 && st->iter < iter_max && fabs(st->alpha) > kRealSmall &&
+          st->norm > st->eps)
+             ? 1
+             : 0;
+}
+
+// begin: x0 on the local rows, local b.b
+struct DOpPre {
+  static constexpr int NRED = 1;
+  struct Regs { double b; };
+  const double* b;
+  double* x;
+  int x0_mode;
+  DistArgs a;
+  __device__ bool prepare() { return true; }
+  __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    if (x0_mode == CELG_X0_REF_ONES) x[i] = 1.0;
+    else if (x0_mode == CELG_X0_ZERO) x[i] = 0.0;
+    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+  }
+  __device__ void finish(double* tot) const {
+    DistState* st = a.st;
+    st->err = 0;
+    st->iter = 0;
+    st->active = 1;
+    st->alpha = st->sigma = st->beta = st->norm = 0.0;
+    xch_store(st, a, tot[0], 0.0, 0.0, 0.0);
+  }
+};
+
+// init (after the b.b reduction and the halo of x): r = b - A x, p = J r,
+// local r.p and r.r; ||b|| and eps from the reduced b.b
+struct DEpiInit {
+  static constexpr int NRED = 2;
+  const double* b;
+  double* r;
+  double* p;
+  const double* J;
+  double eps_abs, eps_rel;
+  DistArgs a;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    r[i] = ri;
+    const double z = dmul(ri, J[i]);
+    p[i] = z;
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const {
+    DistState* st = a.st;
+    st->bnorm = sqrt(st->xch[X_BB]);
+    double e = eps_abs;
+    if (eps_rel > 0.0 && eps_rel * st->bnorm > e) e = eps_rel * st->bnorm;
+    st->eps = e;
+    if (st->xch[X_ERR] != 0.0) st->err = kErrTimeout;
+    xch_store(st, a, 0.0, tot[0], tot[1], 0.0);
+  }
+};
+
+// start (after the r.p / r.r reduction): alpha, ||r||, the first test
+__global__ void dist_start_kernel(DistArgs a) {
+  DistState* st = a.st;
+  st->alpha = st->xch[X_RZ];
+  st->norm = sqrt(st->xch[X_RR]);
+  if (st->xch[X_ERR] != 0.0 && st->err == 0) st->err = kErrTimeout;
+  st->iter = 0;
+  if (a.hist && a.hist_cap > 0) a.hist[0] = st->norm;
+  st->hist_len = 1;
+  st->active = dist_go(st, a.iter_max);
+}
+
+// ap (after the halo of p): v = 0 + A p, local p.v
+struct DEpiAp {
+  static constexpr int NRED = 1;
+  double* v;
+  const double* p;
+  DistArgs a;
+  __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double vi = dadd(0.0, s);
+    v[i] = vi;
+    acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
+  }
+  __device__ void finish(double* tot) const { xch_store(a.st, a, 0.0, 0.0, 0.0, tot[0]); }
+};
+
+// update (after the p.v reduction): sigma = alpha / p.v; x += sigma p;
+// r += (-sigma) v; local r.z and r.r with z = J r
+struct DOpUpdate {
+  static constexpr int NRED = 2;
+  struct Regs { double x, r, p, v, J; };
+  double* x;
+  double* r;
+  const double* p;
+  const double* v;
+  const double* J;
+  DistArgs a;
+  double sg;
+  bool ok;
+  __device__ bool prepare() {
+    const DistState* st = a.st;
+    if (*(volatile const int*)&st->active == 0) return false;
+    sg = st->alpha / st->xch[X_PV];
+    ok = isfinite(sg) && st->xch[X_ERR] == 0.0;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const {
+    g.x = x[i];
+    g.r = r[i];
+    g.p = __ldg(p + i);
+    g.v = __ldg(v + i);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    if (!ok) return;
+    x[i] = dadd(g.x, dmul(sg, g.p));
+    const double ri = dadd(g.r, dmul(-sg, g.v));
+    r[i] = ri;
+    const double z = dmul(ri, g.J);
+    acc[0] = dadd(acc[0], dmul(ri, z));
+    acc[1] = dadd(acc[1], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const {
+    DistState* st = a.st;
+    if (!ok) {
+      if (st->err == 0) st->err = st->xch[X_ERR] != 0.0 ? kErrTimeout : kErrBreakdown;
+      st->active = 0;
+    }
+    st->sigma = sg;
+    xch_store(st, a, 0.0, tot[0], tot[1], 0.0);
+  }
+};
+
+// direction (after the r.z / r.r reduction): beta = r.z / alpha;
+// p = beta p + J r; then alpha = r.z, ||r||, iteration count and the test
+// (by the last CTA, after every CTA has read the old alpha)
+struct DOpDirection {
+  static constexpr int NRED = 0;
+  static constexpr bool kFinishAlways = true;
+  struct Regs { double p, r, J; };
+  double* p;
+  const double* r;
+  const double* J;
+  DistArgs a;
+  double bt;
+  __device__ bool prepare() {
+    const DistState* st = a.st;
+    if (*(volatile const int*)&st->active == 0) return false;
+    bt = st->xch[X_RZ] / st->alpha;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  __device__ void compute(long i, Regs& g, double*) const {
+    p[i] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
+  }
+  __device__ void finish(double*) const {
+    DistState* st = a.st;
+    if (st->xch[X_ERR] != 0.0 && st->err == 0) st->err = kErrTimeout;
+    st->beta = bt;
+    st->alpha = st->xch[X_RZ];
+    st->norm = sqrt(st->xch[X_RR]);
+    st->iter += 1;
+    if (a.hist && st->iter < a.hist_cap) a.hist[st->iter] = st->norm;
+    st->hist_len = st->iter + 1;
+    st->active = dist_go(st, a.iter_max);
+  }
+};
+
+// verify (after the halo of x): local ||b - A x||^2
+struct DEpiVerify {
+  static constexpr int NRED = 1;
+  const double* b;
+  DistArgs a;
+  __device__ bool active() const { return true; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish(double* tot) const { xch_store(a.st, a, tot[0], 0.0, 0.0, 0.0); }
+};
+
+}  // namespace celg
+
+using namespace celg;
+
+struct celg_dist {
+  celg_handle* h = nullptr;
+  celg_mat* m = nullptr;
+  DistState* st = nullptr;
+  bool own_state = false;
+  double* hist = nullptr;
+  int hist_cap = 0;
+  celg_params p{};
+  DistState* host = nullptr;  // pinned mirror for poll/result
+  DistArgs args() const { return DistArgs{st, hist, hist_cap, p.iter_max, h->err_d}; }
+};
+
+static int dist_check(const celg_dist* d) {
+  if (!d || !d->h || !d->m) return CELG_ERR_ARG;
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* p, void* state_d,
+                                double* hist_d, int hist_cap, celg_dist** out) {
+  if (!h || !m || !p || !out || m->h != h || hist_cap < 0 || (hist_cap > 0 && !hist_d))
+    return CELG_ERR_ARG;
+  if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0)
+    return CELG_ERR_ARG;
+  if (p->fmt != CELG_FMT_CSR || p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
+  if (m->csr.n <= 0) return CELG_ERR_ARG;  // every rank holds at least one row
+  if (!m->jacobi) return CELG_ERR_STATE;
+  if (state_d && (reinterpret_cast<uintptr_t>(state_d) & 15)) return CELG_ERR_ARG;
+  *out = nullptr;
+  CELG_CUDA(cudaSetDevice(h->device));
+  celg_dist* d = new celg_dist();
+  d->h = h;
+  d->m = m;
+  d->p = *p;
+  d->hist = hist_cap > 0 ? hist_d : nullptr;
+  d->hist_cap = hist_cap;
+  cudaError_t e = cudaSuccess;
+  if (state_d) {
+    d->st = static_cast<DistState*>(state_d);
+  } else {
+    e = cudaMalloc(&d->st, CELG_DIST_STATE_BYTES);
+    d->own_state = e == cudaSuccess;
+  }
+  if (e == cudaSuccess) e = cudaMallocHost(&d->host, sizeof(DistState));
+  if (e == cudaSuccess) e = cudaMemsetAsync(d->st, 0, sizeof(DistState), h->stream);
+  if (e != cudaSuccess) {
+    if (d->own_state) cudaFree(d->st);
+    if (d->host) cudaFreeHost(d->host);
+    delete d;
+    return cuda_status(e, "celg_dist_create");
+  }
+  *out = d;
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_destroy(celg_dist* d) {
+  if (!d) return CELG_OK;
+  cudaSetDevice(d->h->device);
+  cudaStreamSynchronize(d->h->stream);
+  if (d->own_state) cudaFree(d->st);
+  cudaFreeHost(d->host);
+  delete d;
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_exchange_buffer(celg_dist* d, double** xch_d) {
+  if (dist_check(d) || !xch_d) return CELG_ERR_ARG;
+  *xch_d = d->st->xch;
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_pcg_begin(celg_dist* d, const double* b_d, double* x_ext_d) {
+  if (dist_check(d) || !b_d || !x_ext_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  return launch_tile(d->h, d->m->csr.n, DOpPre{b_d, x_ext_d, d->p.x0_mode, d->args()});
+}
+
+extern "C" int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double* x_ext_d,
+                                  double* r_d, double* p_ext_d) {
+  if (dist_check(d) || !b_d || !x_ext_d || !r_d || !p_ext_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  const CsrDev& A = d->m->csr;
+  DEpiInit epi{b_d, r_d, p_ext_d, d->m->jacobi, d->p.eps_abs, d->p.eps_rel, d->args()};
+  return launch_csr<double>(d->h, A, A.v, x_ext_d, epi);
+}
+
+extern "C" int celg_dist_pcg_start(celg_dist* d) {
+  if (dist_check(d)) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  dist_start_kernel<<<1, 1, 0, d->h->stream>>>(d->args());
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d) {
+  if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  const CsrDev& A = d->m->csr;
+  return launch_csr<double>(d->h, A, A.v, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
+}
+
+extern "C" int celg_dist_pcg_update(celg_dist* d, double* x_ext_d, double* r_d,
+                                    const double* p_ext_d, const double* v_d) {
+  if (dist_check(d) || !x_ext_d || !r_d || !p_ext_d || !v_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  DOpUpdate op{x_ext_d, r_d, p_ext_d, v_d, d->m->jacobi, d->args(), 0.0, true};
+  return launch_tile(d->h, d->m->csr.n, op);
+}
+
+extern "C" int celg_dist_pcg_direction(celg_dist* d, const double* r_d, double* p_ext_d) {
+  if (dist_check(d) || !r_d || !p_ext_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  DOpDirection op{p_ext_d, r_d, d->m->jacobi, d->args(), 0.0};
+  return launch_tile(d->h, d->m->csr.n, op);
+}
+
+extern "C" int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const double* x_ext_d) {
+  if (dist_check(d) || !b_d || !x_ext_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  const CsrDev& A = d->m->csr;
+  return launch_csr<double>(d->h, A, A.v, x_ext_d, DEpiVerify{b_d, d->args()});
+}
+
+static int dist_fetch(celg_dist* d) {
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  CELG_CUDA(cudaMemcpyAsync(d->host, d->st, sizeof(DistState), cudaMemcpyDeviceToHost, d->h->stream));
+  CELG_CUDA(cudaStreamSynchronize(d->h->stream));
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_pcg_poll(celg_dist* d, int* active, int* iter) {
+  if (dist_check(d)) return CELG_ERR_ARG;
+  int st = dist_fetch(d);
+  if (st) return st;
+  if (active) *active = d->host->active;
+  if (iter) *iter = d->host->iter;
+  return CELG_OK;
+}
+
+extern "C" int celg_dist_pcg_result(celg_dist* d, celg_result* res) {
+  if (dist_check(d)) return CELG_ERR_ARG;
+  int st = dist_fetch(d);
+  if (st) return st;
+  const DistState& s = *d->host;
+  int ret = CELG_OK;
+  if (s.err) ret = s.err;
+  else if (s.xch[X_ERR] != 0.0) ret = CELG_ERR_TIMEOUT;
+  else if (!(s.norm <= s.eps) && s.iter >= d->p.iter_max && std::fabs(s.alpha) > kRealSmall)
+    ret = CELG_ERR_NOCONV;
+  if (res) {
+    res->iter_done = s.iter;
+    res->final_norm2 = s.norm;
+    res->bnorm = s.bnorm;
+    res->verified_relres = s.bnorm > 0.0 ? std::sqrt(s.xch[X_BB]) / s.bnorm : std::sqrt(s.xch[X_BB]);
+    res->err = ret;
+    res->arnoldi_steps = 0;
+    res->history_len = 0;
+    if (res->history && res->history_cap > 0 && d->hist) {
+      const int len = std::min(std::min(s.hist_len, d->hist_cap), res->history_cap);
+      CELG_CUDA(cudaMemcpy(res->history, d->hist, sizeof(double) * (size_t)len, cudaMemcpyDeviceToHost));
+      res->history_len = len;
+    }
+  }
+  return ret;
+}

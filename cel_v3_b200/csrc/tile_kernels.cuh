@@ -56,9 +56,11 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   }
   if constexpr (kB) {
     batch_grid_done(red, op, &s_flag, j, 1);
-  } else if (NR > 0) {
+  } else if constexpr (NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, &s_flag, j, 1)) op.finish(tot);
+  } else if constexpr (finishes_always<Op>::value) {
+    if (grid_last(red.ticket, &s_flag, j, 1)) op.finish(nullptr);
   }
 }
 

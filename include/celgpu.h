@@ -108,6 +108,14 @@ int celg_sm_count(celg_handle* h, int* sms);
  * Host arrays are copied; the caller keeps ownership. */
 int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr, const int* cols,
                       const double* vals, int index_base, celg_mat** out);
+/* One rank's row block of a matrix distributed by rows (the reference's
+ * vtxdist blocks, src/fspmtdistr/cel_sp_mat_distr_module.f90:330-339): n local
+ * rows whose columns 0..n-1 are the local rows and n..ncols-1 the halo values
+ * received from other ranks.  Usable with celg_spmv (x of ncols entries),
+ * celg_mat_jacobi and the celg_dist_* solver below; the single-system solvers
+ * reject it (CELG_ERR_ARG). */
+int celg_mat_from_csr_ext(celg_handle* h, int n, int ncols, int nnz, const int* row_ptr,
+                          const int* cols, const double* vals, int index_base, celg_mat** out);
 /* same with device arrays (0-based), copied device to device */
 int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_d,
                              const int* cols_d, const double* vals_d, celg_mat** out);
@@ -223,6 +231,55 @@ int celg_pcg_adjoint(celg_handle* h, celg_mat* m, const double* x_d, const doubl
  * with shapes (nz, ny, nx+1), (nz, ny+1, nx), (nz+1, ny, nx). */
 int celg_diffusion7_face_grad(celg_handle* h, int nx, int ny, int nz, const double* lambda_d,
                               const double* x_d, double* gkx_d, double* gky_d, double* gkz_d);
+
+/* ---- distributed Jacobi-PCG (one row block per rank) ------------------------------ */
+/* The multi-process form of cel_cgalg_jacobi (src/fcgalg/cel_cgalg_module.f90:
+ * 178-305): per iteration a halo exchange of p before the SpMV
+ * (src/fspmtdistr/cel_sp_mat_distr_vec_module.f90:265-724) and sum-allreduces
+ * of the dot products (src/fop/cel_fop_vec_distr_module.f90:419-832).  The
+ * library runs the local sweeps as stream-ordered kernels; the caller runs the
+ * exchanges (NCCL, CUDA-aware MPI, ...) on the handle's stream between them.
+ * Nothing synchronises the host except _poll and _result, so iterations can be
+ * queued back to back or captured in a CUDA graph together with the caller's
+ * collectives.
+ *
+ * Vectors: b_d, r_d, v_d have n entries; x_ext_d and p_ext_d have ncols
+ * entries (local part first, halo after).  The exchange buffer holds
+ * CELG_DIST_NEXCH doubles on the device; each phase marked [R] below
+ * overwrites all of them with this rank's partial sums, and the caller then
+ * sum-all-reduces the whole buffer before the next phase.  Sequence:
+ *   begin [R]; halo(x); init [R]; start;
+ *   repeat: halo(p); ap [R]; update [R]; direction;    (until poll says done)
+ *   halo(x); verify [R]; result.
+ * Iterations queued after convergence do no work (their exchanges still run,
+ * identically on every rank).  Every rank reaches the same decisions because
+ * they are taken from the reduced values only; a bounded-wait timeout on any
+ * rank is reduced with the sums and stops all ranks.
+ * state_d: CELG_DIST_STATE_BYTES of 16-byte aligned device memory owned by
+ * the caller (exchange buffer at its start), or NULL to let the library
+ * allocate it.  hist_d: device array of hist_cap doubles for ||r|| per
+ * iteration, or NULL.  params: x0_mode, eps_abs, eps_rel, iter_max (FP64
+ * CSR only). */
+#define CELG_DIST_NEXCH 5
+#define CELG_DIST_STATE_BYTES 256
+typedef struct celg_dist celg_dist;
+int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* p, void* state_d,
+                     double* hist_d, int hist_cap, celg_dist** out);
+int celg_dist_destroy(celg_dist* d);
+int celg_dist_exchange_buffer(celg_dist* d, double** xch_d);
+int celg_dist_pcg_begin(celg_dist* d, const double* b_d, double* x_ext_d);            /* [R] */
+int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double* x_ext_d, double* r_d,
+                       double* p_ext_d);                                              /* [R] */
+int celg_dist_pcg_start(celg_dist* d);
+int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d);               /* [R] */
+int celg_dist_pcg_update(celg_dist* d, double* x_ext_d, double* r_d, const double* p_ext_d,
+                         const double* v_d);                                          /* [R] */
+int celg_dist_pcg_direction(celg_dist* d, const double* r_d, double* p_ext_d);
+/* synchronises the stream; active = 0 once the loop has ended */
+int celg_dist_pcg_poll(celg_dist* d, int* active, int* iter);
+int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const double* x_ext_d);      /* [R] */
+/* synchronises; returns the solve status, fills res (history from hist_d) */
+int celg_dist_pcg_result(celg_dist* d, celg_result* res);
 
 /* ---- allocation-free entry point ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

@@ -1,0 +1,131 @@
+"""Distributed Jacobi-PCG phases (celg_dist_*) on one GPU.
+
+Several ranks are emulated in this process: each rank's kernels run in turn
+on the one device, and LocalComm sums the exchange buffers in rank order and
+copies the halos (no kernel waits on another rank's).  Checked bit for bit
+against the CPU mirror of the same ranks, and -- for one rank -- against the
+single-system solve.  The last test runs one rank through torch.distributed
+with NCCL (world size 1) to check the stream ordering of the collectives."""
+import numpy as np
+import pytest
+
+from cel_v3_b200 import dist as D
+from cel_v3_b200 import synth
+from oracle import celref as R
+from tests import dist_mirror as M
+from tests.helpers import random_csr, spd_from_pattern
+
+pytestmark = pytest.mark.gpu
+
+GRID = (20, 18, 16)
+
+
+def poisson():
+    rp, ci, v = synth.poisson7(*GRID)
+    xt = np.random.default_rng(12).random(rp.size - 1)
+    return rp, ci, v, R.spmv_csr(rp, ci, v, xt)
+
+
+def random_spd(n=5000, seed=8):
+    rp, ci, v = spd_from_pattern(*random_csr(n, np.random.default_rng(seed), max_len=7,
+                                             empty_frac=0.0))
+    return rp, ci, v, np.random.default_rng(seed + 1).uniform(-1, 1, n)
+
+
+def blocks_of(rp, ci, v, world, align):
+    bounds = D.partition(rp.size - 1, world, align)
+    return [D.RowBlock(rp, ci, v, bounds, q) for q in range(world)]
+
+
+def run_gpu(h, blocks, b, comm=None, **kw):
+    ranks = [D.GpuRank(h, blk, b[blk.r0:blk.r1], history=True, **kw) for blk in blocks]
+    try:
+        res = D.run_pcg(ranks, comm or D.LocalComm(), check_every=5)
+        x = np.concatenate([r.x().cpu().numpy() for r in ranks])
+    finally:
+        for r in ranks:
+            r.close()
+    return x, res
+
+
+def run_cpu(blocks, b, **kw):
+    ranks = [M.CpuRank(blk, b[blk.r0:blk.r1], **kw) for blk in blocks]
+    res = D.run_pcg(ranks, D.LocalComm(), check_every=5)
+    return np.concatenate([r.x() for r in ranks]), res
+
+
+def test_one_rank_equals_single_system_solve(gpu):
+    celgpu, h, torch = gpu
+    rp, ci, v, b = poisson()
+    x, (res,) = run_gpu(h, blocks_of(rp, ci, v, 1, 1), b, eps_rel=1e-8, iter_max=1000)
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+    info = h.pcg_jacobi(m, bd.data_ptr(), xd.data_ptr(), history=True, eps_rel=1e-8, iter_max=1000)
+    m.destroy()
+    assert res.status == celgpu.OK and info.status == celgpu.OK
+    assert res.iter_done == info.iter_done
+    assert np.array_equal(res.history, info.history)
+    assert np.array_equal(x, xd.cpu().numpy())
+    assert res.verified_relres == info.verified_relres
+
+
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_emulated_slab_ranks_match_cpu_mirror(gpu, world):
+    celgpu, h, torch = gpu
+    rp, ci, v, b = poisson()
+    blocks = blocks_of(rp, ci, v, world, GRID[0] * GRID[1])
+    x, res = run_gpu(h, blocks, b, eps_rel=1e-8, iter_max=1000)
+    xc, rc = run_cpu(blocks, b, eps_rel=1e-8, iter_max=1000)
+    assert all(r.status == celgpu.OK for r in res)
+    assert len({r.iter_done for r in res}) == 1
+    assert res[0].iter_done == rc[0]["iter_done"]
+    assert np.array_equal(res[0].history, rc[0]["history"])
+    assert np.array_equal(x, xc)
+    assert res[0].verified_relres == rc[0]["verified_relres"]
+    assert res[0].verified_relres <= 1.5e-8
+
+
+def test_emulated_general_partition_user_start(gpu):
+    """Unaligned blocks of an unstructured matrix (scattered send lists),
+    a user start vector and an iteration cap."""
+    celgpu, h, torch = gpu
+    rp, ci, v, b = random_spd()
+    blocks = blocks_of(rp, ci, v, 3, 1)
+    x0 = np.random.default_rng(2).random(rp.size - 1)
+    kw = dict(eps_rel=1e-30, iter_max=12)
+    ranks = [D.GpuRank(h, blk, b[blk.r0:blk.r1], x0=x0[blk.r0:blk.r1], history=True, **kw)
+             for blk in blocks]
+    res = D.run_pcg(ranks, D.LocalComm(), check_every=4)
+    x = np.concatenate([r.x().cpu().numpy() for r in ranks])
+    for r in ranks:
+        r.close()
+    xc, rc = run_cpu(blocks, b, x0=x0, **kw)
+    assert all(r.status == celgpu.ERR_NOCONV and r.iter_done == 12 for r in res)
+    assert np.array_equal(x, xc)
+    assert np.array_equal(res[0].history, rc[0]["history"])
+
+
+def test_nccl_world_one(gpu):
+    """One rank over torch.distributed with NCCL: the collectives queue on
+    torch's stream between the phases; same bits as the single solve."""
+    celgpu, h, torch = gpu
+    import socket
+    from datetime import timedelta
+
+    import torch.distributed as td
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    td.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                          timeout=timedelta(seconds=60))
+    try:
+        rp, ci, v, b = poisson()
+        x, (res,) = run_gpu(h, blocks_of(rp, ci, v, 1, 1), b, comm=D.TorchComm(), eps_rel=1e-8,
+                            iter_max=1000)
+    finally:
+        td.destroy_process_group()
+    xl, (rl,) = run_gpu(h, blocks_of(rp, ci, v, 1, 1), b, eps_rel=1e-8, iter_max=1000)
+    assert res.status == celgpu.OK
+    assert res.iter_done == rl.iter_done
+    assert np.array_equal(x, xl)
