@@ -103,8 +103,14 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
   }
 }
 
-// ---- SpMM with a fused per-row epilogue (matrix read straight from global:
-// the k-wide gathers dominate the traffic, the matrix is 12 nnz bytes) ------
+// ---- SpMM with a fused per-row epilogue ---------------------------------------
+// A warp takes its 32 rows as one run of stored entries: 32 entries at a time
+// are loaded coalesced (column index and value per lane) and broadcast by
+// shuffles, so each lane has 32 independent k-wide gathers of X in flight
+// before it adds them up.  Row sums still run over each row's entries in
+// stored order from 0.0, and rows are finished in order; the epilogue's own
+// operands for a row (Epi::Pre) are loaded when the row starts, so their
+// latency overlaps the gathers.
 template <class Epi>
 __global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp,
                                                       const int* __restrict__ ci,
@@ -112,6 +118,7 @@ __global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp
                                                       const double* __restrict__ X, Epi epi,
                                                       RedCtx red) {
   constexpr int NR = Epi::NRED;
+  constexpr unsigned kFull = 0xffffffffu;
   __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
   __shared__ double scratch[8];
   __shared__ double s_tot[(NR > 0 ? NR : 1) * kMaxRhs];
@@ -125,26 +132,46 @@ __global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
     for (int q = 0; q < 4; ++q) {
-      for (int r = 0; r < 32; ++r) {
-        const long row = t * kTile + q * kSub + warp * 32 + r;
-        if (row >= n) break;
-        const int b = __ldg(rp + row), e = __ldg(rp + row + 1);
-        double sum = 0.0;
-        for (int kk = b; kk < e; kk += 8) {
-          double xv[8], vv[8];
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      if (row0 >= n) break;
+      const int nrows = (int)min(32L, (long)n - row0);
+      const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
+      const int e0 = __ldg(rp + row0);
+      const int e1 = __shfl_sync(kFull, re, nrows - 1);
+      int cur = 0;
+      int bnd = __shfl_sync(kFull, re, 0);
+      typename Epi::Pre pre;
+      if (on) pre = epi.pre(row0, lane);
+      double sum = 0.0;
+      for (int c0 = e0; c0 < e1; c0 += 32) {
+        const int cnt = min(32, e1 - c0);
+        const int cc = lane < cnt ? __ldg(ci + c0 + lane) : 0;
+        const double cv = lane < cnt ? __ldg(v + c0 + lane) : 0.0;
+        double xv[32];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            if (kk + u < e) {
-              vv[u] = __ldg(v + kk + u);
-              const int c = __ldg(ci + kk + u);
-              xv[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u)
-            if (kk + u < e) sum = dadd(sum, dmul(vv[u], xv[u]));
+        for (int j = 0; j < 32; ++j) {
+          const int col = __shfl_sync(kFull, cc, j);
+          xv[j] = (on && j < cnt) ? __ldg(X + (long)col * k + lane) : 0.0;
         }
-        if (on) epi.row(row, lane, sum, acc);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const double val = __shfl_sync(kFull, cv, j);
+          if (j < cnt) {
+            while (c0 + j >= bnd) {  // rows ending before this entry (empty rows too)
+              if (on) epi.row(row0 + cur, lane, sum, pre, acc);
+              sum = 0.0;
+              ++cur;
+              bnd = __shfl_sync(kFull, re, cur);
+              if (on) pre = epi.pre(row0 + cur, lane);
+            }
+            sum = dadd(sum, dmul(val, xv[j]));
+          }
+        }
+      }
+      for (; cur < nrows; ++cur) {  // the last non-empty row and empty rows after it
+        if (on) epi.row(row0 + cur, lane, sum, pre, acc);
+        sum = 0.0;
+        if (on && cur + 1 < nrows) pre = epi.pre(row0 + cur + 1, lane);
       }
     }
     if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
@@ -231,13 +258,15 @@ struct MEpiInit {
   const double* J;
   int k;
   MultiArgs a;
+  struct Pre { double b, J; };
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
-  __device__ void row(long i, int c, double s, double* acc) const {
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c), __ldg(J + i)}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const long e = i * k + c;
-    const double ri = __dsub_rn(B[e], dadd(0.0, s));
+    const double ri = __dsub_rn(g.b, dadd(0.0, s));
     R[e] = ri;
-    const double z = dmul(ri, __ldg(J + i));
+    const double z = dmul(ri, g.J);
     P[e] = z;
     acc[0] = dadd(acc[0], dmul(ri, z));
     acc[1] = dadd(acc[1], dmul(ri, ri));
@@ -259,12 +288,13 @@ struct MEpiAp {
   int k;
   MultiArgs a;
   __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
+  struct Pre { double p; };
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
-  __device__ void row(long i, int c, double s, double* acc) const {
-    const long e = i * k + c;
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(P + i * k + c)}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const double vi = dadd(0.0, s);
-    V[e] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, __ldg(P + e)));
+    V[i * k + c] = vi;
+    acc[0] = dadd(acc[0], dmul(vi, g.p));
   }
   __device__ void finish_col(int c, double* tot) const {
     if (!a.active[c]) return;
@@ -345,10 +375,12 @@ struct MEpiVerify {
   const double* B;
   int k;
   MultiArgs a;
+  struct Pre { double b; };
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
-  __device__ void row(long i, int c, double s, double* acc) const {
-    const double ri = __dsub_rn(B[i * k + c], dadd(0.0, s));
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c)}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
+    const double ri = __dsub_rn(g.b, dadd(0.0, s));
     acc[0] = dadd(acc[0], dmul(ri, ri));
   }
   __device__ void finish_col(int c, double* tot) const {

@@ -48,8 +48,9 @@ def run_gpu(h, blocks, b, comm=None, **kw):
     return x, res
 
 
-def run_cpu(blocks, b, **kw):
-    ranks = [M.CpuRank(blk, b[blk.r0:blk.r1], **kw) for blk in blocks]
+def run_cpu(blocks, b, x0=None, **kw):
+    ranks = [M.CpuRank(blk, b[blk.r0:blk.r1], x0=None if x0 is None else x0[blk.r0:blk.r1], **kw)
+             for blk in blocks]
     res = D.run_pcg(ranks, D.LocalComm(), check_every=5)
     return np.concatenate([r.x() for r in ranks]), res
 
