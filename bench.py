@@ -14,8 +14,11 @@ Also reported on the same line:
   e2e           the same solves through the reference-facing ELM interface
                 (celg_elm_doit + celg_elm_collect_solution: b copied from
                 pinned host memory, x copied back) inside the timed region
-  forms         FP32-storage refinement to rel-res 1e-10 and plain FP64 PCG
-                to 1e-10 on the same system (solves/s of each)
+  forms         the other configurations, each against its plain FP64
+                counterpart on the GPU: FP32 refinement on the 256^3
+                lognormal-coefficient diffusion system (rel-res 1e-10), 64
+                batched uneven systems, 32 right-hand sides on 128^3, and the
+                adjoint gradients of a batch of 8 128^3 diffusion solves
   cpu_baseline  the C restatement of the reference's MPI+OpenMP PCG (oracle/)
                 on the host cores, on a bounded sample of iterations
 
@@ -131,6 +134,43 @@ def build_problem():
     return rp, ci, v, x_true
 
 
+def precision_form(h, celgpu, torch, stream, side=256, reps=2):
+    """-div(k grad u) on side^3, k = exp(g), g ~ N(0,1) per face (seed 2),
+    b ~ U[-1,1) (seed 3), assembled in device memory: plain FP64 PCG, FP32
+    refinement (restarted inner PCG, inner tol 1e-4) and FP32 PCG with FP64
+    reliable updates, each to FP64-verified rel-res 1e-10."""
+    from cel_v3_b200 import synth
+    g, _ = synth.lognormal_faces(np.random.default_rng(2), side, side, side)
+    rp_d, ci_d, v_d = synth.diffusion7_device(side, side, side, np.exp(g))
+    n, nnz = side ** 3, int(ci_d.numel())
+    m = h.matrix_from_csr_device(n, nnz, rp_d.data_ptr(), ci_d.data_ptr(), v_d.data_ptr()).jacobi()
+    del rp_d, ci_d, v_d
+    b = torch.from_numpy(np.random.default_rng(3).uniform(-1.0, 1.0, n)).cuda()
+    x = torch.zeros_like(b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"rows": n, "nnz": nnz, "rel_res": 1e-10}
+    for name, kw in (("fp64_pcg", dict()),
+                     ("fp32_ir", dict(precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4)),
+                     ("fp32_ru", dict(precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2))):
+        pf = celgpu.params(eps_rel=1e-10, iter_max=20000, x0_mode=celgpu.X0_ZERO, **kw)
+        h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            inf = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fms = e0.elapsed_time(e1) / reps
+        out[name] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
+                     "inner_iters": inf.arnoldi_steps, "verified_relres": inf.verified_relres,
+                     "status": inf.status}
+    base = out["fp64_pcg"]["solves_per_s"]
+    for k in ("fp32_ir", "fp32_ru"):
+        out[k]["speedup_vs_fp64"] = out[k]["solves_per_s"] / base
+    m.destroy()
+    return out
+
+
 def batch_form(h, celgpu, torch, stream):
     """64 variable-coefficient systems (sides 16..96, seed 4) to rel-res 1e-8:
     one batched launch against the plain path solving them one by one."""
@@ -205,6 +245,97 @@ def multirhs_form(h, celgpu, torch, stream):
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     m.destroy()
     return out
+
+
+def differentiation_form(h, celgpu, torch, stream, side=128, batch=8, fd_dirs=64, step=1e-6):
+    """Gradients of L = 0.5 ||x - x_target||^2, x = A(k)^{-1} b, k = exp(g) per
+    face of a side^3 7-point diffusion operator, for `batch` instances (seeds
+    6 and 7): one batched forward solve, one batched adjoint solve
+    (A lambda = x - x_target; A is symmetric), the face gradients
+    dL/dk = -(lambda_i - lambda_j)(x_i - x_j) (boundary: -lambda_i x_i) and
+    dL/dg = k dL/dk.  Checked by central differences of L along random unit
+    directions of g (instance 0), each perturbed operator rebuilt in device
+    memory from the face map."""
+    from cel_v3_b200 import synth
+    probs = synth.differentiation_problems(side, batch)
+    n = side ** 3
+    cx, cy, cz = synth.face_counts(side, side, side)
+    eps = 1e-10
+    p = celgpu.params(eps_rel=eps, iter_max=20000, x0_mode=celgpu.X0_ZERO)
+    # finite differences resolve 1e-6 steps only with tighter solves
+    p_fd = celgpu.params(eps_rel=1e-13, iter_max=20000, x0_mode=celgpu.X0_ZERO)
+
+    def operator(g_d):
+        rp_d, ci_d, v_d = synth.diffusion7_device(side, side, side, torch.exp(g_d))
+        return h.matrix_from_csr_device(n, int(ci_d.numel()), rp_d.data_ptr(), ci_d.data_ptr(),
+                                        v_d.data_ptr()).jacobi()
+
+    gs = [torch.from_numpy(g).cuda() for g, _, _ in probs]
+    bs = [torch.from_numpy(b).cuda() for _, b, _ in probs]
+    xts = [torch.from_numpy(xt).cuda() for _, _, xt in probs]
+    mats = [operator(g) for g in gs]
+    xs = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in probs]
+    lams = [torch.zeros_like(x) for x in xs]
+    gks = [torch.zeros(cx + cy + cz, dtype=torch.float64, device="cuda") for _ in probs]
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+
+    def forward():
+        return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p)
+
+    def backward():
+        rhs = [x - xt for x, xt in zip(xs, xts)]
+        infos = h.pcg_batched(mats, [r.data_ptr() for r in rhs], [l.data_ptr() for l in lams], p)
+        for lam, x, gk in zip(lams, xs, gks):
+            h.diffusion7_face_grad(side, side, side, lam.data_ptr(), x.data_ptr(), gk.data_ptr(),
+                                   gk[cx:].data_ptr(), gk[cx + cy:].data_ptr())
+        return infos, [torch.exp(g) * gk for g, gk in zip(gs, gks)]
+
+    forward()
+    backward()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fi = forward()
+    e1.record(stream)
+    bi, dLdg = backward()
+    e2.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    def loss(g_d, b_d, xt_d):
+        m = operator(g_d)
+        x = torch.zeros(n, dtype=torch.float64, device="cuda")
+        info = h.pcg_jacobi(m, b_d.data_ptr(), x.data_ptr(), p_fd)
+        m.destroy()
+        return 0.5 * float(((x - xt_d) ** 2).sum()), info
+
+    rng = np.random.default_rng(64)
+    g0, b0, xt0, d0 = gs[0], bs[0], xts[0], dLdg[0]
+    scale = float(d0.abs().max())
+    errs = []
+    for _ in range(fd_dirs):
+        d = torch.from_numpy(rng.standard_normal(g0.numel())).cuda()
+        d /= torch.linalg.vector_norm(d)
+        lp, _ = loss(g0 + step * d, b0, xt0)
+        lm, _ = loss(g0 - step * d, b0, xt0)
+        fd = (lp - lm) / (2 * step)
+        errs.append(abs(fd - float(d0 @ d)) / max(abs(fd), scale))
+    e = torch.from_numpy(rng.standard_normal(n)).cuda()
+    e /= torch.linalg.vector_norm(e)
+    lp, _ = loss(g0, b0 + step * e, xt0)
+    lm, _ = loss(g0, b0 - step * e, xt0)
+    db_err = abs((lp - lm) / (2 * step) - float(lams[0] @ e)) / float(lams[0].abs().max())
+    for m in mats:
+        m.destroy()
+    return {"instances": batch, "rows_per_instance": n, "faces_per_instance": cx + cy + cz,
+            "rel_res": eps, "fd_rel_res": 1e-13, "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "backward_over_forward": bwd_ms / fwd_ms,
+            "gradients_per_s": batch * 1e3 / (fwd_ms + bwd_ms),
+            "forward_max_iters": max(i.iter_done for i in fi),
+            "adjoint_max_iters": max(i.iter_done for i in bi),
+            "all_ok": all(i.status == celgpu.OK for i in list(fi) + list(bi)),
+            "fd_check": {"directions": fd_dirs, "step": step,
+                         "max_rel_err_dLdg": max(errs), "rel_err_dLdb": db_err,
+                         "scale": "max(|fd|, max|dL/dg|)"}}
 
 
 def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
@@ -364,29 +495,10 @@ def run_gpu(args):
     # ---- other precision forms on the same system (reported, not the value) ----
     forms = {}
     if not args.quick:
-        for name, kw in (("fp64_pcg_1e-10", dict(eps_rel=1e-10)),
-                         ("fp32_ir_1e-10", dict(eps_rel=1e-10, precision=celgpu.PREC_FP32_IR,
-                                                inner_eps_rel=1e-4)),
-                         ("fp32_ru_1e-10", dict(eps_rel=1e-10, precision=celgpu.PREC_FP32_RU,
-                                                inner_eps_rel=1e-2))):
-            pf = celgpu.params(iter_max=5000, x0_mode=celgpu.X0_ZERO, **kw)
-            h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
-            torch.cuda.synchronize()
-            e0.record(stream)
-            k = 3
-            for _ in range(k):
-                inf = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            fms = e0.elapsed_time(e1) / k
-            forms[name] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
-                           "inner_iters": inf.arnoldi_steps, "verified_relres": inf.verified_relres,
-                           "status": inf.status}
-        base = forms["fp64_pcg_1e-10"]["solves_per_s"]
-        for k in ("fp32_ir_1e-10", "fp32_ru_1e-10"):
-            forms[k]["speedup_vs_fp64_at_1e-10"] = forms[k]["solves_per_s"] / base
+        forms["precision_diffusion256"] = precision_form(h, celgpu, torch, stream)
         forms["batched_64"] = batch_form(h, celgpu, torch, stream)
         forms["multirhs_128_k32"] = multirhs_form(h, celgpu, torch, stream)
+        forms["differentiation_128_b8"] = differentiation_form(h, celgpu, torch, stream)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))

@@ -154,3 +154,66 @@ def multirhs_problem(side=128, k=32, seed=5):
     rp, ci, v = poisson7(side)
     B = np.random.default_rng(seed).uniform(-1.0, 1.0, (side ** 3, k))
     return rp, ci, v, B
+
+
+def differentiation_problems(side=128, batch=8):
+    """`batch` instances of the gradient workload on a side^3 grid: per
+    instance g ~ N(0,1) per face (drawn in order from default_rng(6)), then
+    b ~ U[-1,1) and x_target ~ U[0,1) (drawn in order from default_rng(7))."""
+    r6, r7 = np.random.default_rng(6), np.random.default_rng(7)
+    cx, cy, cz = face_counts(side, side, side)
+    n = side ** 3
+    out = []
+    for _ in range(batch):
+        g = r6.standard_normal(cx + cy + cz)
+        b = r7.uniform(-1.0, 1.0, n)
+        xt = r7.random(n)
+        out.append((g, b, xt))
+    return out
+
+
+def diffusion7_device(nx, ny, nz, k, device="cuda"):
+    """The diffusion7 assembly computed with torch on `device` (same entry
+    order and the same additions for the diagonal, so the values equal the
+    host assembly's bit for bit): k is the concatenated per-face coefficient
+    vector (x-, y-, z-faces) as a float64 tensor or array.  Returns int32
+    row pointers, int32 columns and float64 values on the device."""
+    import torch
+    k = torch.as_tensor(k, dtype=torch.float64, device=device)
+    cx, cy, cz = face_counts(nx, ny, nz)
+    n, nxy = nx * ny * nz, nx * ny
+    idx = torch.arange(n, dtype=torch.int64, device=device)
+    x, y, z = idx % nx, (idx // nx) % ny, idx // nxy
+    west = (z * ny + y) * (nx + 1) + x
+    south = cx + (z * (ny + 1) + y) * nx + x
+    bottom = cx + cy + (z * ny + y) * nx + x
+    kw, ke = k[west], k[west + 1]
+    ks, kn = k[south], k[south + nx]
+    kb, kt = k[bottom], k[bottom + nxy]
+    diag = ((((kw + ke) + ks) + kn) + kb) + kt
+    present = [z > 0, y > 0, x > 0, None, x < nx - 1, y < ny - 1, z < nz - 1]
+    offsets = [-nxy, -nx, -1, 0, 1, nx, nxy]
+    vals = [-kb, -ks, -kw, diag, -ke, -kn, -kt]
+    counts = torch.ones(n, dtype=torch.int64, device=device)
+    for m in present:
+        if m is not None:
+            counts += m
+    rp = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    torch.cumsum(counts, 0, out=rp[1:])
+    nnz = int(rp[-1])
+    if nnz >= 2**31:
+        raise ValueError("nnz does not fit int32 indices")
+    ci = torch.empty(nnz, dtype=torch.int32, device=device)
+    v = torch.empty(nnz, dtype=torch.float64, device=device)
+    pos = rp[:-1].clone()
+    for m, off, val in zip(present, offsets, vals):
+        if m is None:
+            ci[pos] = (idx + off).to(torch.int32)
+            v[pos] = val
+            pos += 1
+        else:
+            p = pos[m]
+            ci[p] = (idx[m] + off).to(torch.int32)
+            v[p] = val[m]
+            pos += m
+    return rp.to(torch.int32), ci, v
