@@ -122,10 +122,12 @@ struct BEpiAp {
   __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
   __device__ void begin_tile(long) {}
   __device__ const BatchRed& bred() const { return a.br; }
-  __device__ void row(long i, double s, double* acc) const {
+  struct Pre { double p; };
+  __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
+  __device__ void row(long i, double s, const Pre& g, double* acc) const {
     const double vi = dadd(0.0, s);
     v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
+    acc[0] = dadd(acc[0], dmul(vi, g.p));
   }
   __device__ void finish_sys(int s, double* tot) const {
     const double sg = a.alpha[s] / tot[0];

@@ -104,27 +104,15 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
 }
 
 // ---- SpMM with a fused per-row epilogue ---------------------------------------
-// A warp takes its 32 rows as one run of stored entries: 32 entries at a time
-// are loaded coalesced (column index and value per lane) and broadcast by
-// shuffles, so each lane has 32 independent k-wide gathers of X in flight
-// before it adds them up.  Row sums still run over each row's entries in
-// stored order from 0.0, and rows are finished in order.  The epilogue's own
-// operands for the warp's 32 rows (a contiguous run of 32 k values, plus one
-// value per row) are copied into the warp's shared-memory slice with
-// cp.async when the group starts, so that load overlaps the gathers.
-__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-// cnt consecutive doubles from global memory into a warp's staging slice
-__device__ __forceinline__ void stage_run(double* st, const double* g, int cnt, int lane) {
-  for (int q = lane; q < cnt; q += 32) cp_async8(st + q, g + q);
-}
-// staging slice per warp: 32 rows x k operands, then 32 per-row operands
-__host__ __device__ constexpr int stage_doubles(int k) { return 32 * k + 32; }
-
+// Warp w takes rows in order; lane c owns column c, so each stored entry is
+// one k-wide (k*8-byte contiguous) gather of X.  A row's entries are read in
+// chunks of 8 whose gathers are all issued before the first add (the adds stay
+// in stored order from 0.0).  The row ends of the warp's 32 rows are held one
+// per lane and shuffled out, and the epilogue's operands for the next row
+// (Epi::Pre) are loaded before the current row's gathers, so the only memory
+// latency left on a row's path is its gathers.
 template <class Epi>
-__global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp,
+__global__ void __launch_bounds__(kLanes, 3) spmm_kernel(const int* __restrict__ rp,
                                                       const int* __restrict__ ci,
                                                       const double* __restrict__ v, int n, int k,
                                                       const double* __restrict__ X, Epi epi,
@@ -135,11 +123,9 @@ __global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp
   __shared__ double scratch[8];
   __shared__ double s_tot[(NR > 0 ? NR : 1) * kMaxRhs];
   __shared__ int s_flag;
-  extern __shared__ __align__(16) double s_stage[];
   if (!epi.active()) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const bool on = lane < k && epi.col_active(lane);
-  double* st = s_stage + warp * stage_doubles(k);
   const long ntiles = ((long)n + kTile - 1) / kTile;
   for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     double acc[NR > 0 ? NR : 1];
@@ -149,45 +135,32 @@ __global__ void __launch_bounds__(kLanes) spmm_kernel(const int* __restrict__ rp
       const long row0 = t * kTile + q * kSub + warp * 32;
       if (row0 >= n) break;
       const int nrows = (int)min(32L, (long)n - row0);
-      __syncwarp();  // the previous group's rows are finished with st
-      epi.stage(row0, nrows, lane, st);
       const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
-      const int e0 = __ldg(rp + row0);
-      const int e1 = __shfl_sync(kFull, re, nrows - 1);
-      int cur = 0;
-      int bnd = __shfl_sync(kFull, re, 0);
-      double sum = 0.0;
-      for (int c0 = e0; c0 < e1; c0 += 32) {
-        const int cnt = min(32, e1 - c0);
-        const int cc = lane < cnt ? __ldg(ci + c0 + lane) : 0;
-        const double cv = lane < cnt ? __ldg(v + c0 + lane) : 0.0;
-        double xv[32];
+      int b = __ldg(rp + row0);
+      typename Epi::Pre pre_next;
+      if (on) pre_next = epi.pre(row0, lane);
+      for (int r = 0; r < nrows; ++r) {
+        const long row = row0 + r;
+        const int e = __shfl_sync(kFull, re, r);
+        const typename Epi::Pre pre = pre_next;
+        if (on && r + 1 < nrows) pre_next = epi.pre(row + 1, lane);
+        double sum = 0.0;
+        for (int kk = b; kk < e; kk += 8) {
+          double xv[8], vv[8];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = __shfl_sync(kFull, cc, j);
-          xv[j] = (on && j < cnt) ? __ldg(X + (long)col * k + lane) : 0.0;
-        }
-        cp_async_wait_all();
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const double val = __shfl_sync(kFull, cv, j);
-          if (j < cnt) {
-            while (c0 + j >= bnd) {  // rows ending before this entry (empty rows too)
-              if (on) epi.row(row0 + cur, cur, lane, sum, st, acc);
-              sum = 0.0;
-              ++cur;
-              bnd = __shfl_sync(kFull, re, cur);
+          for (int u = 0; u < 8; ++u) {
+            if (kk + u < e) {
+              vv[u] = __ldg(v + kk + u);
+              const int c = __ldg(ci + kk + u);
+              xv[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
             }
-            sum = dadd(sum, dmul(val, xv[j]));
           }
+#pragma unroll
+          for (int u = 0; u < 8; ++u)
+            if (kk + u < e) sum = dadd(sum, dmul(vv[u], xv[u]));
         }
-      }
-      cp_async_wait_all();
-      __syncwarp();
-      for (; cur < nrows; ++cur) {  // the last non-empty row and empty rows after it
-        if (on) epi.row(row0 + cur, cur, lane, sum, st, acc);
-        sum = 0.0;
+        if (on) epi.row(row, lane, sum, pre, acc);
+        b = e;
       }
     }
     if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
@@ -274,17 +247,15 @@ struct MEpiInit {
   const double* J;
   int k;
   MultiArgs a;
+  struct Pre { double b, J; };
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
-  __device__ void stage(long row0, int nrows, int lane, double* st) const {
-    stage_run(st, B + row0 * k, nrows * k, lane);
-    if (lane < nrows) cp_async8(st + 32 * k + lane, J + row0 + lane);
-  }
-  __device__ void row(long i, int r, int c, double s, const double* st, double* acc) const {
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c), __ldg(J + i)}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const long e = i * k + c;
-    const double ri = __dsub_rn(st[r * k + c], dadd(0.0, s));
+    const double ri = __dsub_rn(g.b, dadd(0.0, s));
     R[e] = ri;
-    const double z = dmul(ri, st[32 * k + r]);
+    const double z = dmul(ri, g.J);
     P[e] = z;
     acc[0] = dadd(acc[0], dmul(ri, z));
     acc[1] = dadd(acc[1], dmul(ri, ri));
@@ -306,14 +277,13 @@ struct MEpiAp {
   int k;
   MultiArgs a;
   __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
+  struct Pre { double p; };
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
-  __device__ void stage(long row0, int nrows, int lane, double* st) const {
-    stage_run(st, P + row0 * k, nrows * k, lane);
-  }
-  __device__ void row(long i, int r, int c, double s, const double* st, double* acc) const {
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(P + i * k + c)}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const double vi = dadd(0.0, s);
     V[i * k + c] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, st[r * k + c]));
+    acc[0] = dadd(acc[0], dmul(vi, g.p));
   }
   __device__ void finish_col(int c, double* tot) const {
     if (!a.active[c]) return;
@@ -394,13 +364,12 @@ struct MEpiVerify {
   const double* B;
   int k;
   MultiArgs a;
+  struct Pre { double b; };
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
-  __device__ void stage(long row0, int nrows, int lane, double* st) const {
-    stage_run(st, B + row0 * k, nrows * k, lane);
-  }
-  __device__ void row(long, int r, int c, double s, const double* st, double* acc) const {
-    const double ri = __dsub_rn(st[r * k + c], dadd(0.0, s));
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c)}; }
+  __device__ void row(long, int, double s, const Pre& g, double* acc) const {
+    const double ri = __dsub_rn(g.b, dadd(0.0, s));
     acc[0] = dadd(acc[0], dmul(ri, ri));
   }
   __device__ void finish_col(int c, double* tot) const {
@@ -414,13 +383,11 @@ static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, 
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
-  const int smem = 8 * stage_doubles(k) * (int)sizeof(double);
   auto kern = spmm_kernel<Epi>;
-  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
-  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
+  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, 0));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
-  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  kern<<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
 }

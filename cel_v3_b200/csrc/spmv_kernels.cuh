@@ -44,13 +44,21 @@ __device__ __forceinline__ int entry_col(uint8_t c, long row, const int* dict) {
 }
 constexpr int kCsrHeader = 256;  // mbarriers, stage meta, fold scratch
 
+// An epilogue may declare `struct Pre` and `Pre pre(long row) const`: the
+// consumer then loads the row's epilogue operands before its x gathers (so
+// both latencies overlap) and calls row(i, s, pre, acc).
+template <class E, class = void>
+struct has_pre : std::false_type {};
+template <class E>
+struct has_pre<E, std::void_t<typename E::Pre>> : std::true_type {};
+
 template <int N>
 struct Acc {
   double a[N > 0 ? N : 1];
 };
 
 template <typename VT, class Epi, typename CT = int>
-__global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
     csr_tma_kernel(const int* __restrict__ rp, const CT* __restrict__ ci,
                    const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
                    RedCtx red, int* err, const int* __restrict__ dict, int ndict) {
@@ -164,6 +172,10 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
       const int fb = meta[2 * st + 1];
       const long row = s * kSub + j;
       if (row < n) {
+        [[maybe_unused]] auto pr = [&] {
+          if constexpr (has_pre<Epi>::value) return ep.pre(row);
+          else return 0;
+        }();
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
         if (!fb) {
@@ -187,7 +199,8 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 3 : 2)
           for (int k = b; k < e; ++k)
             sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + entry_col(__ldg(ci + k), row, s_dict))));
         }
-        ep.row(row, sum, acc.a);
+        if constexpr (has_pre<Epi>::value) ep.row(row, sum, pr, acc.a);
+        else ep.row(row, sum, acc.a);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
@@ -245,8 +258,13 @@ __global__ void __launch_bounds__(kLanes)
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (i[k] < n) epi.row((long)__ldg(perm + i[k]), sum[k], acc.a);
+    for (int k = 0; k < 4; ++k) {
+      if (i[k] < n) {
+        const long row = (long)__ldg(perm + i[k]);
+        if constexpr (has_pre<Epi>::value) epi.row(row, sum[k], epi.pre(row), acc.a);
+        else epi.row(row, sum[k], acc.a);
+      }
+    }
     if (NR > 0) {
 #pragma unroll
       for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
