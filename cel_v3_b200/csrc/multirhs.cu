@@ -17,6 +17,7 @@
 //
 // Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 104 n k.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -105,18 +106,31 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
 
 // ---- SpMM with a fused per-row epilogue ---------------------------------------
 // Warp w takes rows in order; lane c owns column c, so each stored entry is
-// one k-wide (k*8-byte contiguous) gather of X.  A row's entries are read in
-// chunks of 8 whose gathers are all issued before the first add (the adds stay
-// in stored order from 0.0).  The row ends of the warp's 32 rows are held one
-// per lane and shuffled out, and the epilogue's operands for the next row
-// (Epi::Pre) are loaded before the current row's gathers, so the only memory
-// latency left on a row's path is its gathers.
-template <class Epi>
-__global__ void __launch_bounds__(kLanes, 3) spmm_kernel(const int* __restrict__ rp,
-                                                      const int* __restrict__ ci,
-                                                      const double* __restrict__ v, int n, int k,
-                                                      const double* __restrict__ X, Epi epi,
-                                                      RedCtx red) {
+// one k-wide (k*8-byte contiguous) gather of X.  Rows are software-pipelined
+// two deep: the gathers of row r+1's first 8 entries (and its epilogue
+// operands, Epi::Pre) are issued before row r is added up, so two rows'
+// gathers are in flight per warp.  A row's adds run over its entries in
+// stored order from 0.0 (entries past the first 8 are gathered in further
+// chunks of 8 when the row is added).  The row ends of the warp's 32 rows are
+// held one per lane and shuffled out.
+template <int U>
+__device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const double* __restrict__ X,
+                                            int b, int e, int k, int lane, bool on, double (&x)[U]) {
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (b + u < e) {
+      const int c = __ldg(ci + b + u);
+      x[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
+    }
+  }
+}
+
+template <class Epi, int MINB, int U>
+__global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restrict__ rp,
+                                                            const int* __restrict__ ci,
+                                                            const double* __restrict__ v, int n,
+                                                            int k, const double* __restrict__ X,
+                                                            Epi epi, RedCtx red) {
   constexpr int NR = Epi::NRED;
   constexpr unsigned kFull = 0xffffffffu;
   __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
@@ -136,31 +150,39 @@ __global__ void __launch_bounds__(kLanes, 3) spmm_kernel(const int* __restrict__
       if (row0 >= n) break;
       const int nrows = (int)min(32L, (long)n - row0);
       const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
-      int b = __ldg(rp + row0);
-      typename Epi::Pre pre_next;
-      if (on) pre_next = epi.pre(row0, lane);
+      int bA = __ldg(rp + row0);
+      int eA = __shfl_sync(kFull, re, 0);
+      double xA[U];
+      spmm_gather<U>(ci, X, bA, eA, k, lane, on, xA);
+      typename Epi::Pre preA;
+      if (on) preA = epi.pre(row0, lane);
       for (int r = 0; r < nrows; ++r) {
-        const long row = row0 + r;
-        const int e = __shfl_sync(kFull, re, r);
-        const typename Epi::Pre pre = pre_next;
-        if (on && r + 1 < nrows) pre_next = epi.pre(row + 1, lane);
-        double sum = 0.0;
-        for (int kk = b; kk < e; kk += 8) {
-          double xv[8], vv[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            if (kk + u < e) {
-              vv[u] = __ldg(v + kk + u);
-              const int c = __ldg(ci + kk + u);
-              xv[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < 8; ++u)
-            if (kk + u < e) sum = dadd(sum, dmul(vv[u], xv[u]));
+        const bool more = r + 1 < nrows;
+        const int bB = eA;
+        const int eB = __shfl_sync(kFull, re, more ? r + 1 : r);
+        double xB[U];
+        typename Epi::Pre preB;
+        if (more) {
+          spmm_gather<U>(ci, X, bB, eB, k, lane, on, xB);
+          if (on) preB = epi.pre(row0 + r + 1, lane);
         }
-        if (on) epi.row(row, lane, sum, pre, acc);
-        b = e;
+        double sum = 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (bA + u < eA) sum = dadd(sum, dmul(__ldg(v + bA + u), xA[u]));
+        for (int kk = bA + U; kk < eA; kk += U) {  // rows longer than U entries
+          double xv[U];
+          spmm_gather<U>(ci, X, kk, eA, k, lane, on, xv);
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (kk + u < eA) sum = dadd(sum, dmul(__ldg(v + kk + u), xv[u]));
+        }
+        if (on) epi.row(row0 + r, lane, sum, preA, acc);
+        bA = bB;
+        eA = eB;
+#pragma unroll
+        for (int u = 0; u < U; ++u) xA[u] = xB[u];
+        preA = preB;
       }
     }
     if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
@@ -378,18 +400,38 @@ struct MEpiVerify {
   __device__ void finish_global() const {}
 };
 
-template <class Epi>
-static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+// SpMM launch variants: the resident CTAs per SM the registers are budgeted
+// for, and the gather chunk width.  The fastest for a matrix and k is picked
+// by timing them (spmm_tune) before the first solve.
+struct SpmmCfg {
+  int minb, u;
+};
+constexpr SpmmCfg kSpmmCfgs[] = {{2, 8}, {3, 8}, {3, 4}, {4, 4}};
+constexpr int kSpmmNumCfgs = 4;
+
+template <class Epi, int MINB, int U>
+static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
-  auto kern = spmm_kernel<Epi>;
+  auto kern = spmm_kernel<Epi, MINB, U>;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, 0));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
   kern<<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
+}
+
+template <class Epi>
+static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi,
+                       int cfg) {
+  switch (cfg) {
+    case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, k, X, epi);
+    case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, k, X, epi);
+    case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, k, X, epi);
+    default: return launch_spmm_cfg<Epi, 4, 4>(h, A, k, X, epi);
+  }
 }
 
 template <class Op>
@@ -405,6 +447,9 @@ static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
 }  // namespace celg
 
 struct Multi {
+  // SpMM variant picked for the last (matrix, n, k) tuned
+  const void* tuned_mat = nullptr;
+  int tuned_n = -1, tuned_k = -1, cfg = 0;
   size_t cap = 0;        // n*k of the work vectors
   double* work = nullptr;  // R, P, V
   double* dstate = nullptr;
@@ -419,6 +464,36 @@ void multi_free(Multi* m) {
   cudaFree(m->dstate);
   cudaFree(m->istate);
   delete m;
+}
+
+// Times every SpMM variant (3 launches each after one warm-up) on this
+// matrix and k with the verification epilogue, which reads B and writes only
+// the per-column verification residual, and returns the fastest.  The
+// variant can be forced with CELG_SPMM_CFG=0..3 (profiling).
+static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, const MultiArgs& a,
+                     int* best) {
+  if (const char* e = std::getenv("CELG_SPMM_CFG")) {
+    *best = std::min(std::max(std::atoi(e), 0), kSpmmNumCfgs - 1);
+    return CELG_OK;
+  }
+  float best_ms = 0.f;
+  *best = 0;
+  for (int c = 0; c < kSpmmNumCfgs; ++c) {
+    int st = launch_spmm(h, A, k, B, MEpiVerify{B, k, a}, c);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    for (int r = 0; r < 3 && !st; ++r) st = launch_spmm(h, A, k, B, MEpiVerify{B, k, a}, c);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+    CELG_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CELG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (c == 0 || ms < best_ms) {
+      best_ms = ms;
+      *best = c;
+    }
+  }
+  return CELG_OK;
 }
 
 int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
@@ -461,19 +536,27 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   a.errw = h->err_d;
   a.cond = 0;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  if (mu->tuned_mat != (const void*)m || mu->tuned_n != (int)n || mu->tuned_k != k) {
+    st = spmm_tune(h, m->csr, k, B, a, &mu->cfg);
+    if (st) return st;
+    mu->tuned_mat = m;
+    mu->tuned_n = (int)n;
+    mu->tuned_k = k;
+  }
+  const int cfg = mu->cfg;
   auto setup = [&](const MultiArgs& ac) -> int {
     int s2 = launch_mtile(h, n, k, MOpPre{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
-    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit{B, R, P, m->jacobi, k, ac});
+    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit{B, R, P, m->jacobi, k, ac}, cfg);
     return s2;
   };
   auto body = [&](const MultiArgs& ac) -> int {
-    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac});
+    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac}, cfg);
     if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate{X, R, P, V, m->jacobi, ac, 0.0});
     if (!s3) s3 = launch_mtile(h, n, k, MOpDirection{P, R, m->jacobi, ac, 0.0});
     return s3;
   };
   auto tail = [&](const MultiArgs& ac) -> int {
-    return launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac});
+    return launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac}, cfg);
   };
   if (!graphs_enabled()) {
     // profiling mode: the same kernels from a host loop (see graph.cuh)
@@ -502,9 +585,9 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
       return s2;
     };
     char kb[256];
-    std::snprintf(kb, sizeof(kb), "mrhs|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%d", (const void*)m, m->csr.n, k,
-                  (const void*)B, (const void*)X, (const void*)R, p->x0_mode, p->eps_abs, p->eps_rel,
-                  p->iter_max);
+    std::snprintf(kb, sizeof(kb), "mrhs|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%d|%d", (const void*)m, m->csr.n,
+                  k, (const void*)B, (const void*)X, (const void*)R, p->x0_mode, p->eps_abs, p->eps_rel,
+                  p->iter_max, cfg);
     const std::string key(kb);
     GraphEntry* ge = graph_cache_find(h, key);
     if (!ge) {
