@@ -512,6 +512,7 @@ extern "C" int celg_mat_destroy(celg_mat* m) {
   cudaStreamSynchronize(h->stream);
   // cached solve graphs (and a cached batch) may reference this matrix
   graph_cache_drop_matrix(h, m);
+  multi_forget_matrix(h->multi, m);
   if (h->batch) {
     graph_cache_clear(h);
     batch_free(h->batch);

@@ -158,5 +158,6 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 int ensure_f32(celg_handle* h, size_t n);
 void batch_free(::Batch* b);
 void multi_free(::Multi* m);
+void multi_forget_matrix(::Multi* m, const void* mat);
 
 }  // namespace celg

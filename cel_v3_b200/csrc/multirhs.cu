@@ -113,6 +113,17 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
 // stored order from 0.0 (entries past the first 8 are gathered in further
 // chunks of 8 when the row is added).  The row ends of the warp's 32 rows are
 // held one per lane and shuffled out.
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+constexpr int kAsyncU = 8;                    // gathers per row slot
+constexpr int kAsyncSlot = (kAsyncU + 2) * 32;  // doubles per slot: U entries + 2 epilogue operands
+
 template <int U>
 __device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const double* __restrict__ X,
                                             int b, int e, int k, int lane, bool on, double (&x)[U]) {
@@ -184,6 +195,88 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restric
         for (int u = 0; u < U; ++u) xA[u] = xB[u];
         preA = preB;
       }
+    }
+    if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<(NR > 0 ? NR : 1)>(red, epi, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
+}
+
+// The same SpMM with the gathers issued as asynchronous copies into a ring of
+// S row slots per warp in shared memory (cp.async, 8 bytes per lane and
+// entry), so the data in flight does not occupy registers: rows r+1..r+S-1
+// are in flight while row r is added up.  Each lane copies and reads only its
+// own column of a slot, so the lanes need no barrier between them; the
+// epilogue's operands travel in the same slot (Epi::stage_pre / staged).
+template <class Epi, int S>
+__global__ void __launch_bounds__(kLanes) spmm_async_kernel(const int* __restrict__ rp,
+                                                           const int* __restrict__ ci,
+                                                           const double* __restrict__ v, int n,
+                                                           int k, const double* __restrict__ X,
+                                                           Epi epi, RedCtx red) {
+  constexpr int NR = Epi::NRED;
+  constexpr int U = kAsyncU;
+  constexpr int SLOT = kAsyncSlot;
+  constexpr unsigned kFull = 0xffffffffu;
+  __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[(NR > 0 ? NR : 1) * kMaxRhs];
+  __shared__ int s_flag;
+  extern __shared__ __align__(16) double s_ring[];
+  if (!epi.active()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const bool on = lane < k && epi.col_active(lane);
+  double* ring = s_ring + (long)warp * S * SLOT;
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      if (row0 >= n) break;
+      const int nrows = (int)min(32L, (long)n - row0);
+      const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
+      const int b0 = __ldg(rp + row0);
+      // issue row r's first U gathers and its epilogue operands into slot r % S
+      auto issue = [&](int r) {
+        const int b = r == 0 ? b0 : __shfl_sync(kFull, re, r > 0 ? r - 1 : 0);
+        const int e = __shfl_sync(kFull, re, r);
+        double* slot = ring + (r % S) * SLOT;
+        if (on) {
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (b + u < e) cp_async8(slot + u * 32 + lane, X + (long)__ldg(ci + b + u) * k + lane);
+          epi.stage_pre(row0 + r, lane, slot + U * 32);
+        }
+        cp_async_commit();
+      };
+      for (int r = 0; r < S - 1; ++r) {
+        if (r < nrows) issue(r);
+        else cp_async_commit();
+      }
+      int b = b0;
+      for (int r = 0; r < nrows; ++r) {
+        if (r + S - 1 < nrows) issue(r + S - 1);
+        else cp_async_commit();
+        cp_async_wait<S - 1>();
+        const int e = __shfl_sync(kFull, re, r);
+        const double* slot = ring + (r % S) * SLOT;
+        double sum = 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (b + u < e) sum = dadd(sum, dmul(__ldg(v + b + u), slot[u * 32 + lane]));
+        for (int kk = b + U; kk < e; kk += U) {  // rows longer than U entries
+          double xv[U];
+          spmm_gather<U>(ci, X, kk, e, k, lane, on, xv);
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (kk + u < e) sum = dadd(sum, dmul(__ldg(v + kk + u), xv[u]));
+        }
+        if (on) epi.row(row0 + r, lane, sum, epi.staged(slot + U * 32, lane), acc);
+        b = e;
+      }
+      cp_async_wait<0>();
     }
     if (NR > 0) multi_tile_store<(NR > 0 ? NR : 1)>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
   }
@@ -273,6 +366,11 @@ struct MEpiInit {
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
   __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c), __ldg(J + i)}; }
+  __device__ void stage_pre(long i, int c, double* st) const {
+    cp_async8(st + c, B + i * k + c);
+    cp_async8(st + 32 + c, J + i);
+  }
+  __device__ Pre staged(const double* st, int c) const { return Pre{st[c], st[32 + c]}; }
   __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const long e = i * k + c;
     const double ri = __dsub_rn(g.b, dadd(0.0, s));
@@ -302,6 +400,8 @@ struct MEpiAp {
   struct Pre { double p; };
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ Pre pre(long i, int c) const { return Pre{__ldg(P + i * k + c)}; }
+  __device__ void stage_pre(long i, int c, double* st) const { cp_async8(st + c, P + i * k + c); }
+  __device__ Pre staged(const double* st, int c) const { return Pre{st[c]}; }
   __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
     const double vi = dadd(0.0, s);
     V[i * k + c] = vi;
@@ -390,6 +490,8 @@ struct MEpiVerify {
   __device__ bool active() const { return true; }
   __device__ bool col_active(int) const { return true; }
   __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c)}; }
+  __device__ void stage_pre(long i, int c, double* st) const { cp_async8(st + c, B + i * k + c); }
+  __device__ Pre staged(const double* st, int c) const { return Pre{st[c]}; }
   __device__ void row(long, int, double s, const Pre& g, double* acc) const {
     const double ri = __dsub_rn(g.b, dadd(0.0, s));
     acc[0] = dadd(acc[0], dmul(ri, ri));
@@ -400,14 +502,12 @@ struct MEpiVerify {
   __device__ void finish_global() const {}
 };
 
-// SpMM launch variants: the resident CTAs per SM the registers are budgeted
-// for, and the gather chunk width.  The fastest for a matrix and k is picked
-// by timing them (spmm_tune) before the first solve.
-struct SpmmCfg {
-  int minb, u;
-};
-constexpr SpmmCfg kSpmmCfgs[] = {{2, 8}, {3, 8}, {3, 4}, {4, 4}};
-constexpr int kSpmmNumCfgs = 4;
+// SpMM launch variants: the register pipeline with the resident CTAs per SM
+// its registers are budgeted for and its gather chunk width (2/8, 3/8, 3/4,
+// 4/4), and the cp.async ring with 2, 3 or 4 row slots per warp.  The
+// fastest for a matrix and k is picked by timing them (spmm_tune) before the
+// first solve.
+constexpr int kSpmmNumCfgs = 7;  // 0-3 register pipeline, 4-6 cp.async ring
 
 template <class Epi, int MINB, int U>
 static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
@@ -423,6 +523,22 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double*
   return CELG_OK;
 }
 
+template <class Epi, int S>
+static int launch_spmm_async(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{h->partials, h->ticket, nt};
+  if (A.n == 0) return CELG_OK;
+  auto kern = spmm_async_kernel<Epi, S>;
+  const int smem = 8 * S * kAsyncSlot * (int)sizeof(double);
+  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
+  const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
+  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 template <class Epi>
 static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi,
                        int cfg) {
@@ -430,7 +546,10 @@ static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, 
     case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, k, X, epi);
     case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, k, X, epi);
     case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, k, X, epi);
-    default: return launch_spmm_cfg<Epi, 4, 4>(h, A, k, X, epi);
+    case 3: return launch_spmm_cfg<Epi, 4, 4>(h, A, k, X, epi);
+    case 4: return launch_spmm_async<Epi, 2>(h, A, k, X, epi);
+    case 5: return launch_spmm_async<Epi, 3>(h, A, k, X, epi);
+    default: return launch_spmm_async<Epi, 4>(h, A, k, X, epi);
   }
 }
 
@@ -458,6 +577,11 @@ struct Multi {
 
 namespace celg {
 
+// a destroyed matrix's address may be reused: drop its tuning record
+void multi_forget_matrix(Multi* m, const void* mat) {
+  if (m && m->tuned_mat == mat) m->tuned_mat = nullptr;
+}
+
 void multi_free(Multi* m) {
   if (!m) return;
   cudaFree(m->work);
@@ -469,7 +593,7 @@ void multi_free(Multi* m) {
 // Times every SpMM variant (3 launches each after one warm-up) on this
 // matrix and k with the verification epilogue, which reads B and writes only
 // the per-column verification residual, and returns the fastest.  The
-// variant can be forced with CELG_SPMM_CFG=0..3 (profiling).
+// variant can be forced with CELG_SPMM_CFG=0..6 (profiling).
 static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, const MultiArgs& a,
                      int* best) {
   if (const char* e = std::getenv("CELG_SPMM_CFG")) {

@@ -99,3 +99,25 @@ def test_multirhs_bitexact_and_close_to_single(gpu, case):
         assert abs(one.iter_done - infos[c].iter_done) <= 1
         assert np.abs(xs.cpu().numpy() - X[:, c]).max() <= 1e-9 * np.abs(X[:, c]).max()
     m.destroy()
+
+
+@pytest.mark.parametrize("cfg", range(7))
+def test_every_spmm_variant_is_bitexact(gpu, cfg, monkeypatch):
+    """Each launch variant the autotuner can pick (forced with
+    CELG_SPMM_CFG) gives the mirror's bits, including rows longer than the
+    gather chunk."""
+    celgpu, h, torch = gpu
+    monkeypatch.setenv("CELG_SPMM_CFG", str(cfg))
+    rng = np.random.default_rng(9)
+    from tests.helpers import random_csr, spd_from_pattern
+    rp, ci, v = spd_from_pattern(*random_csr(3000, rng, max_len=9, empty_frac=0.0, long_rows=3,
+                                             long_len=40))
+    n, k = rp.size - 1, 7
+    B = rng.uniform(-1.0, 1.0, (n, k))
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-10, iter_max=300)
+    Xo, ito, _ = mirror(rp, ci, v, B, 1e-10, 300)
+    m.destroy()
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == list(ito)
