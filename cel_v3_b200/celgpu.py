@@ -130,6 +130,9 @@ def _load():
         "celg_pcg_adjoint": (i, [vp, vp, vp, vp, vp, vp, ctypes.POINTER(Params), ctypes.POINTER(Result)]),
         "celg_diffusion7_face_grad": (i, [vp, i, i, i, vp, vp, vp, vp, vp]),
         "celg_mat_from_csr_ext": (i, [vp, i, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_mat_from_coo": (i, [vp, i, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_mm_info": (i, [ctypes.c_char_p, i, ip, ip, ip, ip]),
+        "celg_mm_read": (i, [ctypes.c_char_p, i, i, vp, vp, vp]),
         "celg_dist_create": (i, [vp, vp, ctypes.POINTER(Params), vp, vp, i, ctypes.POINTER(vp)]),
         "celg_dist_destroy": (i, [vp]),
         "celg_dist_exchange_buffer": (i, [vp, ctypes.POINTER(vp)]),
@@ -187,6 +190,24 @@ def dot_noalloc(n, a_d, b_d, out_d, stream=0):
     include/celgpu.h); returns the status code."""
     return lib.celg_dot_noalloc(int(n), ctypes.c_void_p(a_d), ctypes.c_void_p(b_d),
                                 ctypes.c_void_p(out_d), ctypes.c_void_p(int(stream)) if stream else None)
+
+
+MM_GENERAL, MM_SYMMETRIC, MM_SKEW = 0, 1, 2
+
+
+def mm_read(path, expand=False):
+    """MatrixMarket file -> (nrows, ncols, symmetry, rows, cols, vals), 1-based
+    entries as stored (celg_mm_info + celg_mm_read; host only)."""
+    p = str(path).encode()
+    nr, nc, nz, sy = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(lib.celg_mm_info(p, int(expand), ctypes.byref(nr), ctypes.byref(nc), ctypes.byref(nz),
+                            ctypes.byref(sy)), "celg_mm_info")
+    rows = np.zeros(nz.value, np.int32)
+    cols = np.zeros(nz.value, np.int32)
+    vals = np.zeros(nz.value, np.float64)
+    _check(lib.celg_mm_read(p, int(expand), nz.value, _host_ptr(rows), _host_ptr(cols),
+                            _host_ptr(vals)), "celg_mm_read")
+    return nr.value, nc.value, sy.value, rows, cols, vals
 
 
 DIST_NEXCH = 5
@@ -389,6 +410,20 @@ class Handle:
         _check(lib.celg_mat_from_csr(self.ptr, n, int(ci.size), _host_ptr(rp), _host_ptr(ci),
                                      _host_ptr(v), int(index_base), ctypes.byref(m)),
                "celg_mat_from_csr")
+        mat = Matrix(self, m)
+        self.mats.append(mat)
+        return mat
+
+    def matrix_from_coo(self, n, rows, cols, vals, index_base=0, ncols=None):
+        """COO triplets -> CSR on the device (celg_mat_from_coo)."""
+        rows = np.ascontiguousarray(rows, np.int32)
+        cols = np.ascontiguousarray(cols, np.int32)
+        vals = np.ascontiguousarray(vals, np.float64)
+        m = ctypes.c_void_p()
+        _check(lib.celg_mat_from_coo(self.ptr, int(n), int(n if ncols is None else ncols),
+                                     int(vals.size), _host_ptr(rows), _host_ptr(cols),
+                                     _host_ptr(vals), int(index_base), ctypes.byref(m)),
+               "celg_mat_from_coo")
         mat = Matrix(self, m)
         self.mats.append(mat)
         return mat

@@ -181,7 +181,7 @@ static int build_offset_dict(celg_handle* h, celg_mat* m) {
   return CELG_OK;
 }
 
-static void free_mat_arrays(celg_mat* m) {
+void free_mat_arrays(celg_mat* m) {
   cudaFree(m->csr.rp);
   cudaFree(m->csr.ci);
   cudaFree(m->csr.v);
@@ -199,7 +199,7 @@ static void free_mat_arrays(celg_mat* m) {
 }
 
 // Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.
-static int alloc_csr(celg_mat* m, int n, int nnz, int ncols) {
+int alloc_csr(celg_mat* m, int n, int nnz, int ncols) {
   m->csr.n = n;
   m->csr.nnz = nnz;
   m->csr.ncols = ncols;
@@ -211,7 +211,7 @@ static int alloc_csr(celg_mat* m, int n, int nnz, int ncols) {
   return CELG_OK;
 }
 
-static int finish_csr(celg_handle* h, celg_mat* m, int base) {
+int finish_csr(celg_handle* h, celg_mat* m, int base) {
   const int n = m->csr.n, nnz = m->csr.nnz;
   int* bad = h->err_d + 2;
   CELG_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int), h->stream));

@@ -156,6 +156,15 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
              celg_result* res);
 int ensure_f32(celg_handle* h, size_t n);
+// api.cu: matrix storage (alloc_csr leaves row_ptr/cols/vals for the caller
+// to fill; finish_csr shifts to 0-based, validates and sets the staging cap)
+int alloc_csr(celg_mat* m, int n, int nnz, int ncols);
+int finish_csr(celg_handle* h, celg_mat* m, int base);
+void free_mat_arrays(celg_mat* m);
+// assemble.cu: COO (device arrays, row and column bases) -> CSR matrix
+int coo_to_mat_device(celg_handle* h, int n, int ncols, int nnz, const int* rows_d,
+                      const int* cols_d, const double* vals_d, int row_base, int col_base,
+                      celg_mat** out);
 void batch_free(::Batch* b);
 void multi_free(::Multi* m);
 void multi_forget_matrix(::Multi* m, const void* mat);

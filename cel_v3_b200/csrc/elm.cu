@@ -156,38 +156,38 @@ extern "C" int celg_elm_insert_rows(celg_handle* h, int first_row, int nrows, co
 
 // cel_elmSolverMatrixCompleted (:193-439) for one rank: entries sorted by
 // row, then column (cel_sp_mat_format_sparse_31_sort,
-// src/fspmt/cel_sp_mat_module.f90:518-585; equal keys keep insertion order),
-// CSR row pointer (cel_sp_mat_to_csr, :430-456), upload, Jacobi, optional
-// diagonal scaling (:375-388 of the ELM module), JAD when selected.
+// src/fspmt/cel_sp_mat_module.f90:518-585; equal keys keep insertion order)
+// and the CSR row pointer (cel_sp_mat_to_csr, :430-456), both on the device;
+// then Jacobi, optional diagonal scaling (:375-388 of the ELM module), JAD
+// when selected.
 extern "C" int celg_elm_matrix_completed(celg_handle* h) {
   if (!h || !h->elm) return CELG_ERR_STATE;
   Elm* e = h->elm;
   if (e->completed) return CELG_ERR_STATE;
   const size_t nnz = e->vals.size();
   if (nnz >= (size_t)1 << 31) return CELG_ERR_ARG;
-  bool sorted = true;
-  for (size_t k = 1; k < nnz && sorted; ++k)
-    sorted = e->rows[k - 1] < e->rows[k] ||
-             (e->rows[k - 1] == e->rows[k] && e->cols[k - 1] <= e->cols[k]);
-  std::vector<int> rp((size_t)e->n_local + 1, 0), ci(nnz);
-  std::vector<double> v(nnz);
-  std::vector<size_t> order;
-  if (!sorted) {
-    order.resize(nnz);
-    std::iota(order.begin(), order.end(), (size_t)0);
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-      return e->rows[a] < e->rows[b] || (e->rows[a] == e->rows[b] && e->cols[a] < e->cols[b]);
-    });
-  }
-  for (size_t k = 0; k < nnz; ++k) {
-    const size_t s = sorted ? k : order[k];
-    ci[k] = e->cols[s] - 1;
-    v[k] = e->vals[s];
-    rp[(size_t)(e->rows[s] - e->row_low) + 1]++;
-  }
-  for (int i = 0; i < e->n_local; ++i) rp[(size_t)i + 1] += rp[(size_t)i];
+  // the triplets go to the device as inserted; the stable (row, column) sort
+  // and the row pointer are built there (assemble.cu)
+  const size_t nz = std::max<size_t>(nnz, 1);
+  int *r_d = nullptr, *c_d = nullptr;
+  double* v_d = nullptr;
+  cudaError_t ce = cudaMalloc(&r_d, sizeof(int) * nz);
+  if (ce == cudaSuccess) ce = cudaMalloc(&c_d, sizeof(int) * nz);
+  if (ce == cudaSuccess) ce = cudaMalloc(&v_d, sizeof(double) * nz);
+  if (ce == cudaSuccess && nnz)
+    ce = cudaMemcpyAsync(r_d, e->rows.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, h->stream);
+  if (ce == cudaSuccess && nnz)
+    ce = cudaMemcpyAsync(c_d, e->cols.data(), sizeof(int) * nnz, cudaMemcpyHostToDevice, h->stream);
+  if (ce == cudaSuccess && nnz)
+    ce = cudaMemcpyAsync(v_d, e->vals.data(), sizeof(double) * nnz, cudaMemcpyHostToDevice, h->stream);
   celg_mat* m = nullptr;
-  int st = celg_mat_from_csr(h, e->n_local, (int)nnz, rp.data(), ci.data(), v.data(), 0, &m);
+  int st = ce == cudaSuccess ? coo_to_mat_device(h, e->n_local, e->n_local, (int)nnz, r_d, c_d, v_d,
+                                                 e->row_low, 1, &m)
+                             : cuda_status(ce, "ELM triplet upload");
+  cudaStreamSynchronize(h->stream);
+  cudaFree(r_d);
+  cudaFree(c_d);
+  cudaFree(v_d);
   if (st) return st;
   st = celg_mat_jacobi(m);
   if (!st && e->diag_scaling) st = celg_mat_scale_diagonal(m);

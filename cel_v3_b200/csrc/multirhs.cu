@@ -591,22 +591,29 @@ void multi_free(Multi* m) {
 }
 
 // Times every SpMM variant (3 launches each after one warm-up) on this
-// matrix and k with the verification epilogue, which reads B and writes only
-// the per-column verification residual, and returns the fastest.  The
-// variant can be forced with CELG_SPMM_CFG=0..6 (profiling).
-static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, const MultiArgs& a,
-                     int* best) {
+// matrix and k with the iteration's own epilogue (v = A p with the per-column
+// p.v), applied to B with the output in a work vector; the per-column state
+// is set up first by MOpPre in the user-start mode, which leaves X alone, and
+// the solve's own set-up overwrites everything the timing wrote.  Returns the
+// fastest variant; CELG_SPMM_CFG=0..6 forces one (profiling).
+static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, double* X,
+                     double* work, const MultiArgs& a, int* best) {
   if (const char* e = std::getenv("CELG_SPMM_CFG")) {
     *best = std::min(std::max(std::atoi(e), 0), kSpmmNumCfgs - 1);
     return CELG_OK;
   }
+  int st = launch_mtile(h, A.n, k, MOpPre{B, X, CELG_X0_USER, 0.0, 0.0, a});
+  if (st) return st;
+  // alpha = 0 keeps sigma = 0 / p.v finite, so no column drops out
+  CELG_CUDA(cudaMemsetAsync(a.alpha, 0, sizeof(double) * kMaxRhs, h->stream));
+  const MEpiAp ep{work, B, k, a};
   float best_ms = 0.f;
   *best = 0;
   for (int c = 0; c < kSpmmNumCfgs; ++c) {
-    int st = launch_spmm(h, A, k, B, MEpiVerify{B, k, a}, c);
+    st = launch_spmm(h, A, k, B, ep, c);
     if (st) return st;
     CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
-    for (int r = 0; r < 3 && !st; ++r) st = launch_spmm(h, A, k, B, MEpiVerify{B, k, a}, c);
+    for (int r = 0; r < 3 && !st; ++r) st = launch_spmm(h, A, k, B, ep, c);
     if (st) return st;
     CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
     CELG_CUDA(cudaEventSynchronize(h->ev1));
@@ -661,7 +668,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   a.cond = 0;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
   if (mu->tuned_mat != (const void*)m || mu->tuned_n != (int)n || mu->tuned_k != k) {
-    st = spmm_tune(h, m->csr, k, B, a, &mu->cfg);
+    st = spmm_tune(h, m->csr, k, B, X, V, a, &mu->cfg);
     if (st) return st;
     mu->tuned_mat = m;
     mu->tuned_n = (int)n;

@@ -116,6 +116,26 @@ int celg_mat_from_csr(celg_handle* h, int n, int nnz, const int* row_ptr, const 
  * reject it (CELG_ERR_ARG). */
 int celg_mat_from_csr_ext(celg_handle* h, int n, int ncols, int nnz, const int* row_ptr,
                           const int* cols, const double* vals, int index_base, celg_mat** out);
+/* COO triplets (host arrays, any order, duplicates allowed and kept) -> CSR on
+ * the device: a stable sort by (row, column), so equal keys keep their input
+ * order, and the row pointer from the row counts.  Replaces
+ * cel_sp_mat_format_sparse_31_sort (src/fspmt/cel_sp_mat_module.f90:518-585)
+ * followed by cel_sp_mat_to_csr (:430-456).  ncols >= n (halo columns as in
+ * celg_mat_from_csr_ext). */
+int celg_mat_from_coo(celg_handle* h, int n, int ncols, int nnz, const int* rows, const int* cols,
+                      const double* vals, int index_base, celg_mat** out);
+/* MatrixMarket files, read as mmread does (src/fbase/cel_mmio_module.f90:17-341):
+ * coordinate or array, real / integer / pattern (pattern values are 1.0),
+ * general / symmetric / skew-symmetric; complex files are rejected.  Entries
+ * come back 1-based in file order, exactly as stored; expand != 0 adds the
+ * mirrored entry (negated for skew-symmetric) after each off-diagonal entry
+ * of a symmetric file.  celg_mm_info gives the sizes and the entry count for
+ * that choice of expand. */
+#define CELG_MM_GENERAL 0
+#define CELG_MM_SYMMETRIC 1
+#define CELG_MM_SKEW 2
+int celg_mm_info(const char* path, int expand, int* nrows, int* ncols, int* nnz, int* symmetry);
+int celg_mm_read(const char* path, int expand, int nnz_cap, int* rows, int* cols, double* vals);
 /* same with device arrays (0-based), copied device to device */
 int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_d,
                              const int* cols_d, const double* vals_d, celg_mat** out);
