@@ -23,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
          "-I", INCLUDE, "--expt-relaxed-constexpr"]
 SOURCES = ["api.cu", "spmv.cu", "blas1.cu", "pcg.cu", "krylov.cu", "ir.cu", "ru.cu", "elm.cu", "noalloc.cu",
-           "batched.cu", "selftest.cu", "multirhs.cu", "adjoint.cu", "dist.cu", "assemble.cu"]
+           "batched.cu", "selftest.cu", "multirhs.cu", "adjoint.cu", "dist.cu", "assemble.cu",
+           "blockjacobi.cu"]
 
 
 def _newer(target, deps):

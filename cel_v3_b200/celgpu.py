@@ -39,6 +39,9 @@ ERR_STATE = 6
 
 FMT_CSR = 0
 FMT_JAD = 1
+PRECOND_JACOBI = 0
+PRECOND_BLOCK_JACOBI = 1
+
 X0_REF_ONES = 0
 X0_ZERO = 1
 X0_USER = 2
@@ -62,7 +65,7 @@ class Params(ctypes.Structure):
         ("iter_max", ctypes.c_int), ("fmt", ctypes.c_int), ("precision", ctypes.c_int),
         ("literal_ref_bugs", ctypes.c_int), ("restart", ctypes.c_int),
         ("inner_eps_rel", ctypes.c_double), ("inner_iter_max", ctypes.c_int),
-        ("outer_max", ctypes.c_int),
+        ("outer_max", ctypes.c_int), ("precond", ctypes.c_int),
     ]
 
 
@@ -131,6 +134,9 @@ def _load():
         "celg_diffusion7_face_grad": (i, [vp, i, i, i, vp, vp, vp, vp, vp]),
         "celg_mat_from_csr_ext": (i, [vp, i, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
         "celg_mat_from_coo": (i, [vp, i, i, i, vp, vp, vp, i, ctypes.POINTER(vp)]),
+        "celg_mat_block_jacobi": (i, [vp, i]),
+        "celg_mat_get_block_jacobi": (i, [vp, vp]),
+        "celg_block_jacobi_apply": (i, [vp, vp, vp, vp]),
         "celg_mm_info": (i, [ctypes.c_char_p, i, ip, ip, ip, ip]),
         "celg_mm_read": (i, [ctypes.c_char_p, i, i, vp, vp, vp]),
         "celg_dist_create": (i, [vp, vp, ctypes.POINTER(Params), vp, vp, i, ctypes.POINTER(vp)]),
@@ -330,6 +336,18 @@ class Matrix:
         _check(lib.celg_mat_get_jacobi(self.ptr, _host_ptr(J)), "celg_mat_get_jacobi")
         return J[: self.n]
 
+    def block_jacobi(self, block_size):
+        """Inverse diagonal blocks for PCG with precond=PRECOND_BLOCK_JACOBI."""
+        _check(lib.celg_mat_block_jacobi(self.ptr, int(block_size)), "celg_mat_block_jacobi")
+        self.bj_bs = int(block_size)
+        return self
+
+    def get_block_jacobi(self):
+        n = self.n
+        inv = np.zeros((n, self.bj_bs))
+        _check(lib.celg_mat_get_block_jacobi(self.ptr, _host_ptr(inv)), "celg_mat_get_block_jacobi")
+        return inv
+
     def scale_diagonal(self):
         _check(lib.celg_mat_scale_diagonal(self.ptr), "celg_mat_scale_diagonal")
         return self
@@ -479,6 +497,10 @@ class Handle:
     def xpby(self, n, x_d, beta, y_d):
         _check(lib.celg_xpby(self.ptr, int(n), ctypes.c_void_p(x_d), float(beta),
                              ctypes.c_void_p(y_d)), "celg_xpby")
+
+    def block_jacobi_apply(self, mat, r_d, z_d):
+        _check(lib.celg_block_jacobi_apply(self.ptr, mat.ptr, ctypes.c_void_p(r_d), ctypes.c_void_p(z_d)),
+               "celg_block_jacobi_apply")
 
     def jacobi_apply(self, mat, r_d, z_d):
         _check(lib.celg_jacobi_apply(self.ptr, mat.ptr, ctypes.c_void_p(r_d), ctypes.c_void_p(z_d)),

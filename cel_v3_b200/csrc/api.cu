@@ -196,6 +196,7 @@ void free_mat_arrays(celg_mat* m) {
   cudaFree(m->jacobi);
   cudaFree(m->jacobi32);
   cudaFree(m->scale);
+  cudaFree(m->bjinv);
 }
 
 // Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.
@@ -320,6 +321,7 @@ extern "C" void celg_params_default(celg_params* p) {
   p->inner_eps_rel = 1e-4;
   p->inner_iter_max = 1000;
   p->outer_max = 20;
+  p->precond = CELG_PRECOND_JACOBI;
 }
 
 extern "C" const char* celg_status_string(int s) {
@@ -396,6 +398,7 @@ extern "C" int celg_destroy(celg_handle* h) {
   cudaFree(h->wr);
   cudaFree(h->wp);
   cudaFree(h->wv);
+  cudaFree(h->wz);
   cudaFree(h->state_d);
   cudaFreeHost(h->state_h);
   cudaFree(h->ru_state_d);
@@ -672,6 +675,7 @@ static int check_solve_args(celg_handle* h, celg_mat* m, const double* b, double
   if (!h || !m || !p || (m->csr.n > 0 && (!b || !x))) return CELG_ERR_ARG;
   if (p->fmt != CELG_FMT_CSR && p->fmt != CELG_FMT_JAD) return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER) return CELG_ERR_ARG;
+  if (p->precond != CELG_PRECOND_JACOBI && p->precond != CELG_PRECOND_BLOCK_JACOBI) return CELG_ERR_ARG;
   if (m->h != h) return CELG_ERR_ARG;
   if (m->csr.ncols != m->csr.n) return CELG_ERR_ARG;  // row blocks: celg_dist_* only
   return CELG_OK;
@@ -682,6 +686,7 @@ extern "C" int celg_pcg_jacobi(celg_handle* h, celg_mat* m, const double* b_d, d
   int st = check_solve_args(h, m, b_d, x_d, p);
   if (st) return st;
   CELG_CUDA(cudaSetDevice(h->device));
+  if (p->precision != CELG_PREC_FP64 && p->precond != CELG_PRECOND_JACOBI) return CELG_ERR_ARG;
   if (p->precision == CELG_PREC_FP32_IR) return ir_solve(h, m, b_d, x_d, p, res);
   if (p->precision == CELG_PREC_FP32_RU) return ru_solve(h, m, b_d, x_d, p, res);
   return pcg_solve(h, m, b_d, x_d, p, res);
@@ -691,6 +696,7 @@ extern "C" int celg_cg(celg_handle* h, celg_mat* m, const double* b_d, double* x
                        const celg_params* p, celg_result* res) {
   int st = check_solve_args(h, m, b_d, x_d, p);
   if (st) return st;
+  if (p->precond != CELG_PRECOND_JACOBI) return CELG_ERR_ARG;  // no preconditioner in CG
   CELG_CUDA(cudaSetDevice(h->device));
   return cg_solve(h, m, b_d, x_d, p, res);
 }
@@ -699,6 +705,7 @@ extern "C" int celg_gmres_jacobi(celg_handle* h, celg_mat* m, const double* b_d,
                                  const celg_params* p, celg_result* res) {
   int st = check_solve_args(h, m, b_d, x_d, p);
   if (st) return st;
+  if (p->precond != CELG_PRECOND_JACOBI) return CELG_ERR_ARG;  // point Jacobi only
   CELG_CUDA(cudaSetDevice(h->device));
   return gmres_solve(h, m, b_d, x_d, p, res);
 }

@@ -518,6 +518,7 @@ extern "C" int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats
                                 celg_result* res) {
   if (!h || count <= 0 || !mats || !b_d || !x_d || !p) return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0) return CELG_ERR_ARG;
+  if (p->precond != CELG_PRECOND_JACOBI) return CELG_ERR_ARG;
   for (int s = 0; s < count; ++s)
     if (mats[s] && mats[s]->csr.ncols != mats[s]->csr.n) return CELG_ERR_ARG;  // square systems only
   CELG_CUDA(cudaSetDevice(h->device));

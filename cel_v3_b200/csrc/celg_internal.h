@@ -69,6 +69,8 @@ struct celg_handle {
   double* wp = nullptr;
   double* wv = nullptr;
   size_t wcap = 0;           // elements
+  double* wz = nullptr;      // z = M r of block-Jacobi solves (wzcap elements)
+  size_t wzcap = 0;
   celg::PcgState* state_d = nullptr;
   celg::PcgState* state_h = nullptr;  // pinned
   void* ru_state_d = nullptr;         // reliable-update solver state
@@ -107,6 +109,8 @@ struct celg_mat {
   double* jacobi = nullptr;   // n
   float* jacobi32 = nullptr;  // n
   double* scale = nullptr;    // sqrt|d| when row-scaled, else null
+  double* bjinv = nullptr;    // n x bj_bs inverse diagonal blocks (block Jacobi)
+  int bj_bs = 0;
   bool scaled = false;
 };
 

@@ -266,7 +266,8 @@ extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* 
     return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0)
     return CELG_ERR_ARG;
-  if (p->fmt != CELG_FMT_CSR || p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
+  if (p->fmt != CELG_FMT_CSR || p->precision != CELG_PREC_FP64 || p->precond != CELG_PRECOND_JACOBI)
+    return CELG_ERR_ARG;
   if (m->csr.n <= 0) return CELG_ERR_ARG;  // every rank holds at least one row
   if (!m->jacobi) return CELG_ERR_STATE;
   if (state_d && (reinterpret_cast<uintptr_t>(state_d) & 15)) return CELG_ERR_ARG;

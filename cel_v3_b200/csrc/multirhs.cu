@@ -767,7 +767,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
 extern "C" int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
                                  const celg_params* p, celg_result* res) {
   if (!h || !m || !p || k <= 0 || k > celg::kMaxRhs || m->h != h) return CELG_ERR_ARG;
-  if (m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
+  if (m->csr.ncols != m->csr.n || p->precond != CELG_PRECOND_JACOBI) return CELG_ERR_ARG;
   if (m->csr.n > 0 && (!B_d || !X_d)) return CELG_ERR_ARG;
   if (p->x0_mode < CELG_X0_REF_ONES || p->x0_mode > CELG_X0_USER || p->iter_max < 0) return CELG_ERR_ARG;
   if (!m->jacobi) return CELG_ERR_STATE;

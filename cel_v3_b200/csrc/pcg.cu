@@ -95,6 +95,7 @@ static int pcg_setup(celg_handle* h, const PcgBind<VT>& B, const celg_params* p,
       if (!st) st = launch_tile(h, n, OpInitNat<double>{B.b, B.r, B.p, B.J, a});
       return st;
     }
+    if (B.bj) return bj_pcg_setup_tail(h, B, a);
   }
   return launch_csr<VT>(h, *B.A, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
 }
@@ -110,6 +111,13 @@ static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
       s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
   } else {
     s2 = launch_csr<VT>(h, *B.A, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+  }
+  if constexpr (std::is_same<VT, double>::value) {
+    if (B.bj) {
+      if (!s2) s2 = bj_pcg_update(h, B, a);
+      if (!s2) s2 = bj_pcg_direction(h, B, a);
+      return s2;
+    }
   }
   if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.x, B.r, B.p, B.v, B.J, a, 0.0});
   if (!s2) s2 = launch_tile(h, n, OpDirection<VT>{B.p, B.r, B.J, a, 0.0});
@@ -166,11 +174,12 @@ template <typename VT>
 static std::string pcg_key(const PcgBind<VT>& B, const celg_params* p, int hist_cap,
                            const void* mat) {
   char buf[640];
-  std::snprintf(buf, sizeof(buf), "pcg%d|%p|%d|%d|%p|%p|%p|%p|%p|%p|%d|%.17g|%.17g|%d|%d|%p|%p",
+  std::snprintf(buf, sizeof(buf), "pcg%d|%p|%d|%d|%p|%p|%p|%p|%p|%p|%d|%.17g|%.17g|%d|%d|%p|%p|%p|%d|%p",
                 (int)sizeof(VT), mat, B.A->n, B.jad ? 1 : 0, (const void*)B.b, (const void*)B.x,
                 (const void*)B.r, (const void*)B.p, (const void*)B.v, (const void*)B.J,
                 p->x0_mode, p->eps_abs, p->eps_rel, p->iter_max, hist_cap,
-                (const void*)B.vals, (const void*)B.verify_vals);
+                (const void*)B.vals, (const void*)B.verify_vals, (const void*)B.bj, B.bs,
+                (const void*)B.z);
   return std::string(buf);
 }
 
@@ -253,6 +262,23 @@ int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const cel
   B.p = h->wp;
   B.v = h->wv;
   B.J = m->jacobi;
+  if (p->precond == CELG_PRECOND_BLOCK_JACOBI) {
+    if (jad) return CELG_ERR_ARG;
+    if (!m->bjinv) return CELG_ERR_STATE;
+    if ((size_t)n > h->wzcap || !h->wz) {
+      CELG_CUDA(cudaStreamSynchronize(h->stream));
+      graph_cache_clear(h);
+      cudaFree(h->wz);
+      h->wz = nullptr;
+      h->wzcap = std::max<size_t>((size_t)n, 1024);
+      CELG_CUDA(cudaMalloc(&h->wz, h->wzcap * sizeof(double)));
+    }
+    B.bj = m->bjinv;
+    B.bs = m->bj_bs;
+    B.z = h->wz;
+  } else if (p->precond != CELG_PRECOND_JACOBI) {
+    return CELG_ERR_ARG;
+  }
   PcgState s;
   std::memset(&s, 0, sizeof(s));
   const int ret = pcg_run<double>(h, B, p, m, &s);

@@ -37,7 +37,16 @@ struct PcgBind {
   VT* p = nullptr;
   VT* v = nullptr;
   const VT* J = nullptr;
+  // block Jacobi (FP64 CSR only): inverse rows, block size, z = M r
+  const double* bj = nullptr;
+  int bs = 0;
+  double* z = nullptr;
 };
+
+// blockjacobi.cu: the block-Jacobi forms of the set-up and of K2/K3
+int bj_pcg_setup_tail(celg_handle* h, const PcgBind<double>& B, const PcgArgs& a);
+int bj_pcg_update(celg_handle* h, const PcgBind<double>& B, const PcgArgs& a);
+int bj_pcg_direction(celg_handle* h, const PcgBind<double>& B, const PcgArgs& a);
 
 int ensure_state(celg_handle* h, int hist_cap);
 template <typename VT>

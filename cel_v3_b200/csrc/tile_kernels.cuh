@@ -19,6 +19,13 @@
 
 namespace celg {
 
+// An op with `static constexpr bool kAllLanes = true` has load/compute called
+// for every lane of every tile, including rows past n.
+template <class T, class = void>
+struct all_lanes : std::false_type {};
+template <class T>
+struct all_lanes<T, std::void_t<decltype(T::kAllLanes)>> : std::integral_constant<bool, T::kAllLanes> {};
+
 template <class Op>
 __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx red) {
   constexpr int NR = Op::NRED;
@@ -39,12 +46,21 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
     typename Op::Regs regs[4];
     const long base = t * kTile + j;
+    if constexpr (all_lanes<Op>::value) {
+      // every lane takes part (rows past n included: the op guards them), so
+      // ops may exchange values between lanes with warp shuffles
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (base + (long)k * kLanes < n) op.load(base + (long)k * kLanes, regs[k]);
+      for (int k = 0; k < 4; ++k) op.load(base + (long)k * kLanes, regs[k]);
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (base + (long)k * kLanes < n) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+      for (int k = 0; k < 4; ++k) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (base + (long)k * kLanes < n) op.load(base + (long)k * kLanes, regs[k]);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (base + (long)k * kLanes < n) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+    }
     if (NR > 0) {
 #pragma unroll
       for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {

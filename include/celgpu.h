@@ -46,6 +46,9 @@ extern "C" {
                              * residual, update and test in FP64, the search
                              * direction kept across corrections              */
 
+#define CELG_PRECOND_JACOBI 0       /* point Jacobi, the reference's cel_cgalg_jacobi */
+#define CELG_PRECOND_BLOCK_JACOBI 1 /* inverse diagonal blocks (celg_mat_block_jacobi) */
+
 #define CELG_SOLVER_PCG 0   /* cel_cgalg_jacobi   (BENCHMARK_CG + Jacobi)     */
 #define CELG_SOLVER_CG 1    /* cel_cgalg          (BENCHMARK_CG, no precond.) */
 #define CELG_SOLVER_GMRES 2 /* cel_gmresalg_2jacobi (BENCHMARK_GMRES + Jacobi) */
@@ -69,6 +72,7 @@ typedef struct {
                          FP32-RU: residual drop that triggers an FP64 update */
   int inner_iter_max;   /* FP32-IR: inner iteration cap                         */
   int outer_max;        /* FP32-IR: refinement steps cap                        */
+  int precond;          /* CELG_PRECOND_*: PCG preconditioner (FP64 CSR solves)  */
 } celg_params;
 
 /* Solve report.  history (caller-owned host buffer of history_cap doubles,
@@ -180,6 +184,21 @@ int celg_norm2(celg_handle* h, int n, const double* a_d, double* out);
 int celg_axpy(celg_handle* h, int n, double alpha, const double* x_d, double* y_d);
 /* y = beta y + x: cel_fop_vec_distr_scale_1 (:918-956) */
 int celg_xpby(celg_handle* h, int n, const double* x_d, double beta, double* y_d);
+/* Block Jacobi: inverse diagonal blocks of block_size rows (1, 2, 4, 8, 16 or
+ * 32; the last block may be shorter), built as the reference's dead
+ * cel_prec_build_diagonal + cel_prec_build_diagonal_inv intend
+ * (src/fspmtdistr/cel_prec_module.f90:27-339): a row's entries are scanned in
+ * stored order up to the first column right of the block, Doolittle LU without
+ * pivoting, inverse by forward and back substitution per unit vector.
+ * CELG_ERR_BREAKDOWN when an inverse has a non-finite entry (zero pivot).
+ * Used by celg_pcg_jacobi with params.precond = CELG_PRECOND_BLOCK_JACOBI. */
+int celg_mat_block_jacobi(celg_mat* m, int block_size);
+/* host copy of the n x block_size inverse rows (row-major, zero-padded) */
+int celg_mat_get_block_jacobi(const celg_mat* m, double* inv_host);
+/* z = blockdiag(D^-1) r (cel_fop_block_jacobi_vec_mult,
+ * src/fop/cel_fop_block_jacobi_module.f90:29-190, with r(j) where the
+ * reference's general case reads r(i)) */
+int celg_block_jacobi_apply(celg_handle* h, const celg_mat* m, const double* r_d, double* z_d);
 /* z = r * jacobi: cel_fop_vec_mult_distr_jacobi (:338-375) */
 int celg_jacobi_apply(celg_handle* h, const celg_mat* m, const double* r_d, double* z_d);
 

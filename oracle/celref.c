@@ -426,6 +426,94 @@ void celref_jacobi(int n, const double* d, const double* s, double* J) {
   for (int i = 0; i < n; i++) J[i] = s ? s[i] / d[i] : 1.0 / d[i];
 }
 
+/* Block-Jacobi set-up: the intended form of cel_prec_build_diagonal and
+ * cel_prec_build_diagonal_inv (src/fspmtdistr/cel_prec_module.f90:27-339;
+ * dead code in the reference, whose block indexing is out of range for
+ * every block after the first).  Rows are cut into blocks of bs from row 0,
+ * the last one possibly shorter.
+ *  - extraction (:96-130): a row's entries are scanned in stored order; an
+ *    entry left of the block is skipped, one inside is written to the dense
+ *    block (the last one wins), the first one right of it ends the row;
+ *  - inverse (:256-339, cel_prec_inverse_matrix_serial1_nxn): Doolittle LU
+ *    without pivoting, then for every unit vector e_k the forward solve
+ *    L d = e_k and the back solve U x = d give column k of the inverse; a
+ *    1x1 block is 1/a.
+ * inv is n x bs, row-major: inv[i*bs + j] = (D_b^-1)(i - b0, j), zero-padded
+ * for the last block.  Returns 0, or 1 when an entry of an inverse is not
+ * finite (a zero pivot). */
+int celref_block_jacobi_inv(int n, const int* rp, const int* ci, const double* v, int bs,
+                            double* inv) {
+  int bad = 0;
+  double* a = (double*)calloc((size_t)bs * bs, sizeof(double));
+  double* L = (double*)calloc((size_t)bs * bs, sizeof(double));
+  double* c = (double*)calloc((size_t)bs * bs, sizeof(double));
+  double* d = (double*)calloc((size_t)bs, sizeof(double));
+  double* x = (double*)calloc((size_t)bs, sizeof(double));
+  double* b = (double*)calloc((size_t)bs, sizeof(double));
+  for (int b0 = 0; b0 < n; b0 += bs) {
+    const int nb = (n - b0 < bs) ? n - b0 : bs;
+    for (int q = 0; q < bs * bs; q++) a[q] = L[q] = c[q] = 0.0;
+    for (int i = 0; i < nb; i++) {
+      const int row = b0 + i;
+      for (int k = rp[row]; k < rp[row + 1]; k++) {
+        const int col = ci[k];
+        if (col < b0) continue;
+        if (col >= b0 + nb) break;
+        a[i * bs + (col - b0)] = v[k];
+      }
+    }
+    if (nb == 1) {
+      c[0] = 1.0 / a[0];
+    } else {
+      for (int k = 0; k < nb - 1; k++)
+        for (int i = k + 1; i < nb; i++) {
+          const double coeff = a[i * bs + k] / a[k * bs + k];
+          L[i * bs + k] = coeff;
+          for (int j = k + 1; j < nb; j++) a[i * bs + j] = a[i * bs + j] - coeff * a[k * bs + j];
+        }
+      for (int k = 0; k < nb; k++) {
+        for (int i = 0; i < nb; i++) b[i] = 0.0;
+        b[k] = 1.0;
+        d[0] = b[0];
+        for (int i = 1; i < nb; i++) {
+          d[i] = b[i];
+          for (int j = 0; j < i; j++) d[i] = d[i] - L[i * bs + j] * d[j];
+        }
+        x[nb - 1] = d[nb - 1] / a[(nb - 1) * bs + (nb - 1)];
+        for (int i = nb - 2; i >= 0; i--) {
+          x[i] = d[i];
+          for (int j = nb - 1; j > i; j--) x[i] = x[i] - a[i * bs + j] * x[j];
+          x[i] = x[i] / a[i * bs + i];
+        }
+        for (int i = 0; i < nb; i++) c[i * bs + k] = x[i];
+      }
+    }
+    for (int i = 0; i < nb; i++)
+      for (int j = 0; j < bs; j++) {
+        const double e = j < nb ? c[i * bs + j] : 0.0;
+        if (!isfinite(e)) bad = 1;
+        inv[(size_t)(b0 + i) * bs + j] = e;
+      }
+  }
+  free(a); free(L); free(c); free(d); free(x); free(b);
+  return bad;
+}
+
+/* z = blockdiag(D_b^-1) r (cel_fop_vec_mult_distr_jacobi_block,
+ * src/fop/cel_fop_block_jacobi_module.f90:96-190, in its intended form: the
+ * reference's n x n case multiplies by r(i) where r(j) is meant):
+ * z_i = r_b0 inv_i0 + r_b0+1 inv_i1 + ... left to right over the block. */
+void celref_block_jacobi_apply(int n, int bs, const double* inv, const double* r, double* z) {
+  for (int i = 0; i < n; i++) {
+    const int b0 = i - i % bs;
+    const int nb = (n - b0 < bs) ? n - b0 : bs;
+    const double* row = inv + (size_t)i * bs;
+    double s = r[b0] * row[0];
+    for (int j = 1; j < nb; j++) s = s + r[b0 + j] * row[j];
+    z[i] = s;
+  }
+}
+
 /* Diagonal row scaling, src/fspmtdistr/cel_sp_mat_distr_format_module.f90:120-121
  * (s = sqrt|d|) and :298-303 (row i divided by s_i).  d stays unscaled. */
 void celref_row_scale(int n, const int* rp, double* v, const double* d, double* s) {

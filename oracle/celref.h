@@ -115,6 +115,9 @@ void celref_spmv(const celref_mat* A, const double* x, double* y, int nworkers);
 void celref_diag(int n, const int* rp, const int* ci, const double* v, double* d);
 void celref_jacobi(int n, const double* d, const double* s, double* J);
 void celref_row_scale(int n, const int* rp, double* v, const double* d, double* s);
+int celref_block_jacobi_inv(int n, const int* rp, const int* ci, const double* v, int bs,
+                            double* inv);
+void celref_block_jacobi_apply(int n, int bs, const double* inv, const double* r, double* z);
 
 /* --- reductions and sweeps ------------------------------------------------ */
 double celref_dot(int n, const double* a, const double* b, int red, int nworkers);

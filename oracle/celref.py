@@ -164,6 +164,24 @@ def jacobi(d, s=None):
     return J
 
 
+def block_jacobi_inv(rp, ci, v, bs):
+    """n x bs inverse diagonal blocks (celref_block_jacobi_inv); returns
+    (inv, ok)."""
+    rp, ci, v = _i32(rp), _i32(ci), _f64(v)
+    n = rp.size - 1
+    inv = np.zeros((n, bs))
+    bad = lib().celref_block_jacobi_inv(n, _p(rp), _p(ci), _p(v), int(bs), _p(inv))
+    return inv, bad == 0
+
+
+def block_jacobi_apply(inv, r):
+    inv, r = _f64(inv), _f64(r)
+    n, bs = inv.shape
+    z = np.zeros(n)
+    lib().celref_block_jacobi_apply(n, bs, _p(inv), _p(r), _p(z))
+    return z
+
+
 def row_scale(rp, v, d):
     rp, d = _i32(rp), _f64(d)
     v = _f64(v).copy()

@@ -112,7 +112,7 @@ def test_matrix_market_to_pcg(gpu, tmp_path):
     n = rp.size - 1
     rows = np.repeat(np.arange(n), np.diff(rp))
     low = ci <= rows
-    lines = [f"{r + 1} {c + 1} {val!r}" for r, c, val in zip(rows[low], ci[low], v[low])]
+    lines = [f"{r + 1} {c + 1} {float(val)!r}" for r, c, val in zip(rows[low], ci[low], v[low])]
     p = write(tmp_path, "poisson.mtx", "%%MatrixMarket matrix coordinate real symmetric\n"
               f"{n} {n} {len(lines)}\n" + "\n".join(lines) + "\n")
     nr, nc, sy, r, c, vv = celgpu.mm_read(p, expand=True)
