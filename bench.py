@@ -167,6 +167,21 @@ def precision_form(h, celgpu, torch, stream, side=256, reps=2):
     base = out["fp64_pcg"]["solves_per_s"]
     for k in ("fp32_ir", "fp32_ru"):
         out[k]["speedup_vs_fp64"] = out[k]["solves_per_s"] / base
+    # the block-Jacobi preconditioner (8-row blocks) on the same system, FP64
+    m.block_jacobi(8)
+    pf = celgpu.params(eps_rel=1e-10, iter_max=20000, x0_mode=celgpu.X0_ZERO,
+                       precond=celgpu.PRECOND_BLOCK_JACOBI)
+    h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        inf = h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pf)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fms = e0.elapsed_time(e1) / reps
+    out["fp64_pcg_block_jacobi8"] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
+                                     "verified_relres": inf.verified_relres, "status": inf.status,
+                                     "speedup_vs_fp64": 1e3 / fms / base}
     m.destroy()
     return out
 
