@@ -399,6 +399,9 @@ static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle 
   return a;
 }
 
+// The solve as recorded into the graph; with a.cond == 0 (profiling mode,
+// CELG_GRAPH=0) the loop body is instead launched from the host in chunks of
+// 8 iterations between reads of the live-system count.
 static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
                           const celg_params* p, BatchArgs a) {
   const long N = bt->N;
@@ -412,13 +415,22 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
   }
   int st = launch_tile(h, N, BOpPre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a});
   if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiInit{bt->B, bt->R, bt->P, bt->J, a});
-  if (!st)
-    st = capture_while(h, a.cond, [&]() -> int {
-      int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, BEpiAp{bt->V, bt->P, a});
-      if (!s2) s2 = launch_tile(h, N, BOpUpdate{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0});
-      if (!s2) s2 = launch_tile(h, N, BOpDirection{bt->P, bt->R, bt->J, a, 0.0});
-      return s2;
-    });
+  auto body = [&]() -> int {
+    int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, BEpiAp{bt->V, bt->P, a});
+    if (!s2) s2 = launch_tile(h, N, BOpUpdate{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0});
+    if (!s2) s2 = launch_tile(h, N, BOpDirection{bt->P, bt->R, bt->J, a, 0.0});
+    return s2;
+  };
+  if (!st && a.cond) st = capture_while(h, a.cond, body);
+  for (int it = 0; !st && !a.cond && it < p->iter_max; it += 8) {
+    for (int q = 0; q < 8 && !st; ++q) st = body();
+    int live = 0;
+    if (!st) {
+      CELG_CUDA(cudaMemcpyAsync(&live, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      CELG_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (!live) break;
+  }
   if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiVerify{bt->B, a});
   if (st) return st;
   for (int s = 0; s < bt->nsys; ++s) {
@@ -459,16 +471,23 @@ int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* 
   }
   std::snprintf(buf, sizeof(buf), "|%d|%.17g|%.17g|%d", p->x0_mode, p->eps_abs, p->eps_rel, p->iter_max);
   gkey += buf;
-  GraphEntry* ge = graph_cache_find(h, gkey);
-  if (!ge) {
-    st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
-      return record_batched(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, cond, h->err_d));
-    }, &ge);
+  if (!graphs_enabled()) {
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = record_batched(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, 0, h->err_d));
     if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    GraphEntry* ge = graph_cache_find(h, gkey);
+    if (!ge) {
+      st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
+        return record_batched(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, cond, h->err_d));
+      }, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   }
-  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
-  CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
-  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
   std::vector<double> ds(7 * (size_t)count);
   std::vector<int> is(3 * (size_t)count + 1);
   CELG_CUDA(cudaMemcpyAsync(ds.data(), bt->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost,

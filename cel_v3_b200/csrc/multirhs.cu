@@ -122,7 +122,9 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 constexpr int kAsyncU = 8;                    // gathers per row slot
-constexpr int kAsyncSlot = (kAsyncU + 2) * 32;  // doubles per slot: U entries + 2 epilogue operands
+// doubles per slot: U gathered entries and 2 epilogue operands per lane, then
+// the row's U matrix values (padded to 16 bytes)
+constexpr int kAsyncSlot = (kAsyncU + 2) * 32 + ((kAsyncU + 1) & ~1);
 
 template <int U>
 __device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const double* __restrict__ X,
@@ -205,11 +207,14 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restric
 // The same SpMM with the gathers issued as asynchronous copies into a ring of
 // S row slots per warp in shared memory (cp.async, 8 bytes per lane and
 // entry), so the data in flight does not occupy registers: rows r+1..r+S-1
-// are in flight while row r is added up.  Each lane copies and reads only its
-// own column of a slot, so the lanes need no barrier between them; the
-// epilogue's operands travel in the same slot (Epi::stage_pre / staged).
-template <class Epi, int S>
-__global__ void __launch_bounds__(kLanes) spmm_async_kernel(const int* __restrict__ rp,
+// are in flight while row r is added up.  A slot also receives the row's
+// matrix values (lanes 0..U-1) and the epilogue's operands (Epi::stage_pre),
+// and the column indices of the next row to issue are loaded one row ahead,
+// so no global load is waited for on the issue path.  Each lane copies and
+// reads only its own column of a slot (the values area is read by all lanes
+// after the wait and the warp barrier).
+template <class Epi, int S, int MINB>
+__global__ void __launch_bounds__(kLanes, MINB) spmm_async_kernel(const int* __restrict__ rp,
                                                            const int* __restrict__ ci,
                                                            const double* __restrict__ v, int n,
                                                            int k, const double* __restrict__ X,
@@ -217,6 +222,7 @@ __global__ void __launch_bounds__(kLanes) spmm_async_kernel(const int* __restric
   constexpr int NR = Epi::NRED;
   constexpr int U = kAsyncU;
   constexpr int SLOT = kAsyncSlot;
+  constexpr int VOFF = (U + 2) * 32;  // matrix values of the row
   constexpr unsigned kFull = 0xffffffffu;
   __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
   __shared__ double scratch[8];
@@ -238,34 +244,43 @@ __global__ void __launch_bounds__(kLanes) spmm_async_kernel(const int* __restric
       const int nrows = (int)min(32L, (long)n - row0);
       const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
       const int b0 = __ldg(rp + row0);
-      // issue row r's first U gathers and its epilogue operands into slot r % S
-      auto issue = [&](int r) {
-        const int b = r == 0 ? b0 : __shfl_sync(kFull, re, r > 0 ? r - 1 : 0);
-        const int e = __shfl_sync(kFull, re, r);
-        double* slot = ring + (r % S) * SLOT;
-        if (on) {
+      // next row to issue (rI), its entry range and its first U column indices
+      int rI = 0, bI = b0, eI = __shfl_sync(kFull, re, 0);
+      int cn[U];
 #pragma unroll
-          for (int u = 0; u < U; ++u)
-            if (b + u < e) cp_async8(slot + u * 32 + lane, X + (long)__ldg(ci + b + u) * k + lane);
-          epi.stage_pre(row0 + r, lane, slot + U * 32);
+      for (int u = 0; u < U; ++u) cn[u] = bI + u < eI ? __ldg(ci + bI + u) : 0;
+      auto issue_next = [&]() {
+        if (rI < nrows) {
+          double* slot = ring + (rI % S) * SLOT;
+          if (on) {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              if (bI + u < eI) cp_async8(slot + u * 32 + lane, X + (long)cn[u] * k + lane);
+            epi.stage_pre(row0 + rI, lane, slot + U * 32);
+          }
+          if (lane < U && bI + lane < eI) cp_async8(slot + VOFF + lane, v + bI + lane);
         }
         cp_async_commit();
+        ++rI;
+        if (rI < nrows) {
+          bI = eI;
+          eI = __shfl_sync(kFull, re, rI);
+#pragma unroll
+          for (int u = 0; u < U; ++u) cn[u] = bI + u < eI ? __ldg(ci + bI + u) : 0;
+        }
       };
-      for (int r = 0; r < S - 1; ++r) {
-        if (r < nrows) issue(r);
-        else cp_async_commit();
-      }
+      for (int r = 0; r < S - 1; ++r) issue_next();
       int b = b0;
       for (int r = 0; r < nrows; ++r) {
-        if (r + S - 1 < nrows) issue(r + S - 1);
-        else cp_async_commit();
+        issue_next();  // row r + S - 1
         cp_async_wait<S - 1>();
+        __syncwarp();  // the values area of the slot was filled by lanes 0..U-1
         const int e = __shfl_sync(kFull, re, r);
         const double* slot = ring + (r % S) * SLOT;
         double sum = 0.0;
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (b + u < e) sum = dadd(sum, dmul(__ldg(v + b + u), slot[u * 32 + lane]));
+          if (b + u < e) sum = dadd(sum, dmul(slot[VOFF + u], slot[u * 32 + lane]));
         for (int kk = b + U; kk < e; kk += U) {  // rows longer than U entries
           double xv[U];
           spmm_gather<U>(ci, X, kk, e, k, lane, on, xv);
@@ -274,6 +289,7 @@ __global__ void __launch_bounds__(kLanes) spmm_async_kernel(const int* __restric
             if (kk + u < e) sum = dadd(sum, dmul(__ldg(v + kk + u), xv[u]));
         }
         if (on) epi.row(row0 + r, lane, sum, epi.staged(slot + U * 32, lane), acc);
+        __syncwarp();  // every lane has read the values area before it is refilled
         b = e;
       }
       cp_async_wait<0>();
@@ -504,10 +520,11 @@ struct MEpiVerify {
 
 // SpMM launch variants: the register pipeline with the resident CTAs per SM
 // its registers are budgeted for and its gather chunk width (2/8, 3/8, 3/4,
-// 4/4), and the cp.async ring with 2, 3 or 4 row slots per warp.  The
+// 4/4), and the cp.async ring with row slots per warp / CTAs per SM of 2/4,
+// 2/3, 3/3 and 4/2.  The
 // fastest for a matrix and k is picked by timing them (spmm_tune) before the
 // first solve.
-constexpr int kSpmmNumCfgs = 7;  // 0-3 register pipeline, 4-6 cp.async ring
+constexpr int kSpmmNumCfgs = 8;  // 0-3 register pipeline, 4-7 cp.async ring
 
 template <class Epi, int MINB, int U>
 static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
@@ -523,12 +540,12 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double*
   return CELG_OK;
 }
 
-template <class Epi, int S>
+template <class Epi, int S, int MINB>
 static int launch_spmm_async(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
-  auto kern = spmm_async_kernel<Epi, S>;
+  auto kern = spmm_async_kernel<Epi, S, MINB>;
   const int smem = 8 * S * kAsyncSlot * (int)sizeof(double);
   CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
@@ -547,9 +564,10 @@ static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, 
     case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, k, X, epi);
     case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, k, X, epi);
     case 3: return launch_spmm_cfg<Epi, 4, 4>(h, A, k, X, epi);
-    case 4: return launch_spmm_async<Epi, 2>(h, A, k, X, epi);
-    case 5: return launch_spmm_async<Epi, 3>(h, A, k, X, epi);
-    default: return launch_spmm_async<Epi, 4>(h, A, k, X, epi);
+    case 4: return launch_spmm_async<Epi, 2, 4>(h, A, k, X, epi);
+    case 5: return launch_spmm_async<Epi, 2, 3>(h, A, k, X, epi);
+    case 6: return launch_spmm_async<Epi, 3, 3>(h, A, k, X, epi);
+    default: return launch_spmm_async<Epi, 4, 2>(h, A, k, X, epi);
   }
 }
 
@@ -595,7 +613,7 @@ void multi_free(Multi* m) {
 // p.v), applied to B with the output in a work vector; the per-column state
 // is set up first by MOpPre in the user-start mode, which leaves X alone, and
 // the solve's own set-up overwrites everything the timing wrote.  Returns the
-// fastest variant; CELG_SPMM_CFG=0..6 forces one (profiling).
+// fastest variant; CELG_SPMM_CFG=0..7 forces one (profiling).
 static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, double* X,
                      double* work, const MultiArgs& a, int* best) {
   if (const char* e = std::getenv("CELG_SPMM_CFG")) {

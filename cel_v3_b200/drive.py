@@ -4,6 +4,7 @@
   python -m cel_v3_b200.drive pcg SIDE ITERS [fp64|ru|ir]
                                                         one solve capped at ITERS iterations
   python -m cel_v3_b200.drive mrhs SIDE ITERS K         K right-hand sides, capped at ITERS
+  python -m cel_v3_b200.drive batch 0 ITERS             the 64 uneven systems, capped at ITERS
 
 Set CELG_GRAPH=0 to launch the solver kernels from a host loop instead of
 one CUDA graph, so that a kernel profiler can attribute time to each kernel.
@@ -18,6 +19,18 @@ def main(argv):
 
     from cel_v3_b200 import celgpu, synth
     what, side = argv[0], int(argv[1])
+    if what == "batch":
+        h = celgpu.Handle(0, torch.cuda.current_stream().cuda_stream)
+        probs = synth.batch_problems()
+        mats = [h.matrix_from_csr(rp, ci, v).jacobi() for _, rp, ci, v, _ in probs]
+        bs = [torch.from_numpy(b).cuda() for *_, b in probs]
+        xs = [torch.zeros_like(b) for b in bs]
+        infos = h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs],
+                              eps_rel=1e-8, iter_max=int(argv[2]))
+        torch.cuda.synchronize()
+        print("batch", len(mats), max(i.iter_done for i in infos))
+        h.close()
+        return 0
     rp, ci, v, xt = synth.plain(side, 1)
     n = rp.size - 1
     h = celgpu.Handle(0, torch.cuda.current_stream().cuda_stream)
