@@ -1,6 +1,7 @@
 """Runs one workload of the library for profiling (e.g. under ncu).
 
   python -m cel_v3_b200.drive spmv SIDE [REPS]          REPS CSR SpMVs, SIDE^3 Poisson
+  python -m cel_v3_b200.drive spmv32 SIDE [REPS]        the same on the FP32 copy (1-byte columns)
   python -m cel_v3_b200.drive pcg SIDE ITERS [fp64|ru|ir]
                                                         one solve capped at ITERS iterations
   python -m cel_v3_b200.drive mrhs SIDE ITERS K         K right-hand sides, capped at ITERS
@@ -37,7 +38,14 @@ def main(argv):
     m = h.matrix_from_csr(rp, ci, v).jacobi()
     x = torch.from_numpy(xt).cuda()
     y = torch.zeros(n, dtype=torch.float64, device="cuda")
-    if what == "spmv":
+    if what == "spmv32":
+        m.make_fp32()
+        x32, y32 = x.float(), y.float()
+        for _ in range(int(argv[2]) if len(argv) > 2 else 4):
+            h.spmv_f32(m, x32.data_ptr(), y32.data_ptr())
+        torch.cuda.synchronize()
+        print("spmv32", side, float(y32.sum()))
+    elif what == "spmv":
         for _ in range(int(argv[2]) if len(argv) > 2 else 4):
             h.spmv(m, x.data_ptr(), y.data_ptr())
         torch.cuda.synchronize()
