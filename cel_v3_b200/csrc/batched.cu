@@ -59,8 +59,8 @@ struct BOpPre {
   double eps_abs, eps_rel;
   BatchArgs a;
   __device__ bool prepare() { return true; }
-  __device__ bool tile_active(long) const { return true; }
-  __device__ void begin_tile(long) {}
+  __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
+  __device__ void begin_tile(const TileInfo&) {}
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
   __device__ void compute(long i, Regs& g, double* acc) const {
@@ -91,8 +91,8 @@ struct BEpiInit {
   const double* J;
   BatchArgs a;
   __device__ bool active() const { return true; }
-  __device__ bool tile_active(long) const { return true; }
-  __device__ void begin_tile(long) {}
+  __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
+  __device__ void begin_tile(const TileInfo&) {}
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void row(long i, double s, double* acc) const {
     const double ri = __dsub_rn(b[i], dadd(0.0, s));
@@ -119,8 +119,10 @@ struct BEpiAp {
   const double* p;
   BatchArgs a;
   __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
-  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
-  __device__ void begin_tile(long) {}
+  __device__ TileInfo tile_info(long t) const {
+    return TileInfo{*(volatile int*)&a.active[a.sys_of(t)], 0.0};
+  }
+  __device__ void begin_tile(const TileInfo&) {}
   __device__ const BatchRed& bred() const { return a.br; }
   struct Pre { double p; };
   __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
@@ -154,8 +156,11 @@ struct BOpUpdate {
   BatchArgs a;
   double sg;
   __device__ bool prepare() { return true; }
-  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
-  __device__ void begin_tile(long t) { sg = a.sigma[a.sys_of(t)]; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    return TileInfo{*(volatile int*)&a.active[s], a.sigma[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) { sg = ti.s; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const {
     g.x = x[i];
@@ -193,8 +198,11 @@ struct BOpDirection {
   BatchArgs a;
   double bt;
   __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
-  __device__ bool tile_active(long t) const { return *(volatile int*)&a.active[a.sys_of(t)] != 0; }
-  __device__ void begin_tile(long t) { bt = a.beta[a.sys_of(t)]; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    return TileInfo{*(volatile int*)&a.active[s], a.beta[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) { bt = ti.s; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
   __device__ void compute(long i, Regs& g, double*) const {
@@ -211,8 +219,8 @@ struct BEpiVerify {
   const double* b;
   BatchArgs a;
   __device__ bool active() const { return true; }
-  __device__ bool tile_active(long) const { return true; }
-  __device__ void begin_tile(long) {}
+  __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
+  __device__ void begin_tile(const TileInfo&) {}
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void row(long i, double s, double* acc) const {
     const double ri = __dsub_rn(b[i], dadd(0.0, s));

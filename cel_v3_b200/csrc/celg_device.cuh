@@ -240,8 +240,12 @@ struct finishes_always<T, std::void_t<decltype(T::kFinishAlways)>>
 //
 // An epilogue/op with `static constexpr bool kBatched = true` runs over the
 // concatenated rows of many systems (each padded to whole tiles).  It provides
-//   bool tile_active(long t)      skip the tiles of finished systems
-//   void begin_tile(long t)       load the tile's system scalars
+//   TileInfo tile_info(long t)    the tile's system state (active flag and the
+//                                 scalar the op needs), loaded by the kernels
+//                                 one tile ahead so that the dependent loads
+//                                 (tile -> system -> scalars) overlap the
+//                                 current tile's work
+//   void begin_tile(const TileInfo&)  take the tile's system scalars
 //   void finish_sys(int s, tot)   per-system scalars (lane 0 of the CTA that
 //                                 completed the system's last tile)
 //   void finish_global()          lane 0 of the last CTA of the kernel
@@ -252,6 +256,12 @@ struct BatchRed {
   const int* sys_tile0;  // first tile of each system
   const int* sys_ntiles;  // tiles of each system
   unsigned* sys_ticket;   // per-system completion tickets (reset by the finisher)
+};
+
+// per-tile system state of a batched op (act != 0: the tile's system runs)
+struct TileInfo {
+  int act;
+  double s;
 };
 
 template <class T, class = void>

@@ -100,13 +100,19 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
     int bnd = 0;  // lane q (0..4) holds rp at sub-tile boundary q of tile t
     if (t < ntiles && lane <= kSubPerTile)
       bnd = __ldg(rp + min(t * kTile + (long)lane * kSub, (long)n));
+    TileInfo nxt{0, 0.0};
+    if constexpr (kB) {
+      if (t < ntiles) nxt = epi.tile_info(t);
+    }
     for (; t < ntiles; t += gridDim.x) {
       const int cur = bnd;
       const long tn = t + gridDim.x;
       if (tn < ntiles && lane <= kSubPerTile)
         bnd = __ldg(rp + min(tn * kTile + (long)lane * kSub, (long)n));
       if constexpr (kB) {
-        if (!epi.tile_active(t)) continue;
+        const TileInfo ti = nxt;
+        if (tn < ntiles) nxt = epi.tile_info(tn);
+        if (!ti.act) continue;
       }
       for (int q = 0; q < kSubPerTile; ++q) {
         const long s = t * kSubPerTile + q;
@@ -151,10 +157,16 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
   const int j = threadIdx.x;
   int it = 0;
   Epi ep = epi;
+  TileInfo nxt{0, 0.0};
+  if constexpr (kB) {
+    if (blockIdx.x < ntiles) nxt = ep.tile_info(blockIdx.x);
+  }
   for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     if constexpr (kB) {
-      if (!ep.tile_active(t)) continue;
-      ep.begin_tile(t);
+      const TileInfo ti = nxt;
+      if (t + gridDim.x < ntiles) nxt = ep.tile_info(t + gridDim.x);
+      if (!ti.act) continue;
+      ep.begin_tile(ti);
     }
     Acc<NR> acc;
 #pragma unroll

@@ -36,10 +36,16 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   if (!op.prepare()) return;
   const int j = threadIdx.x;
   const long ntiles = (n + kTile - 1) / kTile;
+  TileInfo nxt{0, 0.0};
+  if constexpr (kB) {
+    if (blockIdx.x < ntiles) nxt = op.tile_info(blockIdx.x);
+  }
   for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
     if constexpr (kB) {
-      if (!op.tile_active(t)) continue;
-      op.begin_tile(t);
+      const TileInfo cur = nxt;
+      if (t + gridDim.x < ntiles) nxt = op.tile_info(t + gridDim.x);
+      if (!cur.act) continue;
+      op.begin_tile(cur);
     }
     Acc<NR> acc;
 #pragma unroll
