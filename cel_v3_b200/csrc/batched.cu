@@ -61,6 +61,7 @@ struct BOpPre {
   __device__ bool prepare() { return true; }
   __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
   __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int) const { return true; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
   __device__ void compute(long i, Regs& g, double* acc) const {
@@ -93,6 +94,7 @@ struct BEpiInit {
   __device__ bool active() const { return true; }
   __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
   __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int) const { return true; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void row(long i, double s, double* acc) const {
     const double ri = __dsub_rn(b[i], dadd(0.0, s));
@@ -123,6 +125,7 @@ struct BEpiAp {
     return TileInfo{*(volatile int*)&a.active[a.sys_of(t)], 0.0};
   }
   __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
   struct Pre { double p; };
   __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
@@ -161,6 +164,7 @@ struct BOpUpdate {
     return TileInfo{*(volatile int*)&a.active[s], a.sigma[s]};
   }
   __device__ void begin_tile(const TileInfo& ti) { sg = ti.s; }
+  __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const {
     g.x = x[i];
@@ -203,6 +207,7 @@ struct BOpDirection {
     return TileInfo{*(volatile int*)&a.active[s], a.beta[s]};
   }
   __device__ void begin_tile(const TileInfo& ti) { bt = ti.s; }
+  __device__ bool sys_active(int) const { return false; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
   __device__ void compute(long i, Regs& g, double*) const {
@@ -221,6 +226,7 @@ struct BEpiVerify {
   __device__ bool active() const { return true; }
   __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
   __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int) const { return true; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void row(long i, double s, double* acc) const {
     const double ri = __dsub_rn(b[i], dadd(0.0, s));
@@ -231,6 +237,45 @@ struct BEpiVerify {
   }
   __device__ void finish_global() const {}
 };
+
+// ---- completion of a batched sweep ------------------------------------------------
+
+// One CTA per system: if the system took part, its tile partials are reduced
+// in the single-solve order (lane j sums partials j, j+256, ... from 0.0;
+// butterfly; warps in order) and finish_sys runs; the last CTA to arrive
+// runs finish_global.
+template <int NRED, class Op>
+__global__ void __launch_bounds__(kLanes) batch_finish_kernel(Op op, RedCtx red) {
+  __shared__ double scratch[8];
+  __shared__ int s_flag;
+  const int s = blockIdx.x;
+  const int tid = threadIdx.x;
+  const BatchRed& br = op.bred();
+  const long nt = br.sys_ntiles[s];
+  if (nt > 0 && op.sys_active(s)) {
+    double tot[NRED];
+    const long t0 = br.sys_tile0[s];
+#pragma unroll
+    for (int r = 0; r < NRED; ++r) {
+      double acc = 0.0;
+      const double* p = red.partials + (long)r * red.ntiles + t0;
+      for (long k = tid; k < nt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
+      tot[r] = group_fold256(acc, scratch, tid, 1);
+    }
+    if (tid == 0) op.finish_sys(s, tot);
+  }
+  if (tid == 0) {
+    __threadfence();
+    const unsigned tk = atomicAdd(red.ticket, 1u);
+    s_flag = (tk == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_flag && tid == 0) {
+    __threadfence();
+    op.finish_global();
+    *red.ticket = 0u;
+  }
+}
 
 // ---- concatenation ------------------------------------------------------------
 
@@ -410,6 +455,14 @@ static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle 
 // The solve as recorded into the graph; with a.cond == 0 (profiling mode,
 // CELG_GRAPH=0) the loop body is instead launched from the host in chunks of
 // 8 iterations between reads of the live-system count.
+template <class Op>
+static int batch_finish(celg_handle* h, const Batch* bt, const Op& op) {
+  RedCtx red{h->partials, h->ticket, bt->NT};
+  batch_finish_kernel<Op::NRED, Op><<<bt->nsys, kLanes, 0, h->stream>>>(op, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
                           const celg_params* p, BatchArgs a) {
   const long N = bt->N;
@@ -421,11 +474,19 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
       CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
                                 cudaMemcpyDeviceToDevice, h->stream));
   }
-  int st = launch_tile(h, N, BOpPre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a});
-  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiInit{bt->B, bt->R, bt->P, bt->J, a});
+  const BOpPre pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
+  const BEpiInit init{bt->B, bt->R, bt->P, bt->J, a};
+  const BEpiAp ap{bt->V, bt->P, a};
+  const BOpUpdate upd{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0};
+  int st = launch_tile(h, N, pre);
+  if (!st) st = batch_finish(h, bt, pre);
+  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, init);
+  if (!st) st = batch_finish(h, bt, init);
   auto body = [&]() -> int {
-    int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, BEpiAp{bt->V, bt->P, a});
-    if (!s2) s2 = launch_tile(h, N, BOpUpdate{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0});
+    int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, ap);
+    if (!s2) s2 = batch_finish(h, bt, ap);
+    if (!s2) s2 = launch_tile(h, N, upd);
+    if (!s2) s2 = batch_finish(h, bt, upd);
     if (!s2) s2 = launch_tile(h, N, BOpDirection{bt->P, bt->R, bt->J, a, 0.0});
     return s2;
   };
@@ -439,7 +500,9 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
     }
     if (!live) break;
   }
-  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, BEpiVerify{bt->B, a});
+  const BEpiVerify ver{bt->B, a};
+  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, ver);
+  if (!st) st = batch_finish(h, bt, ver);
   if (st) return st;
   for (int s = 0; s < bt->nsys; ++s) {
     if (bt->n[s] == 0) continue;

@@ -246,16 +246,18 @@ struct finishes_always<T, std::void_t<decltype(T::kFinishAlways)>>
 //                                 (tile -> system -> scalars) overlap the
 //                                 current tile's work
 //   void begin_tile(const TileInfo&)  take the tile's system scalars
-//   void finish_sys(int s, tot)   per-system scalars (lane 0 of the CTA that
-//                                 completed the system's last tile)
-//   void finish_global()          lane 0 of the last CTA of the kernel
+//   bool sys_active(int s)        whether system s took part in the sweep
+//   void finish_sys(int s, tot)   per-system scalars
+//   void finish_global()          after every system's finish_sys
 //   const BatchRed& bred()
-// Each system's partials are reduced in the same order as a single solve.
+// The sweep kernels only store the tile partials; batch_finish_kernel (one
+// CTA per system, batched.cu) reduces each system's partials in the same
+// order as a single solve and runs finish_sys, then finish_global.
 struct BatchRed {
   const int* tile_sys;    // system of each tile
   const int* sys_tile0;  // first tile of each system
   const int* sys_ntiles;  // tiles of each system
-  unsigned* sys_ticket;   // per-system completion tickets (reset by the finisher)
+  unsigned* sys_ticket;   // spare per-system counters
 };
 
 // per-tile system state of a batched op (act != 0: the tile's system runs)
@@ -268,56 +270,5 @@ template <class T, class = void>
 struct is_batched : std::false_type {};
 template <class T>
 struct is_batched<T, std::void_t<decltype(T::kBatched)>> : std::integral_constant<bool, T::kBatched> {};
-
-// After lane 0 wrote tile t's partials: count the tile for its system; the
-// CTA that completes the system reduces its partials and calls finish_sys.
-template <int NRED, class Epi>
-__device__ __forceinline__ void batch_tile_done(const RedCtx& red, Epi& epi, long t,
-                                                double* scratch, int* s_flag, int tid,
-                                                int bar_id) {
-  const BatchRed& br = epi.bred();
-  const int s = br.tile_sys[t];
-  if (tid == 0) {
-    __threadfence();
-    const unsigned tk = atomicAdd(&br.sys_ticket[s], 1u);
-    *s_flag = (tk == (unsigned)br.sys_ntiles[s] - 1u) ? 1 : 0;
-  }
-  named_bar_sync(bar_id, kLanes);
-  if (*s_flag) {
-    __threadfence();
-    double tot[NRED];
-    const long t0 = br.sys_tile0[s];
-    const long nt = br.sys_ntiles[s];
-#pragma unroll
-    for (int r = 0; r < NRED; ++r) {
-      double acc = 0.0;
-      const double* p = red.partials + (long)r * red.ntiles + t0;
-      for (long k = tid; k < nt; k += kLanes) acc = dadd(acc, __ldcg(p + k));
-      tot[r] = group_fold256(acc, scratch, tid, bar_id);
-    }
-    if (tid == 0) {
-      epi.finish_sys(s, tot);
-      br.sys_ticket[s] = 0u;
-    }
-  }
-  named_bar_sync(bar_id, kLanes);
-}
-
-// All CTAs arrive once; lane 0 of the last one calls finish_global.
-template <class Epi>
-__device__ __forceinline__ void batch_grid_done(const RedCtx& red, Epi& epi, int* s_flag, int tid,
-                                                int bar_id) {
-  if (tid == 0) {
-    __threadfence();
-    const unsigned tk = atomicAdd(red.ticket, 1u);
-    *s_flag = (tk == gridDim.x - 1) ? 1 : 0;
-  }
-  named_bar_sync(bar_id, kLanes);
-  if (*s_flag && tid == 0) {
-    __threadfence();
-    epi.finish_global();
-    *red.ticket = 0u;
-  }
-}
 
 }  // namespace celg

@@ -224,12 +224,10 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
         if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
       }
-      if constexpr (kB) batch_tile_done<(NR > 0 ? NR : 1)>(red, ep, t, scratch, s_flag, j, 1);
+      // batched: the systems are completed by batch_finish_kernel
     }
   }
-  if constexpr (kB) {
-    batch_grid_done(red, ep, s_flag, j, 1);
-  } else if (NR > 0) {
+  if constexpr (!kB && NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);
   }

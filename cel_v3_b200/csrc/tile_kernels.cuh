@@ -73,11 +73,11 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
         if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
       }
-      if constexpr (kB) batch_tile_done<(NR > 0 ? NR : 1)>(red, op, t, scratch, &s_flag, j, 1);
+      // batched: the systems are completed by batch_finish_kernel
     }
   }
   if constexpr (kB) {
-    batch_grid_done(red, op, &s_flag, j, 1);
+    // completed by batch_finish_kernel
   } else if constexpr (NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, &s_flag, j, 1)) op.finish(tot);
