@@ -575,7 +575,7 @@ template <class Op>
 static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
-  const int grid = grid_for_tiles(h, nt, 8);
+  const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile_kernel<Op>>(kLanes, 0)));
   mtile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;

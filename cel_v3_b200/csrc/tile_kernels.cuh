@@ -86,6 +86,22 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   }
 }
 
+// Resident CTAs per SM of a kernel at a fixed block size and dynamic shared
+// memory (queried once per kernel).
+template <auto Kern>
+int resident_per_sm(int threads, int smem) {
+  static int cached = 0;
+  if (!cached) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, Kern, threads, smem) != cudaSuccess)
+      per_sm = 1;
+    cached = std::max(1, per_sm);
+  }
+  return cached;
+}
+
+// The grid holds as many CTAs as are resident at once (no second wave: each
+// CTA walks its share of the tiles), at most blocks_per_sm per SM.
 template <class Op>
 int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
   const long nt = ntiles_of(n);
@@ -95,7 +111,8 @@ int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
     if (st) return st;
     red.partials = h->partials;
   }
-  const int grid = grid_for_tiles(h, nt, blocks_per_sm);
+  const int grid =
+      grid_for_tiles(h, nt, std::min(blocks_per_sm, resident_per_sm<tile_kernel<Op>>(kLanes, 0)));
   tile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, op, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
@@ -146,7 +163,7 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
-  const int grid = grid_for_tiles(h, nt, 8);
+  const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi>>(kLanes, 0)));
   jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
                                                     red);
   CELG_CUDA(cudaGetLastError());
