@@ -134,6 +134,45 @@ def build_problem():
     return rp, ci, v, x_true
 
 
+def distributed_form(h, celgpu, torch, stream, rp, ci, v, b, reps=2):
+    """The distributed PCG (celg_dist_* phases driven by cel_v3_b200.dist over
+    torch.distributed / NCCL) at world size 1 on the 256^3 system: the cost
+    of the phase API and its exchanges against the single-graph solve."""
+    import socket
+    import torch.distributed as td
+    from cel_v3_b200 import dist as D
+    own = not td.is_initialized()
+    if own:
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        import datetime
+        td.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                              timeout=datetime.timedelta(seconds=120))
+    try:
+        n = rp.size - 1
+        blk = D.RowBlock(rp, ci, v, [0, n], 0)
+        rk = D.GpuRank(h, blk, b.cpu().numpy(), eps_rel=EPS_REL, iter_max=5000)
+        comm = D.TorchComm()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        D.run_pcg([rk], comm, check_every=8)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            (res,) = D.run_pcg([rk], comm, check_every=8)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        rk.close()
+        return {"world": 1, "solves_per_s": 1e3 / ms, "ms": ms, "iters": res.iter_done,
+                "verified_relres": res.verified_relres, "status": res.status,
+                "exchanges_per_iteration": "1 halo (empty at world 1) + 2 all-reduces of 5 doubles",
+                "poll_every": 8}
+    finally:
+        if own:
+            td.destroy_process_group()
+
+
 def precision_form(h, celgpu, torch, stream, side=256, reps=2):
     """-div(k grad u) on side^3, k = exp(g), g ~ N(0,1) per face (seed 2),
     b ~ U[-1,1) (seed 3), assembled in device memory: plain FP64 PCG, FP32
@@ -509,11 +548,13 @@ def run_gpu(args):
 
     # ---- other precision forms on the same system (reported, not the value) ----
     forms = {}
-    if not args.quick:
+    # the other configurations are single-GPU measurements (run at N = 1)
+    if not args.quick and world == 1:
         forms["precision_diffusion256"] = precision_form(h, celgpu, torch, stream)
         forms["batched_64"] = batch_form(h, celgpu, torch, stream)
         forms["multirhs_128_k32"] = multirhs_form(h, celgpu, torch, stream)
         forms["differentiation_128_b8"] = differentiation_form(h, celgpu, torch, stream)
+        forms["distributed_phases_256"] = distributed_form(h, celgpu, torch, stream, rp, ci, v, b)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))
@@ -541,7 +582,7 @@ def run_gpu(args):
     assert ierr == 0, ierr
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(rp, ci, v, b.cpu().numpy(), iters)
 
     line = {
@@ -567,7 +608,7 @@ def run_gpu(args):
                 "api": "celg_elm_doit + celg_elm_collect_solution (pinned host b/x)",
                 "wall_s": wall_e2e},
         "forms": forms,
-        "gpu_launches": args.steps * (3 * iters + 3),
+        "gpu_launches": world * args.steps * (3 * iters + 3),
         "clocks": clk,
     }
     if cpu is not None:
