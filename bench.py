@@ -134,6 +134,56 @@ def build_problem():
     return rp, ci, v, x_true
 
 
+def plain_large_form(h, celgpu, torch, stream, m, b, x, iters_csr):
+    """The rest of the plain-large configuration: the SpMV bandwidth sweep at
+    64^3, 128^3 and 256^3 (CSR and JAD; the two smaller sizes fit the 126 MB
+    L2), Jacobi-PCG in JAD format and restarted GMRES(30)-Jacobi in CSR on
+    the 256^3 system, each to rel-res 1e-8."""
+    from cel_v3_b200 import synth
+    peak, _ = measured_peaks()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"spmv_sweep": {}}
+
+    def time_it(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, r
+
+    for side in (64, 128, 256):
+        rp, ci, v = synth.poisson7(side)
+        n, nnz = rp.size - 1, int(rp[-1])
+        mm = m if side == 256 else h.matrix_from_csr(rp, ci, v)
+        mm.to_jad()
+        xs = torch.from_numpy(np.random.default_rng(1).random(n)).cuda()
+        ys = torch.zeros(n, dtype=torch.float64, device="cuda")
+        row = {}
+        for name, fmt, nbytes in (("csr", celgpu.FMT_CSR, 12 * nnz + 4 * (n + 1) + 16 * n),
+                                  ("jad", celgpu.FMT_JAD, 12 * nnz + 4 * 8 + 20 * n)):
+            ms, _ = time_it(lambda: h.spmv(mm, xs.data_ptr(), ys.data_ptr(), fmt=fmt), 50)
+            gbs = nbytes / (ms / 1e3) / 1e9
+            row[name] = {"ms": ms, "gbs": gbs, "frac_of_measured": gbs / peak, "bytes": nbytes}
+        row["l2_resident"] = side < 256
+        out["spmv_sweep"][f"{side}^3"] = row
+        if mm is not m:
+            mm.destroy()
+    pj = celgpu.params(eps_rel=EPS_REL, iter_max=5000, x0_mode=celgpu.X0_ZERO, fmt=celgpu.FMT_JAD)
+    ms, inf = time_it(lambda: h.pcg_jacobi(m, b.data_ptr(), x.data_ptr(), pj), 2)
+    out["pcg_jad_256"] = {"solves_per_s": 1e3 / ms, "ms": ms, "iters": inf.iter_done,
+                          "verified_relres": inf.verified_relres, "status": inf.status,
+                          "csr_iters": iters_csr}
+    pg = celgpu.params(eps_rel=EPS_REL, iter_max=2000, x0_mode=celgpu.X0_ZERO, restart=30)
+    ms, inf = time_it(lambda: h.gmres_jacobi(m, b.data_ptr(), x.data_ptr(), pg), 1)
+    out["gmres30_csr_256"] = {"solves_per_s": 1e3 / ms, "ms": ms, "restarts": inf.iter_done,
+                              "arnoldi_steps": inf.arnoldi_steps,
+                              "verified_relres": inf.verified_relres, "status": inf.status}
+    return out
+
+
 def distributed_form(h, celgpu, torch, stream, rp, ci, v, b, reps=2):
     """The distributed PCG (celg_dist_* phases driven by cel_v3_b200.dist over
     torch.distributed / NCCL) at world size 1 on the 256^3 system: the cost
@@ -409,11 +459,18 @@ def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
     R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=k, red=red, nworkers=workers)
     t = time.perf_counter() - t0
     per_iter = t / (k + 1)  # set-up sweep ~ one iteration
+    # the deterministic one-worker setting (the oracle's sequential order)
+    t0 = time.perf_counter()
+    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=4, red=red, nworkers=1)
+    t1 = time.perf_counter() - t0
     return {"value": 1.0 / (per_iter * iters_per_solve), "unit": UNIT, "cores": cores,
             "threads": workers + 1, "kind": "port",
             "sample": f"oracle Jacobi-PCG (reference order, {workers} workers + idle master) on the "
                       f"256^3 system: {k} iterations in {t:.2f} s, scaled by {iters_per_solve} "
-                      f"iterations per solve"}
+                      f"iterations per solve",
+            "one_worker": {"value": 1.0 / (t1 / 5 * iters_per_solve), "unit": UNIT, "threads": 1,
+                           "sample": f"4 iterations + set-up in {t1:.2f} s, scaled by "
+                                     f"{iters_per_solve} iterations per solve"}}
 
 
 def run_reference(args):
@@ -555,6 +612,7 @@ def run_gpu(args):
         forms["multirhs_128_k32"] = multirhs_form(h, celgpu, torch, stream)
         forms["differentiation_128_b8"] = differentiation_form(h, celgpu, torch, stream)
         forms["distributed_phases_256"] = distributed_form(h, celgpu, torch, stream, rp, ci, v, b)
+        forms["plain_large_256"] = plain_large_form(h, celgpu, torch, stream, m, b, x, iters)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))
