@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
 }
 
 template <class Epi>
-__global__ void __launch_bounds__(kLanes)
+__global__ void __launch_bounds__(kLanes, 3)
     jad_kernel(const int* __restrict__ jb, const int* __restrict__ jci,
                const double* __restrict__ jv, const int* __restrict__ perm, int n, int mmax,
                const double* __restrict__ x, Epi epi, RedCtx red) {
@@ -255,17 +255,39 @@ __global__ void __launch_bounds__(kLanes)
       i[k] = t * kTile + (long)k * kLanes + j;
       sum[k] = 0.0;
     }
-    for (int d = 0; d < mmax; ++d) {
-      const int beg = __ldg(jb + d);
-      const int len = __ldg(jb + d + 1) - beg;
-      if (i[0] >= len) break;  // permuted rows are sorted by decreasing length
+    // diagonals in groups of kJadDiag: every load of the group (values,
+    // columns, then the x gathers) is issued before the group's adds, which
+    // keep the diagonal order of each row
+    constexpr int kJadDiag = 2;
+    for (int d = 0; d < mmax; d += kJadDiag) {
+      int beg[kJadDiag], len[kJadDiag];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        if (i[k] < len) {
-          const long q = beg + i[k];
-          sum[k] = dadd(sum[k], dmul(__ldg(jv + q), __ldg(x + __ldg(jci + q))));
-        }
+      for (int g = 0; g < kJadDiag; ++g) {
+        const bool ok = d + g < mmax;
+        beg[g] = ok ? __ldg(jb + d + g) : 0;
+        len[g] = ok ? __ldg(jb + d + g + 1) - beg[g] : 0;
       }
+      if (i[0] >= len[0]) break;  // permuted rows are sorted by decreasing length
+      int col[kJadDiag][4];
+      double vv[kJadDiag][4], xv[kJadDiag][4];
+#pragma unroll
+      for (int g = 0; g < kJadDiag; ++g)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (i[k] < len[g]) {
+            col[g][k] = __ldg(jci + beg[g] + i[k]);
+            vv[g][k] = __ldg(jv + beg[g] + i[k]);
+          }
+#pragma unroll
+      for (int g = 0; g < kJadDiag; ++g)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (i[k] < len[g]) xv[g][k] = __ldg(x + col[g][k]);
+#pragma unroll
+      for (int g = 0; g < kJadDiag; ++g)
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (i[k] < len[g]) sum[k] = dadd(sum[k], dmul(vv[g][k], xv[g][k]));
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
