@@ -292,8 +292,17 @@ def batch_form(h, celgpu, torch, stream):
     def batched():
         return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p)
 
+    # the FP32-refinement variant: FP32 inner solves (tol 1e-4) inside FP64
+    # refinement of every system, to the same FP64-verified 1e-8
+    p32 = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO,
+                        precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4, inner_iter_max=5000)
+
+    def batched_fp32_ir():
+        return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p32)
+
     out = {}
-    for name, fn in (("one_by_one", one_by_one), ("batched", batched)):
+    for name, fn in (("one_by_one", one_by_one), ("batched", batched),
+                     ("batched_fp32_ir", batched_fp32_ir)):
         fn()
         torch.cuda.synchronize()
         reps = 3
@@ -309,6 +318,8 @@ def batch_form(h, celgpu, torch, stream):
                      "worst_verified_relres": max(i.verified_relres for i in infos),
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
     out["speedup_batched_vs_one_by_one"] = out["batched"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
+    out["speedup_batched_fp32_ir_vs_one_by_one"] = (out["batched_fp32_ir"]["solves_per_s"] /
+                                                    out["one_by_one"]["solves_per_s"])
     out["systems"] = len(mats)
     out["rows"] = int(sum(s ** 3 for s, *_ in probs))
     for m in mats:

@@ -48,16 +48,21 @@ struct BatchArgs {
   __device__ int sys_of(long t) const { return br.tile_sys[t]; }
 };
 
-// x0, ||b|| and eps per system
+// x0, ||b|| and eps per system.  With `part` set (the refinement's inner
+// solves) only the systems with part[s] != 0 take part; n_active is then
+// *part_count.
+template <typename VT>
 struct BOpPre {
   static constexpr int NRED = 1;
   static constexpr bool kBatched = true;
-  struct Regs { double b; };
-  const double* b;
-  double* x;
+  struct Regs { VT b; };
+  const VT* b;
+  VT* x;
   int x0_mode;
   double eps_abs, eps_rel;
   BatchArgs a;
+  const int* part = nullptr;
+  const int* part_count = nullptr;
   __device__ bool prepare() { return true; }
   __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
   __device__ void begin_tile(const TileInfo&) {}
@@ -65,9 +70,9 @@ struct BOpPre {
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.b = __ldg(b + i); }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    if (x0_mode == CELG_X0_REF_ONES) x[i] = 1.0;
-    else if (x0_mode == CELG_X0_ZERO) x[i] = 0.0;
-    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+    if (x0_mode == CELG_X0_REF_ONES) x[i] = VT(1);
+    else if (x0_mode == CELG_X0_ZERO) x[i] = VT(0);
+    acc[0] = dadd(acc[0], dmul(D(g.b), D(g.b)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     a.bnorm[s] = sqrt(tot[0]);
@@ -76,33 +81,36 @@ struct BOpPre {
     a.eps[s] = e;
     a.err[s] = 0;
     a.iter[s] = 0;
-    a.active[s] = 1;
+    a.active[s] = part ? (part[s] ? 1 : 0) : 1;
     a.vres[s] = 0.0;
   }
-  __device__ void finish_global() const { *a.n_active = a.nlive; }
+  __device__ void finish_global() const { *a.n_active = part_count ? *part_count : a.nlive; }
 };
 
-// r = b - (0 + A x); p = J r; alpha = r.p; ||r||
+// r = b - (0 + A x); p = J r; alpha = r.p; ||r||  (systems set active by BOpPre)
+template <typename VT>
 struct BEpiInit {
   static constexpr int NRED = 2;
   static constexpr bool kBatched = true;
-  const double* b;
-  double* r;
-  double* p;
-  const double* J;
+  const VT* b;
+  VT* r;
+  VT* p;
+  const VT* J;
   BatchArgs a;
   __device__ bool active() const { return true; }
-  __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
+  __device__ TileInfo tile_info(long t) const {
+    return TileInfo{*(volatile int*)&a.active[a.sys_of(t)], 0.0};
+  }
   __device__ void begin_tile(const TileInfo&) {}
-  __device__ bool sys_active(int) const { return true; }
+  __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
-  __device__ void row(long i, double s, double* acc) const {
-    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+  __device__ void row(long i, VT s, double* acc) const {
+    const VT ri = R<VT>(__dsub_rn(D(b[i]), D(vadd(VT(0), s))));
     r[i] = ri;
-    const double z = dmul(ri, J[i]);
-    p[i] = z;
-    acc[0] = dadd(acc[0], dmul(ri, z));
-    acc[1] = dadd(acc[1], dmul(ri, ri));
+    const double z = dmul(D(ri), D(J[i]));
+    p[i] = R<VT>(z);
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     a.alpha[s] = tot[0];
@@ -114,11 +122,12 @@ struct BEpiInit {
 };
 
 // K1: v = 0 + A p; pv = v.p; sigma = alpha / pv
+template <typename VT>
 struct BEpiAp {
   static constexpr int NRED = 1;
   static constexpr bool kBatched = true;
-  double* v;
-  const double* p;
+  VT* v;
+  const VT* p;
   BatchArgs a;
   __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
   __device__ TileInfo tile_info(long t) const {
@@ -127,12 +136,12 @@ struct BEpiAp {
   __device__ void begin_tile(const TileInfo&) {}
   __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
-  struct Pre { double p; };
+  struct Pre { VT p; };
   __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
-  __device__ void row(long i, double s, const Pre& g, double* acc) const {
-    const double vi = dadd(0.0, s);
+  __device__ void row(long i, VT s, const Pre& g, double* acc) const {
+    const VT vi = vadd(VT(0), s);
     v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, g.p));
+    acc[0] = dadd(acc[0], dmul(D(vi), D(g.p)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     const double sg = a.alpha[s] / tot[0];
@@ -147,15 +156,16 @@ struct BEpiAp {
 };
 
 // K2: x += sigma p; r += (-sigma) v; rz, rr; scalars and per-system test
+template <typename VT>
 struct BOpUpdate {
   static constexpr int NRED = 2;
   static constexpr bool kBatched = true;
-  struct Regs { double x, r, p, v, J; };
-  double* x;
-  double* r;
-  const double* p;
-  const double* v;
-  const double* J;
+  struct Regs { VT x, r, p, v, J; };
+  VT* x;
+  VT* r;
+  const VT* p;
+  const VT* v;
+  const VT* J;
   BatchArgs a;
   double sg;
   __device__ bool prepare() { return true; }
@@ -174,12 +184,12 @@ struct BOpUpdate {
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    x[i] = dadd(g.x, dmul(sg, g.p));
-    const double ri = dadd(g.r, dmul(-sg, g.v));
+    x[i] = R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
+    const VT ri = R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     r[i] = ri;
-    const double z = dmul(ri, g.J);
-    acc[0] = dadd(acc[0], dmul(ri, z));
-    acc[1] = dadd(acc[1], dmul(ri, ri));
+    const double z = dmul(D(ri), D(g.J));
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     a.beta[s] = tot[0] / a.alpha[s];
@@ -192,13 +202,14 @@ struct BOpUpdate {
 };
 
 // K3: p = beta p + J r
+template <typename VT>
 struct BOpDirection {
   static constexpr int NRED = 0;
   static constexpr bool kBatched = true;
-  struct Regs { double p, r, J; };
-  double* p;
-  const double* r;
-  const double* J;
+  struct Regs { VT p, r, J; };
+  VT* p;
+  const VT* r;
+  const VT* J;
   BatchArgs a;
   double bt;
   __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
@@ -211,7 +222,7 @@ struct BOpDirection {
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
   __device__ void compute(long i, Regs& g, double*) const {
-    p[i] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
+    p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
   __device__ void finish_sys(int, double*) const {}
   __device__ void finish_global() const {}
@@ -237,6 +248,125 @@ struct BEpiVerify {
   }
   __device__ void finish_global() const {}
 };
+
+// ---- FP32 refinement of every system (celg_pcg_batched, CELG_PREC_FP32_IR) -------
+//
+// The outer loop of ir_solve (ir.cu) run for all systems at once: each
+// system keeps its own residual norm, outer count and status, and the outer
+// steps of the systems that are still refining advance together.
+
+struct IrState {
+  int* part;         // system needs an inner solve in this outer step
+  int* done;         // system finished (status set)
+  int* status;       // CELG_OK / CELG_ERR_* per system
+  int* outer;        // completed outer steps
+  int* inner_total;  // inner iterations over all outer steps
+  int* part_count;
+  int outer_max;
+};
+
+// r = b - (0 + A x) in FP64, ||r|| per system; the system's outer decision
+struct BEpiIrResidual {
+  static constexpr int NRED = 1;
+  static constexpr bool kBatched = true;
+  const double* b;
+  double* r;
+  BatchArgs a;  // outer state: norm[s] = ||r||, eps[s] = tolerance
+  IrState ir;
+  __device__ bool active() const { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    return TileInfo{*(volatile int*)&ir.done[a.sys_of(t)] == 0 ? 1 : 0, 0.0};
+  }
+  __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int s) const { return *(volatile int*)&ir.done[s] == 0; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double ri = __dsub_rn(b[i], dadd(0.0, s));
+    r[i] = ri;
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    const double rn = sqrt(tot[0]);
+    a.norm[s] = rn;
+    int st = -1;
+    if (rn <= a.eps[s]) st = CELG_OK;
+    else if (!isfinite(rn)) st = kErrBreakdown;
+    else if (ir.outer[s] >= ir.outer_max) st = CELG_ERR_NOCONV;
+    if (st >= 0) {
+      ir.done[s] = 1;
+      ir.status[s] = st;
+    } else {
+      ir.part[s] = 1;
+      atomicAdd(ir.part_count, 1);
+    }
+  }
+  __device__ void finish_global() const {}
+};
+
+// r32 = (float)(r * (1/||r||)) for the systems that refine
+struct BOpIrToF32 {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { double r; };
+  const double* r;
+  float* r32;
+  BatchArgs a;
+  IrState ir;
+  double inv;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    return TileInfo{*(volatile int*)&ir.part[s], 1.0 / a.norm[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) { inv = ti.s; }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const { g.r = __ldg(r + i); }
+  __device__ void compute(long i, Regs& g, double*) const { r32[i] = (float)dmul(g.r, inv); }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// x = x + ||r|| * (double) d32 for the systems that refined
+struct BOpIrAdd {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { double x; float d; };
+  double* x;
+  const float* d;
+  BatchArgs a;
+  IrState ir;
+  double scale;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    return TileInfo{*(volatile int*)&ir.part[s], a.norm[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) { scale = ti.s; }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const { g.x = x[i]; g.d = __ldg(d + i); }
+  __device__ void compute(long i, Regs& g, double*) const { x[i] = dadd(g.x, dmul(scale, (double)g.d)); }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// after an inner solve (before the update): count the inner iterations; an
+// inner failure other than the iteration cap ends the system with that
+// status and without the update, otherwise the outer step counts
+__global__ void ir_count_kernel(int nsys, IrState ir, const int* inner_iter, const int* inner_err) {
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nsys; s += gridDim.x * blockDim.x) {
+    if (!ir.part[s]) continue;
+    ir.inner_total[s] += inner_iter[s];
+    if (inner_err[s] != 0) {
+      ir.done[s] = 1;
+      ir.status[s] = inner_err[s];
+      ir.part[s] = 0;
+    } else {
+      ir.outer[s] += 1;
+    }
+  }
+}
 
 // ---- completion of a batched sweep ------------------------------------------------
 
@@ -313,6 +443,12 @@ struct Batch {
   int nlive = 0;               // systems with at least one row
   std::vector<long> row_off;
   std::vector<int> n;
+  // FP32 refinement (allocated on first use): A.v32 holds the FP32 values
+  float* J32 = nullptr;
+  float* F = nullptr;          // 5 x N floats: B32 D32 R32 P32 V32
+  int* irs = nullptr;          // part, done, status, outer, inner_total (nsys each), part_count
+  double* dstate2 = nullptr;   // inner-solve scalars, 7 x nsys
+  int* istate2 = nullptr;      // inner-solve counters, 3 x nsys + 1
 };
 
 namespace celg {
@@ -328,6 +464,12 @@ void batch_free(Batch* b) {
   cudaFree(b->sys_ticket);
   cudaFree(b->dstate);
   cudaFree(b->istate);
+  cudaFree(b->A.v32);
+  cudaFree(b->J32);
+  cudaFree(b->F);
+  cudaFree(b->irs);
+  cudaFree(b->dstate2);
+  cudaFree(b->istate2);
   delete b;
 }
 
@@ -426,17 +568,18 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
   return CELG_OK;
 }
 
-static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle cond, const int* errw) {
+static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle cond, const int* errw,
+                            bool inner = false) {
   BatchArgs a;
   const int c = bt->nsys;
-  a.alpha = bt->dstate;
+  a.alpha = inner ? bt->dstate2 : bt->dstate;
   a.sigma = a.alpha + c;
   a.beta = a.sigma + c;
   a.norm = a.beta + c;
   a.bnorm = a.norm + c;
   a.eps = a.bnorm + c;
   a.vres = a.eps + c;
-  a.iter = bt->istate;
+  a.iter = inner ? bt->istate2 : bt->istate;
   a.active = a.iter + c;
   a.err = a.active + c;
   a.n_active = a.err + c;
@@ -474,10 +617,10 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
       CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
                                 cudaMemcpyDeviceToDevice, h->stream));
   }
-  const BOpPre pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
-  const BEpiInit init{bt->B, bt->R, bt->P, bt->J, a};
-  const BEpiAp ap{bt->V, bt->P, a};
-  const BOpUpdate upd{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0};
+  const BOpPre<double> pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
+  const BEpiInit<double> init{bt->B, bt->R, bt->P, bt->J, a};
+  const BEpiAp<double> ap{bt->V, bt->P, a};
+  const BOpUpdate<double> upd{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0};
   int st = launch_tile(h, N, pre);
   if (!st) st = batch_finish(h, bt, pre);
   if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, init);
@@ -487,7 +630,7 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
     if (!s2) s2 = batch_finish(h, bt, ap);
     if (!s2) s2 = launch_tile(h, N, upd);
     if (!s2) s2 = batch_finish(h, bt, upd);
-    if (!s2) s2 = launch_tile(h, N, BOpDirection{bt->P, bt->R, bt->J, a, 0.0});
+    if (!s2) s2 = launch_tile(h, N, BOpDirection<double>{bt->P, bt->R, bt->J, a, 0.0});
     return s2;
   };
   if (!st && a.cond) st = capture_while(h, a.cond, body);
@@ -512,8 +655,9 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
   return CELG_OK;
 }
 
-int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
-                double* const* x_d, const celg_params* p, celg_result* res) {
+// The handle's concatenated batch for these matrices (built on first use).
+static int batch_for(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                     double* const* x_d, Batch** out) {
   std::string mkey = "batch";
   char buf[64];
   for (int s = 0; s < count; ++s) {
@@ -532,7 +676,23 @@ int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* 
     if (st) return st;
     h->batch = bt;
   }
-  int st = ensure_partials(h, bt->NT, 2);
+  *out = bt;
+  return CELG_OK;
+}
+
+static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                          double* const* x_d, const celg_params* p, celg_result* res);
+
+int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                double* const* x_d, const celg_params* p, celg_result* res) {
+  if (p->precision == CELG_PREC_FP32_IR) return pcg_batched_ir(h, count, mats, b_d, x_d, p, res);
+  if (p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
+  Batch* bt = nullptr;
+  int st = batch_for(h, count, mats, b_d, x_d, &bt);
+  if (st) return st;
+  char buf[64];
+  const std::string& mkey = bt->key;
+  st = ensure_partials(h, bt->NT, 2);
   if (st) return st;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
   std::string gkey = mkey;
@@ -598,6 +758,190 @@ int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* 
     }
   }
   h->last_iters = iters;
+  return ret;
+}
+
+// FP32 refinement of every system: the outer loop of ir_solve (ir.cu) for
+// all systems at once, each system's inner FP32 Jacobi-PCG in one batched
+// inner solve (a graph with a WHILE node, captured once).  Each system's
+// result equals ir_solve on that system alone, bit for bit.
+static int batch_ensure_f32(celg_handle* h, Batch* bt) {
+  if (bt->F) return CELG_OK;
+  const size_t N = (size_t)std::max(1L, bt->N), NNZ = (size_t)bt->A.nnz, c = (size_t)bt->nsys;
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
+  ok(cudaMalloc(&bt->A.v32, sizeof(float) * (NNZ + 32)));
+  ok(cudaMalloc(&bt->J32, sizeof(float) * N));
+  ok(cudaMalloc(&bt->F, sizeof(float) * N * 5));
+  ok(cudaMalloc(&bt->irs, sizeof(int) * (5 * c + 1)));
+  ok(cudaMalloc(&bt->dstate2, sizeof(double) * 7 * c));
+  ok(cudaMalloc(&bt->istate2, sizeof(int) * (3 * c + 1)));
+  ok(cudaMemsetAsync(bt->F, 0, sizeof(float) * N * 5, h->stream));
+  ok(cudaMemsetAsync(bt->A.v32 + NNZ, 0, sizeof(float) * 32, h->stream));
+  if (e != cudaSuccess) return cuda_status(e, "batch FP32 allocation");
+  int st = launch_to_f32(h, (long)NNZ, bt->A.v, bt->A.v32);
+  if (!st && bt->N > 0) st = launch_to_f32(h, bt->N, bt->J, bt->J32);
+  return st;
+}
+
+template <class Body>
+static int run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int* n_active, int iter_max,
+                     Body&& body) {
+  if (cond) return capture_while(h, cond, body);
+  for (int it = 0; it < iter_max; it += 8) {
+    int st = CELG_OK;
+    for (int q = 0; q < 8 && !st; ++q) st = body();
+    if (st) return st;
+    int live = 0;
+    CELG_CUDA(cudaMemcpyAsync(&live, n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    if (!live) break;
+  }
+  return CELG_OK;
+}
+
+static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, BatchArgs ai,
+                                double inner_eps_rel) {
+  const long N = bt->N;
+  float* B32 = bt->F;
+  float* D32 = B32 + N;
+  float* R32 = D32 + N;
+  float* P32 = R32 + N;
+  float* V32 = P32 + N;
+  const BOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps_rel, ai, ir.part, ir.part_count};
+  const BEpiInit<float> init{B32, R32, P32, bt->J32, ai};
+  const BEpiAp<float> ap{V32, P32, ai};
+  const BOpUpdate<float> upd{D32, R32, P32, V32, bt->J32, ai, 0.0};
+  int st = launch_tile(h, N, pre);
+  if (!st) st = batch_finish(h, bt, pre);
+  if (!st) st = launch_csr<float>(h, bt->A, bt->A.v32, D32, init);
+  if (!st) st = batch_finish(h, bt, init);
+  if (!st)
+    st = run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
+      int s2 = launch_csr<float>(h, bt->A, bt->A.v32, P32, ap);
+      if (!s2) s2 = batch_finish(h, bt, ap);
+      if (!s2) s2 = launch_tile(h, N, upd);
+      if (!s2) s2 = batch_finish(h, bt, upd);
+      if (!s2) s2 = launch_tile(h, N, BOpDirection<float>{P32, R32, bt->J32, ai, 0.0});
+      return s2;
+    });
+  return st;
+}
+
+static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                          double* const* x_d, const celg_params* p, celg_result* res) {
+  Batch* bt = nullptr;
+  int st = batch_for(h, count, mats, b_d, x_d, &bt);
+  if (!st) st = ensure_partials(h, bt->NT, 2);
+  if (!st) st = batch_ensure_f32(h, bt);
+  if (st) return st;
+  const long N = bt->N;
+  const int c = bt->nsys;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  const int inner_max = p->inner_iter_max > 0 ? p->inner_iter_max : 1000;
+  const double inner_eps = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-4;
+  IrState ir;
+  ir.part = bt->irs;
+  ir.done = ir.part + c;
+  ir.status = ir.done + c;
+  ir.outer = ir.status + c;
+  ir.inner_total = ir.outer + c;
+  ir.part_count = ir.inner_total + c;
+  ir.outer_max = p->outer_max > 0 ? p->outer_max : 20;
+  const BatchArgs a = batch_args(bt, p->iter_max, 0, h->err_d);
+  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  for (int s = 0; s < c; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(bt->B + bt->row_off[s], b_d[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+    if (p->x0_mode == CELG_X0_USER)
+      CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
+                                cudaMemcpyDeviceToDevice, h->stream));
+  }
+  // x0, ||b|| and the tolerance per system
+  const BOpPre<double> pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
+  st = launch_tile(h, N, pre);
+  if (!st) st = batch_finish(h, bt, pre);
+  CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * (5 * (size_t)c + 1), h->stream));
+  // systems with no rows take no part at all
+  std::vector<int> done0((size_t)c, 0);
+  for (int s = 0; s < c; ++s) done0[(size_t)s] = bt->n[s] == 0 ? 1 : 0;
+  CELG_CUDA(cudaMemcpyAsync(ir.done, done0.data(), sizeof(int) * (size_t)c, cudaMemcpyHostToDevice,
+                            h->stream));
+  const BatchArgs ai_host = batch_args(bt, inner_max, 0, h->err_d, true);
+  char kb[96];
+  std::snprintf(kb, sizeof(kb), "|ir|%d|%.17g", inner_max, inner_eps);
+  const std::string gkey = bt->key + kb;
+  for (int k = 0; !st && k <= ir.outer_max; ++k) {
+    CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * (size_t)c, h->stream));
+    CELG_CUDA(cudaMemsetAsync(ir.part_count, 0, sizeof(int), h->stream));
+    const BEpiIrResidual res_op{bt->B, bt->R, a, ir};
+    st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, res_op);
+    if (!st) st = batch_finish(h, bt, res_op);
+    if (st) break;
+    int parts = 0;
+    CELG_CUDA(cudaMemcpyAsync(&parts, ir.part_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    if (parts == 0) break;
+    st = launch_tile(h, N, BOpIrToF32{bt->R, bt->F, a, ir, 0.0});
+    if (st) break;
+    if (graphs_enabled()) {
+      GraphEntry* ge = graph_cache_find(h, gkey);
+      if (!ge) {
+        st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
+          return record_batched_inner(h, bt, ir, batch_args(bt, inner_max, cond, h->err_d, true),
+                                      inner_eps);
+        }, &ge);
+        if (st) break;
+      }
+      CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    } else {
+      st = record_batched_inner(h, bt, ir, ai_host, inner_eps);
+      if (st) break;
+    }
+    ir_count_kernel<<<(c + 127) / 128, 128, 0, h->stream>>>(c, ir, ai_host.iter, ai_host.err);
+    CELG_CUDA(cudaGetLastError());
+    st = launch_tile(h, N, BOpIrAdd{bt->X, bt->F + N, a, ir, 0.0});
+  }
+  if (st) return st;
+  for (int s = 0; s < c; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(x_d[s], bt->X + bt->row_off[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+  }
+  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  std::vector<double> ds(7 * (size_t)c);
+  std::vector<int> is(5 * (size_t)c + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), bt->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), ir.part, sizeof(int) * is.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, inner_max_total = 0;
+  for (int s = 0; s < c; ++s) {
+    const int done = is[(size_t)c + s], status = is[2 * (size_t)c + s];
+    const int outer = is[3 * (size_t)c + s], inner = is[4 * (size_t)c + s];
+    const double rn = ds[3 * (size_t)c + s], bn = ds[4 * (size_t)c + s];
+    int rs = done ? status : CELG_ERR_NOCONV;
+    if (bt->n[s] == 0) rs = CELG_OK;
+    if (rs && !ret) ret = rs;
+    inner_max_total = std::max(inner_max_total, inner);
+    if (res) {
+      std::memset(&res[s], 0, offsetof(celg_result, history));
+      res[s].iter_done = outer;
+      res[s].final_norm2 = rn;
+      res[s].bnorm = bn;
+      res[s].verified_relres = bn > 0 ? rn / bn : rn;
+      res[s].err = rs;
+      res[s].arnoldi_steps = inner;
+      res[s].history_len = 0;
+    }
+  }
+  h->last_iters = inner_max_total;
   return ret;
 }
 

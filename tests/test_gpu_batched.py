@@ -73,3 +73,31 @@ def test_batched_with_empty_system_and_cap(gpu):
     assert infos[3].iter_done == 0 and infos[3].status == celgpu.OK
     for m in mats + [empty]:
         m.destroy()
+
+
+@pytest.mark.parametrize("mode", ["graph", "host_loop"])
+def test_batched_fp32_refinement_matches_single_refinement(gpu, mode, monkeypatch):
+    """FP32 refinement of the whole batch (CELG_PREC_FP32_IR): each system's
+    solution, outer and inner iteration counts and verified residual equal
+    the single-system refinement's bit for bit."""
+    celgpu, h, torch = gpu
+    if mode == "host_loop":
+        monkeypatch.setenv("CELG_GRAPH", "0")
+    sy = systems()
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+    bs = [dev(torch, b) for *_, b in sy]
+    xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    kw = dict(eps_rel=1e-10, iter_max=3000, precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4,
+              inner_iter_max=1500, outer_max=20, x0_mode=celgpu.X0_ZERO)
+    infos = h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], **kw)
+    for s, ((rp, ci, v, b), m) in enumerate(zip(sy, mats)):
+        xo = dev(torch, np.zeros(b.size))
+        one = h.pcg_jacobi(m, bs[s].data_ptr(), xo.data_ptr(), **kw)
+        assert infos[s].status == one.status == celgpu.OK, s
+        assert infos[s].iter_done == one.iter_done, s            # outer steps
+        assert infos[s].arnoldi_steps == one.arnoldi_steps, s    # inner iterations
+        assert infos[s].verified_relres == one.verified_relres, s
+        assert infos[s].verified_relres <= 1e-10
+        assert np.array_equal(xs[s].cpu().numpy(), xo.cpu().numpy()), s
+    for m in mats:
+        m.destroy()
