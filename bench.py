@@ -341,8 +341,11 @@ def multirhs_form(h, celgpu, torch, stream):
     p = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {}
+    p32 = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO,
+                        precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4, inner_iter_max=5000)
     runs = (("one_by_one", lambda: [h.pcg_jacobi(m, c.data_ptr(), x.data_ptr(), p) for c, x in zip(cols, xs)]),
-            ("multirhs", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p)))
+            ("multirhs", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p)),
+            ("multirhs_fp32_ir", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p32)))
     for name, fn in runs:
         fn()
         torch.cuda.synchronize()
@@ -358,6 +361,8 @@ def multirhs_form(h, celgpu, torch, stream):
                      "worst_verified_relres": max(i.verified_relres for i in infos),
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
+    out["speedup_multirhs_fp32_ir_vs_one_by_one"] = (out["multirhs_fp32_ir"]["solves_per_s"] /
+                                                     out["one_by_one"]["solves_per_s"])
     m.destroy()
     return out
 

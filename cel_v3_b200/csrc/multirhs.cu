@@ -126,14 +126,14 @@ constexpr int kAsyncU = 8;                    // gathers per row slot
 // the row's U matrix values (padded to 16 bytes)
 constexpr int kAsyncSlot = (kAsyncU + 2) * 32 + ((kAsyncU + 1) & ~1);
 
-template <int U>
-__device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const double* __restrict__ X,
-                                            int b, int e, int k, int lane, bool on, double (&x)[U]) {
+template <int U, typename VT>
+__device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const VT* __restrict__ X,
+                                            int b, int e, int k, int lane, bool on, VT (&x)[U]) {
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     if (b + u < e) {
       const int c = __ldg(ci + b + u);
-      x[u] = on ? __ldg(X + (long)c * k + lane) : 0.0;
+      x[u] = on ? __ldg(X + (long)c * k + lane) : VT(0);
     }
   }
 }
@@ -141,9 +141,11 @@ __device__ __forceinline__ void spmm_gather(const int* __restrict__ ci, const do
 template <class Epi, int MINB, int U>
 __global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restrict__ rp,
                                                             const int* __restrict__ ci,
-                                                            const double* __restrict__ v, int n,
-                                                            int k, const double* __restrict__ X,
+                                                            const typename Epi::VT* __restrict__ v,
+                                                            int n, int k,
+                                                            const typename Epi::VT* __restrict__ X,
                                                             Epi epi, RedCtx red) {
+  using VT = typename Epi::VT;
   constexpr int NR = Epi::NRED;
   constexpr unsigned kFull = 0xffffffffu;
   __shared__ double s_w[(NR > 0 ? NR : 1) * 8 * 32];
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restric
       const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
       int bA = __ldg(rp + row0);
       int eA = __shfl_sync(kFull, re, 0);
-      double xA[U];
+      VT xA[U];
       spmm_gather<U>(ci, X, bA, eA, k, lane, on, xA);
       typename Epi::Pre preA;
       if (on) preA = epi.pre(row0, lane);
@@ -173,22 +175,22 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_kernel(const int* __restric
         const bool more = r + 1 < nrows;
         const int bB = eA;
         const int eB = __shfl_sync(kFull, re, more ? r + 1 : r);
-        double xB[U];
+        VT xB[U];
         typename Epi::Pre preB;
         if (more) {
           spmm_gather<U>(ci, X, bB, eB, k, lane, on, xB);
           if (on) preB = epi.pre(row0 + r + 1, lane);
         }
-        double sum = 0.0;
+        VT sum = VT(0);
 #pragma unroll
         for (int u = 0; u < U; ++u)
-          if (bA + u < eA) sum = dadd(sum, dmul(__ldg(v + bA + u), xA[u]));
+          if (bA + u < eA) sum = vadd(sum, vmul(__ldg(v + bA + u), xA[u]));
         for (int kk = bA + U; kk < eA; kk += U) {  // rows longer than U entries
-          double xv[U];
+          VT xv[U];
           spmm_gather<U>(ci, X, kk, eA, k, lane, on, xv);
 #pragma unroll
           for (int u = 0; u < U; ++u)
-            if (kk + u < eA) sum = dadd(sum, dmul(__ldg(v + kk + u), xv[u]));
+            if (kk + u < eA) sum = vadd(sum, vmul(__ldg(v + kk + u), xv[u]));
         }
         if (on) epi.row(row0 + r, lane, sum, preA, acc);
         bA = bB;
@@ -338,23 +340,28 @@ __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, 
 
 // ---- the sweeps of the multi-column PCG ------------------------------------------
 
-// x0 and ||b|| per column
+// x0 and ||b|| per column.  With `part` set (the refinement's inner solves)
+// only the columns with part[c] != 0 take part; n_active is then
+// *part_count.
+template <typename VT>
 struct MOpPre {
   static constexpr int NRED = 1;
-  struct Regs { double b; };
-  const double* B;
-  double* X;
+  struct Regs { VT b; };
+  const VT* B;
+  VT* X;
   int x0_mode;
   double eps_abs, eps_rel;
   MultiArgs a;
+  const int* part = nullptr;
+  const int* part_count = nullptr;
   __device__ bool prepare() { return true; }
   __device__ bool col_active(int) const { return true; }
   __device__ void begin_col(int) {}
   __device__ void load(long e, long, Regs& g) const { g.b = __ldg(B + e); }
   __device__ void compute(long e, long, Regs& g, double* acc) const {
-    if (x0_mode == CELG_X0_REF_ONES) X[e] = 1.0;
-    else if (x0_mode == CELG_X0_ZERO) X[e] = 0.0;
-    acc[0] = dadd(acc[0], dmul(g.b, g.b));
+    if (x0_mode == CELG_X0_REF_ONES) X[e] = VT(1);
+    else if (x0_mode == CELG_X0_ZERO) X[e] = VT(0);
+    acc[0] = dadd(acc[0], dmul(D(g.b), D(g.b)));
   }
   __device__ void finish_col(int c, double* tot) const {
     a.bnorm[c] = sqrt(tot[0]);
@@ -363,40 +370,43 @@ struct MOpPre {
     a.eps[c] = e;
     a.err[c] = 0;
     a.iter[c] = 0;
-    a.active[c] = 1;
+    a.active[c] = part ? (part[c] ? 1 : 0) : 1;
     a.vres[c] = 0.0;
   }
-  __device__ void finish_global() const { *a.n_active = a.k; }
+  __device__ void finish_global() const { *a.n_active = part_count ? *part_count : a.k; }
 };
 
-// r = b - (0 + A x); p = J r; alpha = r.p; ||r||
+// r = b - (0 + A x); p = J r; alpha = r.p; ||r||  (columns set active by MOpPre)
+template <typename VT_>
 struct MEpiInit {
+  using VT = VT_;
   static constexpr int NRED = 2;
-  const double* B;
-  double* R;
-  double* P;
-  const double* J;
+  const VT* B;
+  VT* R;
+  VT* P;
+  const VT* J;
   int k;
   MultiArgs a;
-  struct Pre { double b, J; };
+  struct Pre { VT b, J; };
   __device__ bool active() const { return true; }
-  __device__ bool col_active(int) const { return true; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c), __ldg(J + i)}; }
   __device__ void stage_pre(long i, int c, double* st) const {
     cp_async8(st + c, B + i * k + c);
     cp_async8(st + 32 + c, J + i);
   }
   __device__ Pre staged(const double* st, int c) const { return Pre{st[c], st[32 + c]}; }
-  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
+  __device__ void row(long i, int c, VT s, const Pre& g, double* acc) const {
     const long e = i * k + c;
-    const double ri = __dsub_rn(g.b, dadd(0.0, s));
+    const VT ri = celg::R<VT>(__dsub_rn(D(g.b), D(vadd(VT(0), s))));
     R[e] = ri;
-    const double z = dmul(ri, g.J);
-    P[e] = z;
-    acc[0] = dadd(acc[0], dmul(ri, z));
-    acc[1] = dadd(acc[1], dmul(ri, ri));
+    const double z = dmul(D(ri), D(g.J));
+    P[e] = celg::R<VT>(z);
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
   }
   __device__ void finish_col(int c, double* tot) const {
+    if (!a.active[c]) return;
     a.alpha[c] = tot[0];
     a.norm[c] = sqrt(tot[1]);
     a.iter[c] = 0;
@@ -406,22 +416,24 @@ struct MEpiInit {
 };
 
 // K1: v = 0 + A p; pv per column; sigma = alpha / pv
+template <typename VT_>
 struct MEpiAp {
+  using VT = VT_;
   static constexpr int NRED = 1;
-  double* V;
-  const double* P;
+  VT* V;
+  const VT* P;
   int k;
   MultiArgs a;
   __device__ bool active() const { return *(volatile int*)a.n_active > 0; }
-  struct Pre { double p; };
+  struct Pre { VT p; };
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ Pre pre(long i, int c) const { return Pre{__ldg(P + i * k + c)}; }
   __device__ void stage_pre(long i, int c, double* st) const { cp_async8(st + c, P + i * k + c); }
   __device__ Pre staged(const double* st, int c) const { return Pre{st[c]}; }
-  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
-    const double vi = dadd(0.0, s);
+  __device__ void row(long i, int c, VT s, const Pre& g, double* acc) const {
+    const VT vi = vadd(VT(0), s);
     V[i * k + c] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, g.p));
+    acc[0] = dadd(acc[0], dmul(D(vi), D(g.p)));
   }
   __device__ void finish_col(int c, double* tot) const {
     if (!a.active[c]) return;
@@ -437,14 +449,15 @@ struct MEpiAp {
 };
 
 // K2: x += sigma p; r += (-sigma) v; rz, rr; per-column scalars and test
+template <typename VT>
 struct MOpUpdate {
   static constexpr int NRED = 2;
-  struct Regs { double x, r, p, v, J; };
-  double* X;
-  double* R;
-  const double* P;
-  const double* V;
-  const double* J;
+  struct Regs { VT x, r, p, v, J; };
+  VT* X;
+  VT* R;
+  const VT* P;
+  const VT* V;
+  const VT* J;
   MultiArgs a;
   double sg;
   __device__ bool prepare() { return true; }
@@ -458,12 +471,12 @@ struct MOpUpdate {
     g.J = __ldg(J + i);
   }
   __device__ void compute(long e, long, Regs& g, double* acc) const {
-    X[e] = dadd(g.x, dmul(sg, g.p));
-    const double ri = dadd(g.r, dmul(-sg, g.v));
+    X[e] = celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
+    const VT ri = celg::R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     R[e] = ri;
-    const double z = dmul(ri, g.J);
-    acc[0] = dadd(acc[0], dmul(ri, z));
-    acc[1] = dadd(acc[1], dmul(ri, ri));
+    const double z = dmul(D(ri), D(g.J));
+    acc[0] = dadd(acc[0], dmul(D(ri), z));
+    acc[1] = dadd(acc[1], dmul(D(ri), D(ri)));
   }
   __device__ void finish_col(int c, double* tot) const {
     if (!a.active[c]) return;
@@ -477,12 +490,13 @@ struct MOpUpdate {
 };
 
 // K3: p = beta p + J r
+template <typename VT>
 struct MOpDirection {
   static constexpr int NRED = 0;
-  struct Regs { double p, r, J; };
-  double* P;
-  const double* R;
-  const double* J;
+  struct Regs { VT p, r, J; };
+  VT* P;
+  const VT* R;
+  const VT* J;
   MultiArgs a;
   double bt;
   __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
@@ -490,7 +504,7 @@ struct MOpDirection {
   __device__ void begin_col(int c) { bt = a.beta[c]; }
   __device__ void load(long e, long i, Regs& g) const { g.p = P[e]; g.r = __ldg(R + e); g.J = __ldg(J + i); }
   __device__ void compute(long e, long, Regs& g, double*) const {
-    P[e] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
+    P[e] = celg::R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
   __device__ void finish_col(int, double*) const {}
   __device__ void finish_global() const {}
@@ -498,6 +512,7 @@ struct MOpDirection {
 
 // ||b - A x|| / ||b|| per column
 struct MEpiVerify {
+  using VT = double;
   static constexpr int NRED = 1;
   const double* B;
   int k;
@@ -518,6 +533,111 @@ struct MEpiVerify {
   __device__ void finish_global() const {}
 };
 
+// ---- FP32 refinement of every column (celg_pcg_multirhs, CELG_PREC_FP32_IR) -----
+// The outer loop of ir_solve (ir.cu) for all columns at once; each column
+// keeps its own residual norm, outer count and status.
+
+struct MultiIr {
+  int* part;         // column needs an inner solve in this outer step
+  int* done;
+  int* status;
+  int* outer;
+  int* inner_total;
+  int* part_count;
+  int outer_max;
+};
+
+// r = b - (0 + A x) in FP64, ||r|| per column and the column's outer decision
+struct MEpiIrResidual {
+  using VT = double;
+  static constexpr int NRED = 1;
+  const double* B;
+  double* Rr;
+  int k;
+  MultiArgs a;  // outer state: norm[c] = ||r||, eps[c] = tolerance
+  MultiIr ir;
+  struct Pre { double b; };
+  __device__ bool active() const { return true; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&ir.done[c] == 0; }
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c)}; }
+  __device__ void stage_pre(long i, int c, double* st) const { cp_async8(st + c, B + i * k + c); }
+  __device__ Pre staged(const double* st, int c) const { return Pre{st[c]}; }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
+    const double ri = __dsub_rn(g.b, dadd(0.0, s));
+    Rr[i * k + c] = ri;
+    acc[0] = dadd(acc[0], dmul(ri, ri));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    if (ir.done[c]) return;
+    const double rn = sqrt(tot[0]);
+    a.norm[c] = rn;
+    int st = -1;
+    if (rn <= a.eps[c]) st = CELG_OK;
+    else if (!isfinite(rn)) st = kErrBreakdown;
+    else if (ir.outer[c] >= ir.outer_max) st = CELG_ERR_NOCONV;
+    if (st >= 0) {
+      ir.done[c] = 1;
+      ir.status[c] = st;
+    } else {
+      ir.part[c] = 1;
+      atomicAdd(ir.part_count, 1);
+    }
+  }
+  __device__ void finish_global() const {}
+};
+
+// r32 = (float)(r * (1/||r||)) for the columns that refine
+struct MOpIrToF32 {
+  static constexpr int NRED = 0;
+  struct Regs { double r; };
+  const double* Rr;
+  float* R32;
+  MultiArgs a;
+  MultiIr ir;
+  double inv;
+  __device__ bool prepare() { return true; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&ir.part[c] != 0; }
+  __device__ void begin_col(int c) { inv = 1.0 / a.norm[c]; }
+  __device__ void load(long e, long, Regs& g) const { g.r = __ldg(Rr + e); }
+  __device__ void compute(long e, long, Regs& g, double*) const { R32[e] = (float)dmul(g.r, inv); }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// x = x + ||r|| * (double) d32 for the columns that refined
+struct MOpIrAdd {
+  static constexpr int NRED = 0;
+  struct Regs { double x; float d; };
+  double* X;
+  const float* D32;
+  MultiArgs a;
+  MultiIr ir;
+  double scale;
+  __device__ bool prepare() { return true; }
+  __device__ bool col_active(int c) const { return *(volatile int*)&ir.part[c] != 0; }
+  __device__ void begin_col(int c) { scale = a.norm[c]; }
+  __device__ void load(long e, long, Regs& g) const { g.x = X[e]; g.d = __ldg(D32 + e); }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    X[e] = dadd(g.x, dmul(scale, (double)g.d));
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// after an inner solve (before the update): as ir_count_kernel of batched.cu
+__global__ void mir_count_kernel(int k, MultiIr ir, const int* inner_iter, const int* inner_err) {
+  const int c = threadIdx.x;
+  if (c >= k || !ir.part[c]) return;
+  ir.inner_total[c] += inner_iter[c];
+  if (inner_err[c] != 0) {
+    ir.done[c] = 1;
+    ir.status[c] = inner_err[c];
+    ir.part[c] = 0;
+  } else {
+    ir.outer[c] += 1;
+  }
+}
+
 // SpMM launch variants: the register pipeline with the resident CTAs per SM
 // its registers are budgeted for and its gather chunk width (2/8, 3/8, 3/4,
 // 4/4), and the cp.async ring with row slots per warp / CTAs per SM of 2/4,
@@ -527,7 +647,8 @@ struct MEpiVerify {
 constexpr int kSpmmNumCfgs = 8;  // 0-3 register pipeline, 4-7 cp.async ring
 
 template <class Epi, int MINB, int U>
-static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
+                           const typename Epi::VT* X, const Epi& epi) {
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
@@ -535,7 +656,7 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, int k, const double*
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, 0));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
-  kern<<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  kern<<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, vals, A.n, k, X, epi, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
 }
@@ -560,10 +681,10 @@ template <class Epi>
 static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi,
                        int cfg) {
   switch (cfg) {
-    case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, k, X, epi);
-    case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, k, X, epi);
-    case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, k, X, epi);
-    case 3: return launch_spmm_cfg<Epi, 4, 4>(h, A, k, X, epi);
+    case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, A.v, k, X, epi);
+    case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, A.v, k, X, epi);
+    case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, A.v, k, X, epi);
+    case 3: return launch_spmm_cfg<Epi, 4, 4>(h, A, A.v, k, X, epi);
     case 4: return launch_spmm_async<Epi, 2, 4>(h, A, k, X, epi);
     case 5: return launch_spmm_async<Epi, 2, 3>(h, A, k, X, epi);
     case 6: return launch_spmm_async<Epi, 3, 3>(h, A, k, X, epi);
@@ -591,6 +712,12 @@ struct Multi {
   double* work = nullptr;  // R, P, V
   double* dstate = nullptr;
   int* istate = nullptr;
+  // FP32 refinement (allocated on first use)
+  size_t f32cap = 0;
+  float* f32 = nullptr;      // 5 x n*k floats: B32 D32 R32 P32 V32
+  int* irs = nullptr;        // part, done, status, outer, inner_total (kMaxRhs each), part_count
+  double* dstate2 = nullptr; // inner-solve scalars
+  int* istate2 = nullptr;
 };
 
 namespace celg {
@@ -605,6 +732,10 @@ void multi_free(Multi* m) {
   cudaFree(m->work);
   cudaFree(m->dstate);
   cudaFree(m->istate);
+  cudaFree(m->f32);
+  cudaFree(m->irs);
+  cudaFree(m->dstate2);
+  cudaFree(m->istate2);
   delete m;
 }
 
@@ -620,11 +751,11 @@ static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, do
     *best = std::min(std::max(std::atoi(e), 0), kSpmmNumCfgs - 1);
     return CELG_OK;
   }
-  int st = launch_mtile(h, A.n, k, MOpPre{B, X, CELG_X0_USER, 0.0, 0.0, a});
+  int st = launch_mtile(h, A.n, k, MOpPre<double>{B, X, CELG_X0_USER, 0.0, 0.0, a});
   if (st) return st;
   // alpha = 0 keeps sigma = 0 / p.v finite, so no column drops out
   CELG_CUDA(cudaMemsetAsync(a.alpha, 0, sizeof(double) * kMaxRhs, h->stream));
-  const MEpiAp ep{work, B, k, a};
+  const MEpiAp<double> ep{work, B, k, a};
   float best_ms = 0.f;
   *best = 0;
   for (int c = 0; c < kSpmmNumCfgs; ++c) {
@@ -645,8 +776,34 @@ static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, do
   return CELG_OK;
 }
 
+static MultiArgs multi_args(double* ds, int* is, int k, int iter_max, cudaGraphConditionalHandle cond,
+                            const int* errw) {
+  MultiArgs a;
+  a.alpha = ds;
+  a.sigma = a.alpha + kMaxRhs;
+  a.beta = a.sigma + kMaxRhs;
+  a.norm = a.beta + kMaxRhs;
+  a.bnorm = a.norm + kMaxRhs;
+  a.eps = a.bnorm + kMaxRhs;
+  a.vres = a.eps + kMaxRhs;
+  a.iter = is;
+  a.active = a.iter + kMaxRhs;
+  a.err = a.active + kMaxRhs;
+  a.n_active = a.err + kMaxRhs;
+  a.k = k;
+  a.iter_max = iter_max;
+  a.errw = errw;
+  a.cond = cond;
+  return a;
+}
+
+static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
+                       const celg_params* p, celg_result* res);
+
 int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
                  const celg_params* p, celg_result* res) {
+  if (p->precision == CELG_PREC_FP32_IR) return multirhs_ir(h, m, k, B, X, p, res);
+  if (p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
   const long n = m->csr.n;
   const size_t nk = (size_t)n * (size_t)k;
   if (!h->multi) h->multi = new Multi();
@@ -694,14 +851,14 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   }
   const int cfg = mu->cfg;
   auto setup = [&](const MultiArgs& ac) -> int {
-    int s2 = launch_mtile(h, n, k, MOpPre{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
-    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit{B, R, P, m->jacobi, k, ac}, cfg);
+    int s2 = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
+    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit<double>{B, R, P, m->jacobi, k, ac}, cfg);
     return s2;
   };
   auto body = [&](const MultiArgs& ac) -> int {
-    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp{V, P, k, ac}, cfg);
-    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate{X, R, P, V, m->jacobi, ac, 0.0});
-    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection{P, R, m->jacobi, ac, 0.0});
+    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp<double>{V, P, k, ac}, cfg);
+    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate<double>{X, R, P, V, m->jacobi, ac, 0.0});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection<double>{P, R, m->jacobi, ac, 0.0});
     return s3;
   };
   auto tail = [&](const MultiArgs& ac) -> int {
@@ -777,6 +934,181 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   }
   h->last_iters = iters;
   h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 104.0 * (double)nk;
+  return ret;
+}
+
+// FP32 refinement of every column: the outer loop of ir_solve for all
+// columns at once around one FP32 multi-column inner PCG per outer step (the
+// same sweeps instantiated for float storage; register-pipeline SpMM).
+template <class Body>
+static int multi_run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int* n_active,
+                           int iter_max, Body&& body) {
+  if (cond) return capture_while(h, cond, body);
+  for (int it = 0; it < iter_max; it += 8) {
+    int st = CELG_OK;
+    for (int q = 0; q < 8 && !st; ++q) st = body();
+    if (st) return st;
+    int live = 0;
+    CELG_CUDA(cudaMemcpyAsync(&live, n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    if (!live) break;
+  }
+  return CELG_OK;
+}
+
+static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size_t nk,
+                              const MultiIr& ir, MultiArgs ai, double inner_eps) {
+  const long n = m->csr.n;
+  float* B32 = F;
+  float* D32 = B32 + nk;
+  float* R32 = D32 + nk;
+  float* P32 = R32 + nk;
+  float* V32 = P32 + nk;
+  const float* J32 = m->jacobi32;
+  const MOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps, ai, ir.part, ir.part_count};
+  int st = launch_mtile(h, n, k, pre);
+  if (!st)
+    st = launch_spmm_cfg<MEpiInit<float>, 4, 4>(h, m->csr, m->csr.v32, k, D32,
+                                                MEpiInit<float>{B32, R32, P32, J32, k, ai});
+  if (!st)
+    st = multi_run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
+      int s2 = launch_spmm_cfg<MEpiAp<float>, 4, 4>(h, m->csr, m->csr.v32, k, P32,
+                                                    MEpiAp<float>{V32, P32, k, ai});
+      if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{D32, R32, P32, V32, J32, ai, 0.0});
+      if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, ai, 0.0});
+      return s2;
+    });
+  return st;
+}
+
+static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
+                       const celg_params* p, celg_result* res) {
+  const long n = m->csr.n;
+  const size_t nk = (size_t)n * (size_t)k;
+  if (!m->csr.v32 || !m->jacobi32) {
+    int st = celg_mat_make_fp32(m);
+    if (st) return st;
+  }
+  if (!h->multi) h->multi = new Multi();
+  Multi* mu = h->multi;
+  if (nk > mu->cap || !mu->work) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->work);
+    mu->work = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
+    mu->cap = nk;
+  }
+  if (!mu->dstate) {
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 1)));
+  }
+  if (nk > mu->f32cap || !mu->f32) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->f32);
+    mu->f32 = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->f32, sizeof(float) * std::max<size_t>(nk, 1) * 5));
+    mu->f32cap = nk;
+  }
+  if (!mu->irs) {
+    CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
+    CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 7 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 1)));
+  }
+  int st = ensure_partials(h, ntiles_of(n), 2 * k);
+  if (st) return st;
+  double* Rr = mu->work;
+  const int inner_max = p->inner_iter_max > 0 ? p->inner_iter_max : 1000;
+  const double inner_eps = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-4;
+  MultiIr ir;
+  ir.part = mu->irs;
+  ir.done = ir.part + kMaxRhs;
+  ir.status = ir.done + kMaxRhs;
+  ir.outer = ir.status + kMaxRhs;
+  ir.inner_total = ir.outer + kMaxRhs;
+  ir.part_count = ir.inner_total + kMaxRhs;
+  ir.outer_max = p->outer_max > 0 ? p->outer_max : 20;
+  const MultiArgs a = multi_args(mu->dstate, mu->istate, k, p->iter_max, 0, h->err_d);
+  const MultiArgs ai_host = multi_args(mu->dstate2, mu->istate2, k, inner_max, 0, h->err_d);
+  if (mu->tuned_mat != (const void*)m || mu->tuned_n != (int)n || mu->tuned_k != k) {
+    st = spmm_tune(h, m->csr, k, B, X, mu->work + 2 * nk, a, &mu->cfg);
+    if (st) return st;
+    mu->tuned_mat = m;
+    mu->tuned_n = (int)n;
+    mu->tuned_k = k;
+  }
+  const int cfg = mu->cfg;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+  st = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, a});
+  CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * (5 * kMaxRhs + 1), h->stream));
+  char kb[160];
+  std::snprintf(kb, sizeof(kb), "mrhs-ir|%p|%d|%d|%p|%d|%.17g", (const void*)m, m->csr.n, k,
+                (const void*)mu->f32, inner_max, inner_eps);
+  const std::string gkey(kb);
+  for (int it = 0; !st && it <= ir.outer_max; ++it) {
+    CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * kMaxRhs, h->stream));
+    CELG_CUDA(cudaMemsetAsync(ir.part_count, 0, sizeof(int), h->stream));
+    st = launch_spmm(h, m->csr, k, X, MEpiIrResidual{B, Rr, k, a, ir}, cfg);
+    if (st) break;
+    int parts = 0;
+    CELG_CUDA(cudaMemcpyAsync(&parts, ir.part_count, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    if (parts == 0) break;
+    st = launch_mtile(h, n, k, MOpIrToF32{Rr, mu->f32, a, ir, 0.0});
+    if (st) break;
+    if (graphs_enabled()) {
+      GraphEntry* ge = graph_cache_find(h, gkey);
+      if (!ge) {
+        st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
+          return record_multi_inner(h, m, k, mu->f32, nk, ir,
+                                    multi_args(mu->dstate2, mu->istate2, k, inner_max, cond, h->err_d),
+                                    inner_eps);
+        }, &ge);
+        if (st) break;
+      }
+      CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    } else {
+      st = record_multi_inner(h, m, k, mu->f32, nk, ir, ai_host, inner_eps);
+      if (st) break;
+    }
+    mir_count_kernel<<<1, kMaxRhs, 0, h->stream>>>(k, ir, ai_host.iter, ai_host.err);
+    CELG_CUDA(cudaGetLastError());
+    st = launch_mtile(h, n, k, MOpIrAdd{X, mu->f32 + nk, a, ir, 0.0});
+  }
+  if (st) return st;
+  CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  std::vector<double> ds(7 * kMaxRhs);
+  std::vector<int> is(5 * kMaxRhs + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), mu->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), ir.part, sizeof(int) * is.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, inner_most = 0;
+  for (int c = 0; c < k; ++c) {
+    const int done = is[kMaxRhs + c], status = is[2 * kMaxRhs + c];
+    const int outer = is[3 * kMaxRhs + c], inner = is[4 * kMaxRhs + c];
+    const double rn = ds[3 * kMaxRhs + c], bn = ds[4 * kMaxRhs + c];
+    const int rs = done ? status : CELG_ERR_NOCONV;
+    if (rs && !ret) ret = rs;
+    inner_most = std::max(inner_most, inner);
+    if (res) {
+      res[c].iter_done = outer;
+      res[c].final_norm2 = rn;
+      res[c].bnorm = bn;
+      res[c].verified_relres = bn > 0 ? rn / bn : rn;
+      res[c].err = rs;
+      res[c].arnoldi_steps = inner;
+      res[c].history_len = 0;
+    }
+  }
+  h->last_iters = inner_most;
   return ret;
 }
 

@@ -121,3 +121,101 @@ def test_every_spmm_variant_is_bitexact(gpu, cfg, monkeypatch):
     m.destroy()
     assert np.array_equal(Xd.cpu().numpy(), Xo)
     assert [i.iter_done for i in infos] == list(ito)
+
+
+def mirror_ir(rp, ci, v, B, eps_rel, inner_eps, inner_max, outer_max):
+    """FP64 refinement of every column around an FP32 multi-column PCG,
+    composed from oracle pieces in the multi-column reduction order."""
+    f32, f64 = np.float32, np.float64
+    n, k = B.shape
+    J = R.jacobi(R.diag(rp, ci, v))
+    J32 = J.astype(f32)
+    v32 = v.astype(f32)
+    spmm64 = lambda X: np.stack([R.spmv_csr(rp, ci, v, X[:, c]) for c in range(k)], 1)
+    spmm32 = lambda X: np.stack([R.spmv_csr_f32(rp, ci, v32, X[:, c]) for c in range(k)], 1)
+    D = lambda a: a.astype(f64)
+
+    def inner(B32, part):
+        X = np.zeros((n, k), f32)
+        bn = np.sqrt(dot_cols(D(B32), D(B32)))
+        eps = inner_eps * bn
+        Rr = (D(B32) - D(f32(0) + spmm32(X))).astype(f32)
+        Z = D(Rr) * D(J32)[:, None]
+        P = Z.astype(f32)
+        alpha, norm = dot_cols(D(Rr), Z), np.sqrt(dot_cols(D(Rr), D(Rr)))
+        it = np.zeros(k, int)
+        go = lambda c: it[c] < inner_max and abs(alpha[c]) > R.REAL_SMALL and norm[c] > eps[c]
+        active = np.array([bool(part[c]) and go(c) for c in range(k)])
+        while active.any():
+            V = (f32(0) + spmm32(P)).astype(f32)
+            pv = dot_cols(D(V), D(P))
+            for c in np.flatnonzero(active):
+                sg = alpha[c] / pv[c]
+                X[:, c] = (D(X[:, c]) + sg * D(P[:, c])).astype(f32)
+                Rr[:, c] = (D(Rr[:, c]) + (-sg) * D(V[:, c])).astype(f32)
+            Z = D(Rr) * D(J32)[:, None]
+            rz, rr = dot_cols(D(Rr), Z), dot_cols(D(Rr), D(Rr))
+            beta = np.zeros(k)
+            for c in np.flatnonzero(active):
+                beta[c] = rz[c] / alpha[c]
+                alpha[c], norm[c] = rz[c], np.sqrt(rr[c])
+                it[c] += 1
+                active[c] = go(c)
+            for c in np.flatnonzero(active):
+                P[:, c] = (beta[c] * D(P[:, c]) + D(Rr[:, c]) * D(J32)).astype(f32)
+        return X, it
+
+    X = np.zeros((n, k))
+    tol = eps_rel * np.sqrt(dot_cols(B, B))
+    done = np.zeros(k, bool)
+    outer = np.zeros(k, int)
+    inner_total = np.zeros(k, int)
+    rn = np.zeros(k)
+    for _ in range(outer_max + 1):
+        Rr = B - (0.0 + spmm64(X))
+        rn_all = np.sqrt(dot_cols(Rr, Rr))
+        part = np.zeros(k, bool)
+        for c in range(k):
+            if done[c]:
+                continue
+            rn[c] = rn_all[c]
+            if rn[c] <= tol[c] or outer[c] >= outer_max:
+                done[c] = True
+            else:
+                part[c] = True
+        if not part.any():
+            break
+        B32 = np.zeros((n, k), f32)
+        for c in np.flatnonzero(part):
+            B32[:, c] = (Rr[:, c] * (1.0 / rn[c])).astype(f32)
+        Dd, its = inner(B32, part)
+        for c in np.flatnonzero(part):
+            inner_total[c] += its[c]
+            outer[c] += 1
+            X[:, c] = X[:, c] + rn[c] * D(Dd[:, c])
+    return X, outer, inner_total, rn
+
+
+@pytest.mark.parametrize("mode", ["graph", "host_loop"])
+def test_multirhs_fp32_refinement_bitexact(gpu, mode, monkeypatch):
+    celgpu, h, torch = gpu
+    if mode == "host_loop":
+        monkeypatch.setenv("CELG_GRAPH", "0")
+    rng = np.random.default_rng(15)
+    _, (kx, ky, kz) = synth.lognormal_faces(rng, 9, 8, 10, 0.5)
+    rp, ci, v = synth.diffusion7(9, 8, 10, kx, ky, kz)
+    n, k = rp.size - 1, 6
+    B = rng.uniform(-1.0, 1.0, (n, k))
+    B[:, 3] *= 1e-3                         # columns of different scale
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    kw = dict(eps_rel=1e-10, iter_max=3000, precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4,
+              inner_iter_max=800, outer_max=20)
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), **kw)
+    Xo, outer, inner_total, rn = mirror_ir(rp, ci, v, B, 1e-10, 1e-4, 800, 20)
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == list(outer)
+    assert [i.arnoldi_steps for i in infos] == list(inner_total)
+    assert [i.final_norm2 for i in infos] == list(rn)
+    assert all(i.status == celgpu.OK and i.verified_relres <= 1e-10 for i in infos)
+    m.destroy()
