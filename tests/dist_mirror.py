@@ -21,7 +21,8 @@ def tdot(a, b):
 
 
 class CpuRank:
-    def __init__(self, block, b, x0=None, eps_rel=1e-8, eps_abs=0.0, iter_max=1000, x0_mode=None):
+    def __init__(self, block, b, x0=None, eps_rel=1e-8, eps_abs=0.0, iter_max=1000, x0_mode=None,
+                 fail_at=None):
         self.block = block
         n = block.n
         self.b = np.ascontiguousarray(b, dtype=np.float64)
@@ -36,6 +37,9 @@ class CpuRank:
         self.v = np.zeros(n)
         self.err = 0
         self.active = 0
+        # a local failure (as a bounded-wait timeout on this rank's device)
+        # raised during the SpMV of iteration `fail_at`
+        self.fail_at = fail_at
 
     # numpy views sharing the torch tensors' memory
     def _xe(self):
@@ -90,6 +94,8 @@ class CpuRank:
         if not self.active:
             return
         n = self.block.n
+        if self.fail_at is not None and self.iter + 1 == self.fail_at:
+            self.err = 5
         self.v = 0.0 + self._spmv(self._pe())
         self._store(0.0, 0.0, 0.0, tdot(self.v, self._pe()[:n]))
 
@@ -99,14 +105,16 @@ class CpuRank:
         n = self.block.n
         sg = self.alpha / float(self.xch[3])
         rz = rr = 0.0
-        if np.isfinite(sg):
+        flagged = float(self.xch[4]) != 0.0
+        if np.isfinite(sg) and not flagged:
             xe, pe = self._xe(), self._pe()
             xe[:n] = xe[:n] + sg * pe[:n]
             self.r = self.r + (-sg) * self.v
             z = self.r * self.J
             rz, rr = tdot(self.r, z), tdot(self.r, self.r)
         else:
-            self.err = 3
+            if self.err == 0:
+                self.err = 5 if flagged else 3
             self.active = 0
         self._store(0.0, rz, rr)
 

@@ -154,3 +154,33 @@ def test_gloo_ranks_match_in_process_emulation(world, tmp_path):
         assert np.array_equal(parts[0]["hist"], res[0]["history"])
     else:
         assert np.abs(np.concatenate([p["x"] for p in parts]) - x_emul).max() <= 1e-12
+
+
+def _gloo_fail_worker(rank, world, port, out_dir):
+    import torch.distributed as td
+    from datetime import timedelta
+    td.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                          world_size=world, timeout=timedelta(seconds=60))
+    try:
+        rp, ci, v, b = poisson()
+        bounds = D.partition(rp.size - 1, world, GRID[0] * GRID[1])
+        blk = D.RowBlock(rp, ci, v, bounds, rank)
+        rk = M.CpuRank(blk, b[blk.r0:blk.r1], eps_rel=1e-10, iter_max=500,
+                       fail_at=6 if rank == world - 1 else None)
+        (res,) = D.run_pcg([rk], D.TorchComm(), check_every=4)
+        np.savez(os.path.join(out_dir, f"rank{rank}.npz"), iters=res["iter_done"], err=res["err"])
+    finally:
+        td.destroy_process_group()
+
+
+def test_gloo_one_rank_fails_all_stop_together(tmp_path):
+    """A failure on one rank travels with the reduced sums: every rank stops
+    at the same iteration with the timeout status, and no rank is left
+    waiting in a collective."""
+    import torch.multiprocessing as mp
+    world = 3
+    mp.start_processes(_gloo_fail_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
+                       start_method="spawn", join=True)
+    parts = [np.load(tmp_path / f"rank{q}.npz") for q in range(world)]
+    assert {int(p["iters"]) for p in parts} == {5}
+    assert all(int(p["err"]) == 5 for p in parts)
