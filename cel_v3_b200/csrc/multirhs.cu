@@ -302,6 +302,155 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_async_kernel(const int* __r
   else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
 }
 
+// Two rows per warp step (k even): half-warp h takes row 2j+h and lane l of a
+// half owns columns 2l and 2l+1, so each gather is one 16-byte asynchronous
+// copy and every instruction serves two rows.  A ring of S slots per warp
+// holds a row pair's gathered entries, the two rows' matrix values and their
+// epilogue operands.  Per column the rows still enter the reductions in
+// order: each row's epilogue works on a zeroed term that is then added to the
+// column's sum, the first row's before the second's.
+__device__ __forceinline__ void cp_async16(double* dst, const double* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+constexpr int kPairU = 8;
+// doubles per slot: X[U][32 lanes][2], epilogue operands [2 halves][2][32],
+// matrix values [2 halves][U]
+constexpr int kPairSlot = kPairU * 64 + 128 + 2 * kPairU;
+
+template <class Epi, int S, int MINB>
+__global__ void __launch_bounds__(kLanes, MINB) spmm_pair_kernel(const int* __restrict__ rp,
+                                                                const int* __restrict__ ci,
+                                                                const double* __restrict__ v, int n,
+                                                                int k, const double* __restrict__ X,
+                                                                Epi epi, RedCtx red) {
+  constexpr int NR = Epi::NRED;
+  constexpr int NR1 = NR > 0 ? NR : 1;
+  constexpr int U = kPairU;
+  constexpr int SLOT = kPairSlot;
+  constexpr int PRE = U * 64;        // epilogue operands of half h at PRE + 64 h
+  constexpr int VOFF = U * 64 + 128; // matrix values of half h at VOFF + U h
+  constexpr unsigned kFull = 0xffffffffu;
+  __shared__ double s_w[NR1 * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[NR1 * kMaxRhs];
+  __shared__ int s_flag;
+  extern __shared__ __align__(16) double s_ring[];
+  if (!epi.active()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int hh = lane >> 4, hl = lane & 15;
+  const int c0 = 2 * hl, c1 = c0 + 1;
+  const bool in = c0 < k;
+  const bool on0 = in && epi.col_active(c0), on1 = in && epi.col_active(c1);
+  const bool on = on0 || on1;
+  double* ring = s_ring + (long)warp * S * SLOT;
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    double acc0[NR1], acc1[NR1];  // columns c0, c1 (kept in the first half)
+#pragma unroll
+    for (int r = 0; r < NR1; ++r) acc0[r] = acc1[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      if (row0 >= n) break;
+      const int nrows = (int)min(32L, (long)n - row0);
+      const int npairs = (nrows + 1) / 2;
+      const int re = lane < nrows ? __ldg(rp + row0 + lane + 1) : 0;  // end of row lane
+      const int b0 = __ldg(rp + row0);
+      // next pair to issue and this half's row of it: entry range, first U columns
+      int pI = 0;
+      int rI = hh;
+      bool vI = rI < nrows;
+      const int prev0 = __shfl_sync(kFull, re, max(rI - 1, 0));
+      int bI = rI == 0 ? b0 : prev0;
+      int eI = __shfl_sync(kFull, re, min(rI, 31));
+      if (!vI) bI = eI = 0;
+      int cn[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) cn[u] = bI + u < eI ? __ldg(ci + bI + u) : 0;
+      auto issue_next = [&]() {
+        if (pI < npairs) {
+          double* slot = ring + (pI % S) * SLOT;
+          if (vI) {
+            if (on) {
+#pragma unroll
+              for (int u = 0; u < U; ++u)
+                if (bI + u < eI) cp_async16(slot + u * 64 + lane * 2, X + (long)cn[u] * k + c0);
+              if (on0) epi.stage_pre(row0 + rI, c0, slot + PRE + 64 * hh);
+              if (on1) epi.stage_pre(row0 + rI, c1, slot + PRE + 64 * hh);
+            }
+            if (hl < U && bI + hl < eI) cp_async8(slot + VOFF + U * hh + hl, v + bI + hl);
+          }
+        }
+        cp_async_commit();
+        ++pI;
+        if (pI < npairs) {
+          rI = 2 * pI + hh;
+          vI = rI < nrows;
+          bI = __shfl_sync(kFull, re, max(rI - 1, 0));
+          eI = __shfl_sync(kFull, re, min(rI, 31));
+          if (!vI) bI = eI = 0;
+#pragma unroll
+          for (int u = 0; u < U; ++u) cn[u] = bI + u < eI ? __ldg(ci + bI + u) : 0;
+        }
+      };
+      for (int r = 0; r < S - 1; ++r) issue_next();
+      for (int pp = 0; pp < npairs; ++pp) {
+        issue_next();  // pair pp + S - 1
+        cp_async_wait<S - 1>();
+        __syncwarp();
+        const int row = 2 * pp + hh;
+        const bool valid = row < nrows;
+        const int prev = __shfl_sync(kFull, re, max(row - 1, 0));
+        const int b = row == 0 ? b0 : prev;
+        const int e = __shfl_sync(kFull, re, min(row, 31));
+        const double* slot = ring + (pp % S) * SLOT;
+        double t0[NR1], t1[NR1];
+#pragma unroll
+        for (int r = 0; r < NR1; ++r) t0[r] = t1[r] = 0.0;
+        if (valid) {
+          double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (b + u < e) {
+              const double vv = slot[VOFF + U * hh + u];
+              s0 = dadd(s0, dmul(vv, slot[u * 64 + lane * 2]));
+              s1 = dadd(s1, dmul(vv, slot[u * 64 + lane * 2 + 1]));
+            }
+          for (int kk = b + U; kk < e; ++kk) {  // rows longer than U entries
+            const double vv = __ldg(v + kk);
+            const long xo = (long)__ldg(ci + kk) * k + c0;
+            s0 = dadd(s0, dmul(vv, on ? __ldg(X + xo) : 0.0));
+            s1 = dadd(s1, dmul(vv, on ? __ldg(X + xo + 1) : 0.0));
+          }
+          const double* pre = slot + PRE + 64 * hh;
+          if (on0) epi.row(row0 + row, c0, s0, epi.staged(pre, c0), t0);
+          if (on1) epi.row(row0 + row, c1, s1, epi.staged(pre, c1), t1);
+        }
+        // the two rows' terms enter each column's sum in row order
+#pragma unroll
+        for (int r = 0; r < NR1; ++r) {
+          const double u0 = __shfl_down_sync(kFull, t0[r], 16);
+          const double u1 = __shfl_down_sync(kFull, t1[r], 16);
+          acc0[r] = dadd(dadd(acc0[r], t0[r]), u0);
+          acc1[r] = dadd(dadd(acc1[r], t1[r]), u1);
+        }
+        __syncwarp();  // every lane has read the slot before it is refilled
+      }
+      cp_async_wait<0>();
+    }
+    // lane c takes column c's sum from lane c/2 of the first half
+    double acc[NR1];
+#pragma unroll
+    for (int r = 0; r < NR1; ++r) {
+      const double ev = __shfl_sync(kFull, acc0[r], lane >> 1);
+      const double od = __shfl_sync(kFull, acc1[r], lane >> 1);
+      acc[r] = (lane & 1) ? od : ev;
+    }
+    if (NR > 0) multi_tile_store<NR1>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<NR1>(red, epi, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
+}
+
 // ---- n x k vector sweeps with per-column scalars ------------------------------
 template <class Op>
 __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, RedCtx red) {
@@ -641,10 +790,11 @@ __global__ void mir_count_kernel(int k, MultiIr ir, const int* inner_iter, const
 // SpMM launch variants: the register pipeline with the resident CTAs per SM
 // its registers are budgeted for and its gather chunk width (2/8, 3/8, 3/4,
 // 4/4), and the cp.async ring with row slots per warp / CTAs per SM of 2/4,
-// 2/3, 3/3 and 4/2.  The
+// 2/3, 3/3 and 4/2, and the two-rows-per-step ring (k even) with 2 slots at
+// 2 CTAs per SM or 3 slots at 1.  The
 // fastest for a matrix and k is picked by timing them (spmm_tune) before the
 // first solve.
-constexpr int kSpmmNumCfgs = 8;  // 0-3 register pipeline, 4-7 cp.async ring
+constexpr int kSpmmNumCfgs = 10;  // 0-3 register pipeline, 4-7 cp.async ring, 8-9 row pairs
 
 template <class Epi, int MINB, int U>
 static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
@@ -677,10 +827,30 @@ static int launch_spmm_async(celg_handle* h, const CsrDev& A, int k, const doubl
   return CELG_OK;
 }
 
+template <class Epi, int S, int MINB>
+static int launch_spmm_pair(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{h->partials, h->ticket, nt};
+  if (A.n == 0) return CELG_OK;
+  auto kern = spmm_pair_kernel<Epi, S, MINB>;
+  const int smem = 8 * S * kPairSlot * (int)sizeof(double);
+  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
+  const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
+  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 template <class Epi>
 static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi,
                        int cfg) {
+  // the two-rows-per-step kernel needs k even and 16-byte aligned rows of X
+  if (cfg >= 8 && ((k & 1) || (reinterpret_cast<uintptr_t>(X) & 15))) cfg = 5;
   switch (cfg) {
+    case 8: return launch_spmm_pair<Epi, 2, 2>(h, A, k, X, epi);
+    case 9: return launch_spmm_pair<Epi, 3, 1>(h, A, k, X, epi);
     case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, A.v, k, X, epi);
     case 1: return launch_spmm_cfg<Epi, 3, 8>(h, A, A.v, k, X, epi);
     case 2: return launch_spmm_cfg<Epi, 3, 4>(h, A, A.v, k, X, epi);
@@ -744,7 +914,7 @@ void multi_free(Multi* m) {
 // p.v), applied to B with the output in a work vector; the per-column state
 // is set up first by MOpPre in the user-start mode, which leaves X alone, and
 // the solve's own set-up overwrites everything the timing wrote.  Returns the
-// fastest variant; CELG_SPMM_CFG=0..7 forces one (profiling).
+// fastest variant; CELG_SPMM_CFG=0..9 forces one (profiling).
 static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, double* X,
                      double* work, const MultiArgs& a, int* best) {
   if (const char* e = std::getenv("CELG_SPMM_CFG")) {
