@@ -682,7 +682,12 @@ def run_gpu(args):
                 "api": "celg_elm_doit + celg_elm_collect_solution (pinned host b/x)",
                 "wall_s": wall_e2e},
         "forms": forms,
-        "gpu_launches": world * args.steps * (3 * iters + 3),
+        # one solve: 2 set-up sweeps, 3 per iteration and 1 verification; the
+        # graph's loop body holds two iterations (an odd count ends with one
+        # body of 3 kernels that return at once); the distributed phases run
+        # 8 iterations between polls, plus a start kernel
+        "gpu_launches": args.steps * (3 + 3 * (iters + iters % 2) if world == 1 else
+                                      world * (4 + 3 * 8 * ((iters + 7) // 8))),
         "clocks": clk,
     }
     if cpu is not None:

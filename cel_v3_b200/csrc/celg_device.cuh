@@ -37,7 +37,17 @@ struct RedCtx {
   double* partials;
   unsigned* ticket;
   long ntiles;
+  // bit 0: walk the tiles from the last to the first; bit 1: stream the
+  // matrix with the L2 evict-first policy.  Neither changes a result: every
+  // tile is reduced on its own and the tile partials are combined in index
+  // order.
+  int sweep = 0;
 };
+
+// Tile index of the k-th tile a sweep visits.
+__device__ __forceinline__ long tile_at(long k, long ntiles, int sweep) {
+  return (sweep & 1) ? ntiles - 1 - k : k;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -103,6 +113,23 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
           "r"(smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
       : "memory");
+}
+
+// The same copy with an L2 cache policy (from createpolicy).
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar, uint64_t policy) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], "
+      "%2, [%3], %4;" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+      : "memory");
+}
+
+// L2 policy that evicts the lines it covers first (for data read once).
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
 }
 
 __device__ __forceinline__ void named_bar_sync(int id, int nthreads) {

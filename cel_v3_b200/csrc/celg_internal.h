@@ -99,6 +99,8 @@ struct celg_handle {
   int last_iters = 0;
   double last_bytes_per_iter = 0.0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // tile order of the next sweep (RedCtx::sweep bit 0)
+  int sweep_rev = 0;
 };
 
 struct celg_mat {

@@ -104,6 +104,7 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
   }
 }
 
+
 // ---- SpMM with a fused per-row epilogue ---------------------------------------
 // Warp w takes rows in order; lane c owns column c, so each stored entry is
 // one k-wide (k*8-byte contiguous) gather of X.  Rows are software-pipelined
@@ -451,6 +452,125 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_pair_kernel(const int* __re
   else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
 }
 
+// The same SpMM with 16-byte gathers and rows spread over lanes: a warp
+// works on RS = 4 RP rows per step, lanes 8g..8g+7 on rows g, g+4, ... of
+// the step (RP rows each, whose gathers are all in flight together), and
+// lane l of a row owns the column pairs 2l and 2l + 16, so one gather
+// instruction reads 128 contiguous bytes of X for each of four rows (k even,
+// X 16-byte aligned).  Each lane sums its rows' entries in stored order for
+// its four columns; the row sums are then transposed through shared memory
+// to lane = column, where the epilogue runs row by row in order, so the
+// per-column reductions keep the (q, r) order of the other variants.  The
+// epilogue's operands are staged into shared memory by cp.async at the start
+// of the step.  Per row and entry a warp issues half a gather instead of
+// one, and the epilogue's loads and stores stay coalesced.  RP > 1 gives a
+// warp more gathers in flight at fewer resident CTAs, which keeps the rows
+// of X in use by all CTAs together within L2.  FP64 only.
+template <class Epi, int MINB, int U, int RP>
+__global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __restrict__ rp,
+                                                               const int* __restrict__ ci,
+                                                               const double* __restrict__ v, int n,
+                                                               int k, const double* __restrict__ X,
+                                                               Epi epi, RedCtx red) {
+  constexpr int NR = Epi::NRED;
+  constexpr int NR1 = NR > 0 ? NR : 1;
+  constexpr int L = 8;        // lanes per row
+  constexpr int RS = 4 * RP;  // rows per step
+  __shared__ double s_w[NR1 * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[NR1 * kMaxRhs];
+  __shared__ int s_flag;
+  extern __shared__ __align__(16) double s_dyn[];  // per warp: sums [RS][32], operands [RS][64]
+  if (!epi.active()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane / L, l = lane % L;
+  const bool on = lane < k && epi.col_active(lane);
+  const int cm0 = 2 * l;  // column pairs cm0 and cm0 + 16 (k is even)
+  const bool gon0 = cm0 < k && (epi.col_active(cm0) || epi.col_active(cm0 + 1));
+  const bool gon1 = cm0 + 16 < k && (epi.col_active(cm0 + 16) || epi.col_active(cm0 + 17));
+  double* sw = s_dyn + (long)warp * RS * 96;
+  double* sp = sw + RS * 32;
+  const long ntiles = ((long)n + kTile - 1) / kTile;
+  for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
+    const long t = tile_at(kt, ntiles, red.sweep);
+    double acc[NR1];
+#pragma unroll
+    for (int r = 0; r < NR1; ++r) acc[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      if (row0 >= n) break;
+      const int nrows = (int)min(32L, (long)n - row0);
+      for (int s0 = 0; s0 < nrows; s0 += RS) {
+#pragma unroll
+        for (int rr = 0; rr < RS; ++rr)
+          if (on && s0 + rr < nrows) epi.stage_pre(row0 + s0 + rr, lane, sp + rr * 64);
+        cp_async_commit();
+        int b[RP], e[RP];
+        int lmax = 0;
+#pragma unroll
+        for (int j = 0; j < RP; ++j) {
+          const int r = s0 + g + 4 * j;
+          b[j] = r < nrows ? __ldg(rp + row0 + r) : 0;
+          e[j] = r < nrows ? __ldg(rp + row0 + r + 1) : 0;
+          lmax = max(lmax, e[j] - b[j]);
+        }
+        double2 sum0[RP], sum1[RP];
+#pragma unroll
+        for (int j = 0; j < RP; ++j) sum0[j] = sum1[j] = make_double2(0.0, 0.0);
+        for (int c0 = 0; c0 < lmax; c0 += U) {
+          int cc[RP][U];
+          double vv[RP][U];
+#pragma unroll
+          for (int j = 0; j < RP; ++j)
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const int kk = b[j] + c0 + u;
+              cc[j][u] = kk < e[j] ? __ldg(ci + kk) : 0;
+              vv[j][u] = kk < e[j] ? __ldg(v + kk) : 0.0;
+            }
+          double2 x0[RP][U], x1[RP][U];
+#pragma unroll
+          for (int j = 0; j < RP; ++j)
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              const bool ok = b[j] + c0 + u < e[j];
+              const double2* xr = reinterpret_cast<const double2*>(X + (long)cc[j][u] * k + cm0);
+              x0[j][u] = (ok && gon0) ? __ldg(xr) : make_double2(0.0, 0.0);
+              x1[j][u] = (ok && gon1) ? __ldg(xr + 8) : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+          for (int j = 0; j < RP; ++j)
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              if (b[j] + c0 + u < e[j]) {
+                sum0[j].x = dadd(sum0[j].x, dmul(vv[j][u], x0[j][u].x));
+                sum0[j].y = dadd(sum0[j].y, dmul(vv[j][u], x0[j][u].y));
+                sum1[j].x = dadd(sum1[j].x, dmul(vv[j][u], x1[j][u].x));
+                sum1[j].y = dadd(sum1[j].y, dmul(vv[j][u], x1[j][u].y));
+              }
+        }
+#pragma unroll
+        for (int j = 0; j < RP; ++j)
+          if (s0 + g + 4 * j < nrows) {
+            double* srow = sw + (g + 4 * j) * 32;
+            if (cm0 < k) *reinterpret_cast<double2*>(srow + cm0) = sum0[j];
+            if (cm0 + 16 < k) *reinterpret_cast<double2*>(srow + cm0 + 16) = sum1[j];
+          }
+        cp_async_wait<0>();
+        __syncwarp();
+#pragma unroll
+        for (int rr = 0; rr < RS; ++rr)
+          if (on && s0 + rr < nrows)
+            epi.row(row0 + s0 + rr, lane, sw[rr * 32 + lane], epi.staged(sp + rr * 64, lane), acc);
+        __syncwarp();  // the sums are read before the next step overwrites them
+      }
+    }
+    if (NR > 0) multi_tile_store<NR1>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<NR1>(red, epi, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
+}
+
 // ---- n x k vector sweeps with per-column scalars ------------------------------
 template <class Op>
 __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, RedCtx red) {
@@ -465,7 +585,8 @@ __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, 
   const bool on = lane < k && op.col_active(lane);
   op.begin_col(lane < k ? lane : 0);
   const long ntiles = (n + kTile - 1) / kTile;
-  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
+    const long t = tile_at(kt, ntiles, red.sweep);
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
@@ -612,15 +733,17 @@ struct MOpUpdate {
   __device__ bool prepare() { return true; }
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ void begin_col(int c) { sg = a.sigma[c]; }
+  // x and v are not read again before the next update sweep: streamed
+  // (evict-first), so that L2 keeps r and p for the direction sweep
   __device__ void load(long e, long i, Regs& g) const {
-    g.x = X[e];
+    g.x = __ldcs(X + e);
     g.r = R[e];
     g.p = __ldg(P + e);
-    g.v = __ldg(V + e);
+    g.v = __ldcs(V + e);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long e, long, Regs& g, double* acc) const {
-    X[e] = celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
+    __stcs(X + e, celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
     const VT ri = celg::R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     R[e] = ri;
     const double z = dmul(D(ri), D(g.J));
@@ -651,7 +774,12 @@ struct MOpDirection {
   __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ void begin_col(int c) { bt = a.beta[c]; }
-  __device__ void load(long e, long i, Regs& g) const { g.p = P[e]; g.r = __ldg(R + e); g.J = __ldg(J + i); }
+  // r is streamed (evict-first), so that L2 keeps the new p for the SpMM
+  __device__ void load(long e, long i, Regs& g) const {
+    g.p = P[e];
+    g.r = __ldcs(R + e);
+    g.J = __ldg(J + i);
+  }
   __device__ void compute(long e, long, Regs& g, double*) const {
     P[e] = celg::R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
@@ -794,7 +922,9 @@ __global__ void mir_count_kernel(int k, MultiIr ir, const int* inner_iter, const
 // 2 CTAs per SM or 3 slots at 1.  The
 // fastest for a matrix and k is picked by timing them (spmm_tune) before the
 // first solve.
-constexpr int kSpmmNumCfgs = 10;  // 0-3 register pipeline, 4-7 cp.async ring, 8-9 row pairs
+// 0-3 register pipeline, 4-7 cp.async ring, 8-9 row pairs, 10-14 16-byte
+// gathers
+constexpr int kSpmmNumCfgs = 15;
 
 template <class Epi, int MINB, int U>
 static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
@@ -807,6 +937,23 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, 0));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
   kern<<<grid, kLanes, 0, h->stream>>>(A.rp, A.ci, vals, A.n, k, X, epi, red);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+template <class Epi, int MINB, int U, int RP>
+static int launch_spmm_vec(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+  const long nt = ntiles_of(A.n);
+  RedCtx red{h->partials, h->ticket, nt};
+  if (A.n == 0) return CELG_OK;
+  red.sweep = next_sweep(h, false, false);
+  auto kern = spmm_vec_kernel<Epi, MINB, U, RP>;
+  const int smem = 8 * 4 * RP * 96 * (int)sizeof(double);
+  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int per_sm = 0;
+  CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
+  const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
+  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
 }
@@ -846,9 +993,15 @@ static int launch_spmm_pair(celg_handle* h, const CsrDev& A, int k, const double
 template <class Epi>
 static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi,
                        int cfg) {
-  // the two-rows-per-step kernel needs k even and 16-byte aligned rows of X
+  // the two-rows-per-step and 16-byte-gather kernels need k even and 16-byte
+  // aligned rows of X
   if (cfg >= 8 && ((k & 1) || (reinterpret_cast<uintptr_t>(X) & 15))) cfg = 5;
   switch (cfg) {
+    case 10: return launch_spmm_vec<Epi, 2, 8, 1>(h, A, k, X, epi);
+    case 11: return launch_spmm_vec<Epi, 3, 4, 1>(h, A, k, X, epi);
+    case 12: return launch_spmm_vec<Epi, 4, 4, 1>(h, A, k, X, epi);
+    case 13: return launch_spmm_vec<Epi, 2, 4, 2>(h, A, k, X, epi);
+    case 14: return launch_spmm_vec<Epi, 3, 2, 2>(h, A, k, X, epi);
     case 8: return launch_spmm_pair<Epi, 2, 2>(h, A, k, X, epi);
     case 9: return launch_spmm_pair<Epi, 3, 1>(h, A, k, X, epi);
     case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, A.v, k, X, epi);
@@ -866,6 +1019,7 @@ template <class Op>
 static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
+  red.sweep = next_sweep(h, false, false);
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile_kernel<Op>>(kLanes, 0)));
   mtile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
   CELG_CUDA(cudaGetLastError());
@@ -914,7 +1068,7 @@ void multi_free(Multi* m) {
 // p.v), applied to B with the output in a work vector; the per-column state
 // is set up first by MOpPre in the user-start mode, which leaves X alone, and
 // the solve's own set-up overwrites everything the timing wrote.  Returns the
-// fastest variant; CELG_SPMM_CFG=0..9 forces one (profiling).
+// fastest variant; CELG_SPMM_CFG=0..14 forces one (profiling).
 static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, double* X,
                      double* work, const MultiArgs& a, int* best) {
   if (const char* e = std::getenv("CELG_SPMM_CFG")) {
@@ -1056,7 +1210,14 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
       MultiArgs ac = a;
       ac.cond = cond;
       int s2 = setup(ac);
-      if (!s2) s2 = capture_while(h, cond, [&]() -> int { return body(ac); });
+      // two iterations per loop body, so that the sweep order alternates
+      // across iterations (the kernels return at once when no column is
+      // active)
+      if (!s2) s2 = capture_while(h, cond, [&]() -> int {
+        int s3 = body(ac);
+        if (!s3) s3 = body(ac);
+        return s3;
+      });
       if (!s2) s2 = tail(ac);
       return s2;
     };

@@ -1,6 +1,8 @@
 // pcg.cu -- Jacobi-PCG (cel_cgalg_jacobi, src/fcgalg/cel_cgalg_module.f90:178-305)
 // as three fused sweeps per iteration, run to convergence inside one CUDA
-// graph whose WHILE conditional node is driven from the device.
+// graph whose WHILE conditional node is driven from the device.  The loop
+// body holds two iterations; consecutive sweeps walk the tiles in opposite
+// orders (RedCtx::sweep), so six sweeps make the order repeat.
 //
 // Per iteration (reference lines in brackets):
 //   K1  v = 0 + A p, pv = v.p, sigma = alpha/pv          [:251-261]
@@ -144,7 +146,14 @@ template <typename VT>
 static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
   int st = pcg_setup(h, B, p, a);
   if (st) return st;
-  st = capture_while(h, a.cond, [&]() -> int { return pcg_body(h, B, a); });
+  // two iterations per loop body, so that the sweep order alternates across
+  // iterations too (the second iteration's kernels return at once when the
+  // first one ended the solve)
+  st = capture_while(h, a.cond, [&]() -> int {
+    int s = pcg_body(h, B, a);
+    if (!s) s = pcg_body(h, B, a);
+    return s;
+  });
   if (st) return st;
   return pcg_tail(h, B, a);
 }

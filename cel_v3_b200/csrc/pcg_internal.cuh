@@ -203,15 +203,17 @@ struct OpUpdate {
     sg = a.st->sigma;
     return true;
   }
+  // x and v are not read again before the next update sweep: streamed
+  // (evict-first), so that L2 keeps r, p and J for the direction sweep
   __device__ void load(long i, Regs& g) const {
-    g.x = x[i];
+    g.x = __ldcs(x + i);
     g.r = r[i];
     g.p = __ldg(p + i);
-    g.v = __ldg(v + i);
+    g.v = __ldcs(v + i);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    x[i] = R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
+    __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
     const VT ri = R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     r[i] = ri;
     const double z = dmul(D(ri), D(g.J));
@@ -247,7 +249,13 @@ struct OpDirection {
     bt = a.st->beta;
     return true;
   }
-  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  // r and J are streamed (evict-first), so that L2 keeps the new p for the
+  // next SpMV
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    g.r = __ldcs(r + i);
+    g.J = __ldcs(J + i);
+  }
   __device__ void compute(long i, Regs& g, double*) const {
     p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }

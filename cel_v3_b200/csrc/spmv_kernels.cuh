@@ -93,25 +93,30 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
   }
   __syncthreads();
 
+  // batched sweeps keep the forward order (their tile state is prefetched
+  // one tile ahead in that order)
+  const int sweep = kB ? 0 : red.sweep;
   if (warp == kConsumerWarps) {
     // ---------------- producer warp ----------------
-    long t = blockIdx.x;
+    [[maybe_unused]] const uint64_t pol = (sweep & 2) ? l2_evict_first_policy() : 0;
+    long k = blockIdx.x;
     int it = 0;
     int bnd = 0;  // lane q (0..4) holds rp at sub-tile boundary q of tile t
-    if (t < ntiles && lane <= kSubPerTile)
-      bnd = __ldg(rp + min(t * kTile + (long)lane * kSub, (long)n));
+    if (k < ntiles && lane <= kSubPerTile)
+      bnd = __ldg(rp + min(tile_at(k, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
     TileInfo nxt{0, 0.0};
     if constexpr (kB) {
-      if (t < ntiles) nxt = epi.tile_info(t);
+      if (k < ntiles) nxt = epi.tile_info(k);
     }
-    for (; t < ntiles; t += gridDim.x) {
+    for (; k < ntiles; k += gridDim.x) {
+      const long t = tile_at(k, ntiles, sweep);
       const int cur = bnd;
-      const long tn = t + gridDim.x;
-      if (tn < ntiles && lane <= kSubPerTile)
-        bnd = __ldg(rp + min(tn * kTile + (long)lane * kSub, (long)n));
+      const long kn = k + gridDim.x;
+      if (kn < ntiles && lane <= kSubPerTile)
+        bnd = __ldg(rp + min(tile_at(kn, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
       if constexpr (kB) {
         const TileInfo ti = nxt;
-        if (tn < ntiles) nxt = epi.tile_info(tn);
+        if (kn < ntiles) nxt = epi.tile_info(kn);
         if (!ti.act) continue;
       }
       for (int q = 0; q < kSubPerTile; ++q) {
@@ -138,10 +143,20 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
             const uint32_t mb = fb ? 0u : (uint32_t)cnt * (uint32_t)(sizeof(CT) + sizeof(VT));
             unsigned char* sb = stages + (size_t)st * L.bytes;
             mbar_arrive_expect_tx(&full[st], rpb + mb);
-            bulk_g2s(sb, rp + row0, rpb, &full[st]);
-            if (!fb && cnt > 0) {
-              bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT), &full[st]);
-              bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
+            if (sweep & 2) {
+              bulk_g2s_hint(sb, rp + row0, rpb, &full[st], pol);
+              if (!fb && cnt > 0) {
+                bulk_g2s_hint(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT),
+                              &full[st], pol);
+                bulk_g2s_hint(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT),
+                              &full[st], pol);
+              }
+            } else {
+              bulk_g2s(sb, rp + row0, rpb, &full[st]);
+              if (!fb && cnt > 0) {
+                bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT), &full[st]);
+                bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
+              }
             }
           }
         }
@@ -161,10 +176,11 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
   if constexpr (kB) {
     if (blockIdx.x < ntiles) nxt = ep.tile_info(blockIdx.x);
   }
-  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
+    const long t = tile_at(k, ntiles, sweep);
     if constexpr (kB) {
       const TileInfo ti = nxt;
-      if (t + gridDim.x < ntiles) nxt = ep.tile_info(t + gridDim.x);
+      if (k + gridDim.x < ntiles) nxt = ep.tile_info(k + gridDim.x);
       if (!ti.act) continue;
       ep.begin_tile(ti);
     }
@@ -244,7 +260,8 @@ __global__ void __launch_bounds__(kLanes, 3)
   if (!epi.active()) return;
   const int j = threadIdx.x;
   const long ntiles = ((long)n + kTile - 1) / kTile;
-  for (long t = blockIdx.x; t < ntiles; t += gridDim.x) {
+  for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
+    const long t = tile_at(kt, ntiles, red.sweep);
     Acc<NR> acc;
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;

@@ -101,7 +101,7 @@ def test_multirhs_bitexact_and_close_to_single(gpu, case):
     m.destroy()
 
 
-@pytest.mark.parametrize("cfg", range(10))
+@pytest.mark.parametrize("cfg", range(15))
 def test_every_spmm_variant_is_bitexact(gpu, cfg, monkeypatch):
     """Each launch variant the autotuner can pick (forced with
     CELG_SPMM_CFG) gives the mirror's bits, including rows longer than the
