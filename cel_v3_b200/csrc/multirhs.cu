@@ -452,44 +452,77 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_pair_kernel(const int* __re
   else multi_grid_finish<1>(red, epi, 0, scratch, &s_flag, s_tot);
 }
 
+// 16-byte vectors of the storage type and the row-sum step on them (each
+// component: s = s + v x with separate roundings, as every SpMM here).
+template <typename VT> struct Vec16;
+template <> struct Vec16<double> { using T = double2; };
+template <> struct Vec16<float> { using T = float4; };
+__device__ __forceinline__ void vacc(double2& s, double v, const double2& x) {
+  s.x = dadd(s.x, dmul(v, x.x));
+  s.y = dadd(s.y, dmul(v, x.y));
+}
+__device__ __forceinline__ void vacc(float4& s, float v, const float4& x) {
+  s.x = vadd(s.x, vmul(v, x.x));
+  s.y = vadd(s.y, vmul(v, x.y));
+  s.z = vadd(s.z, vmul(v, x.z));
+  s.w = vadd(s.w, vmul(v, x.w));
+}
+
 // The same SpMM with 16-byte gathers and rows spread over lanes: a warp
 // works on RS = 4 RP rows per step, lanes 8g..8g+7 on rows g, g+4, ... of
-// the step (RP rows each, whose gathers are all in flight together), and
-// lane l of a row owns the column pairs 2l and 2l + 16, so one gather
-// instruction reads 128 contiguous bytes of X for each of four rows (k even,
-// X 16-byte aligned).  Each lane sums its rows' entries in stored order for
-// its four columns; the row sums are then transposed through shared memory
-// to lane = column, where the epilogue runs row by row in order, so the
-// per-column reductions keep the (q, r) order of the other variants.  The
-// epilogue's operands are staged into shared memory by cp.async at the start
-// of the step.  Per row and entry a warp issues half a gather instead of
-// one, and the epilogue's loads and stores stay coalesced.  RP > 1 gives a
-// warp more gathers in flight at fewer resident CTAs, which keeps the rows
-// of X in use by all CTAs together within L2.  FP64 only.
+// the step (RP rows each, whose gathers are all in flight together).  Lane l
+// of a row owns the W = 16 / sizeof(VT) columns W l + 8 W m (m < NV; FP64:
+// columns 2l, 2l+1, 2l+16, 2l+17; FP32: 4l..4l+3), so one gather
+// instruction reads 128 contiguous bytes of X for each of four rows (k a
+// multiple of W, X 16-byte aligned).  Each lane sums its rows' entries in
+// stored order for its columns; the row sums are then transposed through
+// shared memory to lane = column, where the epilogue runs row by row in
+// order, so the per-column reductions keep the (q, r) order of the other
+// variants.  The FP64 epilogue's operands are staged into shared memory by
+// cp.async at the start of the step (FP32: loaded into registers).  Per row
+// and entry a warp issues half a gather (FP32: a quarter) instead of one,
+// and the epilogue's loads and stores stay coalesced.  RP > 1 gives a warp
+// more gathers in flight at fewer resident CTAs, which keeps the rows of X in
+// use by all CTAs together within L2.
 template <class Epi, int MINB, int U, int RP>
 __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __restrict__ rp,
                                                                const int* __restrict__ ci,
-                                                               const double* __restrict__ v, int n,
-                                                               int k, const double* __restrict__ X,
+                                                               const typename Epi::VT* __restrict__ v,
+                                                               int n, int k,
+                                                               const typename Epi::VT* __restrict__ X,
                                                                Epi epi, RedCtx red) {
+  using VT = typename Epi::VT;
+  using V16 = typename Vec16<VT>::T;
   constexpr int NR = Epi::NRED;
   constexpr int NR1 = NR > 0 ? NR : 1;
-  constexpr int L = 8;        // lanes per row
-  constexpr int RS = 4 * RP;  // rows per step
+  constexpr int L = 8;                     // lanes per row
+  constexpr int RS = 4 * RP;               // rows per step
+  constexpr int W = 16 / (int)sizeof(VT);  // columns per 16-byte load
+  constexpr int NV = 32 / (W * L);         // 16-byte loads per lane and entry
+  constexpr bool kStaged = sizeof(VT) == 8;
   __shared__ double s_w[NR1 * 8 * 32];
   __shared__ double scratch[8];
   __shared__ double s_tot[NR1 * kMaxRhs];
   __shared__ int s_flag;
-  extern __shared__ __align__(16) double s_dyn[];  // per warp: sums [RS][32], operands [RS][64]
+  // per warp: row sums [RS][32] (VT), then (FP64) the staged operands [RS][64]
+  extern __shared__ __align__(16) double s_dyn[];
   if (!epi.active()) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane / L, l = lane % L;
   const bool on = lane < k && epi.col_active(lane);
-  const int cm0 = 2 * l;  // column pairs cm0 and cm0 + 16 (k is even)
-  const bool gon0 = cm0 < k && (epi.col_active(cm0) || epi.col_active(cm0 + 1));
-  const bool gon1 = cm0 + 16 < k && (epi.col_active(cm0 + 16) || epi.col_active(cm0 + 17));
-  double* sw = s_dyn + (long)warp * RS * 96;
-  double* sp = sw + RS * 32;
+  int cm[NV];
+  bool gon[NV];
+#pragma unroll
+  for (int m = 0; m < NV; ++m) {
+    cm[m] = W * l + W * L * m;
+    bool any = false;
+#pragma unroll
+    for (int w = 0; w < W; ++w) any = any || (cm[m] + w < k && epi.col_active(cm[m] + w));
+    gon[m] = cm[m] < k && any;
+  }
+  constexpr int kWarpDoubles = RS * 32 * (int)sizeof(VT) / 8 + (kStaged ? RS * 64 : 0);
+  VT* sw = reinterpret_cast<VT*>(s_dyn + (long)warp * kWarpDoubles);
+  double* sp = s_dyn + (long)warp * kWarpDoubles + RS * 32 * (int)sizeof(VT) / 8;
   const long ntiles = ((long)n + kTile - 1) / kTile;
   for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
     const long t = tile_at(kt, ntiles, red.sweep);
@@ -501,10 +534,17 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __res
       if (row0 >= n) break;
       const int nrows = (int)min(32L, (long)n - row0);
       for (int s0 = 0; s0 < nrows; s0 += RS) {
+        typename Epi::Pre pre[kStaged ? 1 : RS];
+        if constexpr (kStaged) {
 #pragma unroll
-        for (int rr = 0; rr < RS; ++rr)
-          if (on && s0 + rr < nrows) epi.stage_pre(row0 + s0 + rr, lane, sp + rr * 64);
-        cp_async_commit();
+          for (int rr = 0; rr < RS; ++rr)
+            if (on && s0 + rr < nrows) epi.stage_pre(row0 + s0 + rr, lane, sp + rr * 64);
+          cp_async_commit();
+        } else {
+#pragma unroll
+          for (int rr = 0; rr < RS; ++rr)
+            if (on && s0 + rr < nrows) pre[rr] = epi.pre(row0 + s0 + rr, lane);
+        }
         int b[RP], e[RP];
         int lmax = 0;
 #pragma unroll
@@ -514,54 +554,60 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __res
           e[j] = r < nrows ? __ldg(rp + row0 + r + 1) : 0;
           lmax = max(lmax, e[j] - b[j]);
         }
-        double2 sum0[RP], sum1[RP];
+        V16 sum[RP][NV];
 #pragma unroll
-        for (int j = 0; j < RP; ++j) sum0[j] = sum1[j] = make_double2(0.0, 0.0);
+        for (int j = 0; j < RP; ++j)
+#pragma unroll
+          for (int m = 0; m < NV; ++m) sum[j][m] = V16{};
         for (int c0 = 0; c0 < lmax; c0 += U) {
           int cc[RP][U];
-          double vv[RP][U];
+          VT vv[RP][U];
 #pragma unroll
           for (int j = 0; j < RP; ++j)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int kk = b[j] + c0 + u;
               cc[j][u] = kk < e[j] ? __ldg(ci + kk) : 0;
-              vv[j][u] = kk < e[j] ? __ldg(v + kk) : 0.0;
+              vv[j][u] = kk < e[j] ? __ldg(v + kk) : VT(0);
             }
-          double2 x0[RP][U], x1[RP][U];
+          V16 xg[RP][U][NV];
 #pragma unroll
           for (int j = 0; j < RP; ++j)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const bool ok = b[j] + c0 + u < e[j];
-              const double2* xr = reinterpret_cast<const double2*>(X + (long)cc[j][u] * k + cm0);
-              x0[j][u] = (ok && gon0) ? __ldg(xr) : make_double2(0.0, 0.0);
-              x1[j][u] = (ok && gon1) ? __ldg(xr + 8) : make_double2(0.0, 0.0);
+              const VT* xr = X + (long)cc[j][u] * k;
+#pragma unroll
+              for (int m = 0; m < NV; ++m)
+                xg[j][u][m] = (ok && gon[m]) ? __ldg(reinterpret_cast<const V16*>(xr + cm[m])) : V16{};
             }
 #pragma unroll
           for (int j = 0; j < RP; ++j)
 #pragma unroll
             for (int u = 0; u < U; ++u)
               if (b[j] + c0 + u < e[j]) {
-                sum0[j].x = dadd(sum0[j].x, dmul(vv[j][u], x0[j][u].x));
-                sum0[j].y = dadd(sum0[j].y, dmul(vv[j][u], x0[j][u].y));
-                sum1[j].x = dadd(sum1[j].x, dmul(vv[j][u], x1[j][u].x));
-                sum1[j].y = dadd(sum1[j].y, dmul(vv[j][u], x1[j][u].y));
+#pragma unroll
+                for (int m = 0; m < NV; ++m) vacc(sum[j][m], vv[j][u], xg[j][u][m]);
               }
         }
 #pragma unroll
         for (int j = 0; j < RP; ++j)
           if (s0 + g + 4 * j < nrows) {
-            double* srow = sw + (g + 4 * j) * 32;
-            if (cm0 < k) *reinterpret_cast<double2*>(srow + cm0) = sum0[j];
-            if (cm0 + 16 < k) *reinterpret_cast<double2*>(srow + cm0 + 16) = sum1[j];
+            VT* srow = sw + (g + 4 * j) * 32;
+#pragma unroll
+            for (int m = 0; m < NV; ++m)
+              if (cm[m] < k) *reinterpret_cast<V16*>(srow + cm[m]) = sum[j][m];
           }
-        cp_async_wait<0>();
+        if constexpr (kStaged) cp_async_wait<0>();
         __syncwarp();
 #pragma unroll
         for (int rr = 0; rr < RS; ++rr)
-          if (on && s0 + rr < nrows)
-            epi.row(row0 + s0 + rr, lane, sw[rr * 32 + lane], epi.staged(sp + rr * 64, lane), acc);
+          if (on && s0 + rr < nrows) {
+            if constexpr (kStaged)
+              epi.row(row0 + s0 + rr, lane, sw[rr * 32 + lane], epi.staged(sp + rr * 64, lane), acc);
+            else
+              epi.row(row0 + s0 + rr, lane, sw[rr * 32 + lane], pre[rr], acc);
+          }
         __syncwarp();  // the sums are read before the next step overwrites them
       }
     }
@@ -942,20 +988,32 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::
 }
 
 template <class Epi, int MINB, int U, int RP>
-static int launch_spmm_vec(celg_handle* h, const CsrDev& A, int k, const double* X, const Epi& epi) {
+static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
+                           const typename Epi::VT* X, const Epi& epi) {
+  using VT = typename Epi::VT;
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
   red.sweep = next_sweep(h, false, false);
   auto kern = spmm_vec_kernel<Epi, MINB, U, RP>;
-  const int smem = 8 * 4 * RP * 96 * (int)sizeof(double);
+  const int rs = 4 * RP;
+  const int smem = 8 * (rs * 32 * (int)sizeof(VT) + (sizeof(VT) == 8 ? rs * 64 * 8 : 0));
   CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
-  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, A.v, A.n, k, X, epi, red);
+  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, vals, A.n, k, X, epi, red);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
+}
+
+// SpMM of the FP32 inner solve: the 16-byte-gather kernel when k is a
+// multiple of 4 and X is 16-byte aligned, else the register pipeline.
+template <class Epi>
+static int launch_spmm_f32(celg_handle* h, const CsrDev& A, int k, const float* X, const Epi& epi) {
+  if ((k & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0)
+    return launch_spmm_vec<Epi, 4, 4, 1>(h, A, A.v32, k, X, epi);
+  return launch_spmm_cfg<Epi, 4, 4>(h, A, A.v32, k, X, epi);
 }
 
 template <class Epi, int S, int MINB>
@@ -997,11 +1055,11 @@ static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, 
   // aligned rows of X
   if (cfg >= 8 && ((k & 1) || (reinterpret_cast<uintptr_t>(X) & 15))) cfg = 5;
   switch (cfg) {
-    case 10: return launch_spmm_vec<Epi, 2, 8, 1>(h, A, k, X, epi);
-    case 11: return launch_spmm_vec<Epi, 3, 4, 1>(h, A, k, X, epi);
-    case 12: return launch_spmm_vec<Epi, 4, 4, 1>(h, A, k, X, epi);
-    case 13: return launch_spmm_vec<Epi, 2, 4, 2>(h, A, k, X, epi);
-    case 14: return launch_spmm_vec<Epi, 3, 2, 2>(h, A, k, X, epi);
+    case 10: return launch_spmm_vec<Epi, 2, 8, 1>(h, A, A.v, k, X, epi);
+    case 11: return launch_spmm_vec<Epi, 3, 4, 1>(h, A, A.v, k, X, epi);
+    case 12: return launch_spmm_vec<Epi, 4, 4, 1>(h, A, A.v, k, X, epi);
+    case 13: return launch_spmm_vec<Epi, 2, 4, 2>(h, A, A.v, k, X, epi);
+    case 14: return launch_spmm_vec<Epi, 3, 2, 2>(h, A, A.v, k, X, epi);
     case 8: return launch_spmm_pair<Epi, 2, 2>(h, A, k, X, epi);
     case 9: return launch_spmm_pair<Epi, 3, 1>(h, A, k, X, epi);
     case 0: return launch_spmm_cfg<Epi, 2, 8>(h, A, A.v, k, X, epi);
@@ -1299,12 +1357,10 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
   const MOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps, ai, ir.part, ir.part_count};
   int st = launch_mtile(h, n, k, pre);
   if (!st)
-    st = launch_spmm_cfg<MEpiInit<float>, 4, 4>(h, m->csr, m->csr.v32, k, D32,
-                                                MEpiInit<float>{B32, R32, P32, J32, k, ai});
+    st = launch_spmm_f32(h, m->csr, k, D32, MEpiInit<float>{B32, R32, P32, J32, k, ai});
   if (!st)
     st = multi_run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
-      int s2 = launch_spmm_cfg<MEpiAp<float>, 4, 4>(h, m->csr, m->csr.v32, k, P32,
-                                                    MEpiAp<float>{V32, P32, k, ai});
+      int s2 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ai});
       if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{D32, R32, P32, V32, J32, ai, 0.0});
       if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, ai, 0.0});
       return s2;

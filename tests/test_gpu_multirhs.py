@@ -197,14 +197,17 @@ def mirror_ir(rp, ci, v, B, eps_rel, inner_eps, inner_max, outer_max):
 
 
 @pytest.mark.parametrize("mode", ["graph", "host_loop"])
-def test_multirhs_fp32_refinement_bitexact(gpu, mode, monkeypatch):
+@pytest.mark.parametrize("k", [6, 8])
+def test_multirhs_fp32_refinement_bitexact(gpu, mode, k, monkeypatch):
+    """k = 8 runs the inner SpMM with 16-byte gathers of four FP32 columns,
+    k = 6 the register-pipeline SpMM."""
     celgpu, h, torch = gpu
     if mode == "host_loop":
         monkeypatch.setenv("CELG_GRAPH", "0")
     rng = np.random.default_rng(15)
     _, (kx, ky, kz) = synth.lognormal_faces(rng, 9, 8, 10, 0.5)
     rp, ci, v = synth.diffusion7(9, 8, 10, kx, ky, kz)
-    n, k = rp.size - 1, 6
+    n = rp.size - 1
     B = rng.uniform(-1.0, 1.0, (n, k))
     B[:, 3] *= 1e-3                         # columns of different scale
     m = h.matrix_from_csr(rp, ci, v).jacobi()
