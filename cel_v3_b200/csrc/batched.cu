@@ -633,7 +633,7 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
     if (!s2) s2 = launch_tile(h, N, BOpDirection<double>{bt->P, bt->R, bt->J, a, 0.0});
     return s2;
   };
-  if (!st && a.cond) st = capture_while(h, a.cond, body);
+  if (!st && a.cond) st = capture_while2(h, a.cond, body);
   for (int it = 0; !st && !a.cond && it < p->iter_max; it += 8) {
     for (int q = 0; q < 8 && !st; ++q) st = body();
     int live = 0;
@@ -787,7 +787,7 @@ static int batch_ensure_f32(celg_handle* h, Batch* bt) {
 template <class Body>
 static int run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int* n_active, int iter_max,
                      Body&& body) {
-  if (cond) return capture_while(h, cond, body);
+  if (cond) return capture_while2(h, cond, body);
   for (int it = 0; it < iter_max; it += 8) {
     int st = CELG_OK;
     for (int q = 0; q < 8 && !st; ++q) st = body();

@@ -59,6 +59,21 @@ int capture_while(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
   return CELG_OK;
 }
 
+// The same with the loop body recorded twice.  Consecutive sweeps walk the
+// tiles in opposite orders (RedCtx::sweep), so a body of an odd number of
+// sweeps would repeat the same orders in every iteration; with two
+// iterations per body the orders alternate across iterations too.  The
+// body's kernels must return at once when the solve has ended, since the
+// second iteration runs after the first one stopped the loop.
+template <class Body>
+int capture_while2(celg_handle* h, cudaGraphConditionalHandle cond, Body body) {
+  return capture_while(h, cond, [&]() -> int {
+    int st = body();
+    if (!st) st = body();
+    return st;
+  });
+}
+
 // Create a conditional handle on the graph being captured on h->stream
 // (used for an IF node inside a loop body).
 inline int capture_new_handle(celg_handle* h, unsigned default_value, cudaGraphConditionalHandle* out) {

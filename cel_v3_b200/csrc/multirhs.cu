@@ -994,7 +994,7 @@ static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
-  red.sweep = next_sweep(h, false, false);
+  red.sweep = next_sweep(h, false);
   auto kern = spmm_vec_kernel<Epi, MINB, U, RP>;
   const int rs = 4 * RP;
   const int smem = 8 * (rs * 32 * (int)sizeof(VT) + (sizeof(VT) == 8 ? rs * 64 * 8 : 0));
@@ -1077,7 +1077,7 @@ template <class Op>
 static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
-  red.sweep = next_sweep(h, false, false);
+  red.sweep = next_sweep(h, false);
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile_kernel<Op>>(kLanes, 0)));
   mtile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
   CELG_CUDA(cudaGetLastError());
@@ -1268,14 +1268,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
       MultiArgs ac = a;
       ac.cond = cond;
       int s2 = setup(ac);
-      // two iterations per loop body, so that the sweep order alternates
-      // across iterations (the kernels return at once when no column is
-      // active)
-      if (!s2) s2 = capture_while(h, cond, [&]() -> int {
-        int s3 = body(ac);
-        if (!s3) s3 = body(ac);
-        return s3;
-      });
+      if (!s2) s2 = capture_while2(h, cond, [&]() -> int { return body(ac); });
       if (!s2) s2 = tail(ac);
       return s2;
     };
@@ -1332,7 +1325,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
 template <class Body>
 static int multi_run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int* n_active,
                            int iter_max, Body&& body) {
-  if (cond) return capture_while(h, cond, body);
+  if (cond) return capture_while2(h, cond, body);
   for (int it = 0; it < iter_max; it += 8) {
     int st = CELG_OK;
     for (int q = 0; q < 8 && !st; ++q) st = body();

@@ -146,14 +146,7 @@ template <typename VT>
 static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
   int st = pcg_setup(h, B, p, a);
   if (st) return st;
-  // two iterations per loop body, so that the sweep order alternates across
-  // iterations too (the second iteration's kernels return at once when the
-  // first one ended the solve)
-  st = capture_while(h, a.cond, [&]() -> int {
-    int s = pcg_body(h, B, a);
-    if (!s) s = pcg_body(h, B, a);
-    return s;
-  });
+  st = capture_while2(h, a.cond, [&]() -> int { return pcg_body(h, B, a); });
   if (st) return st;
   return pcg_tail(h, B, a);
 }

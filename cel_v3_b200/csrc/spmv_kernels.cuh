@@ -93,9 +93,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
   }
   __syncthreads();
 
-  // batched sweeps keep the forward order (their tile state is prefetched
-  // one tile ahead in that order)
-  const int sweep = kB ? 0 : red.sweep;
+  const int sweep = red.sweep;
   if (warp == kConsumerWarps) {
     // ---------------- producer warp ----------------
     [[maybe_unused]] const uint64_t pol = (sweep & 2) ? l2_evict_first_policy() : 0;
@@ -106,7 +104,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
       bnd = __ldg(rp + min(tile_at(k, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
     TileInfo nxt{0, 0.0};
     if constexpr (kB) {
-      if (k < ntiles) nxt = epi.tile_info(k);
+      if (k < ntiles) nxt = epi.tile_info(tile_at(k, ntiles, sweep));
     }
     for (; k < ntiles; k += gridDim.x) {
       const long t = tile_at(k, ntiles, sweep);
@@ -116,7 +114,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
         bnd = __ldg(rp + min(tile_at(kn, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
       if constexpr (kB) {
         const TileInfo ti = nxt;
-        if (kn < ntiles) nxt = epi.tile_info(kn);
+        if (kn < ntiles) nxt = epi.tile_info(tile_at(kn, ntiles, sweep));
         if (!ti.act) continue;
       }
       for (int q = 0; q < kSubPerTile; ++q) {
@@ -174,13 +172,13 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
   Epi ep = epi;
   TileInfo nxt{0, 0.0};
   if constexpr (kB) {
-    if (blockIdx.x < ntiles) nxt = ep.tile_info(blockIdx.x);
+    if (blockIdx.x < ntiles) nxt = ep.tile_info(tile_at(blockIdx.x, ntiles, sweep));
   }
   for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
     const long t = tile_at(k, ntiles, sweep);
     if constexpr (kB) {
       const TileInfo ti = nxt;
-      if (k + gridDim.x < ntiles) nxt = ep.tile_info(k + gridDim.x);
+      if (k + gridDim.x < ntiles) nxt = ep.tile_info(tile_at(k + gridDim.x, ntiles, sweep));
       if (!ti.act) continue;
       ep.begin_tile(ti);
     }

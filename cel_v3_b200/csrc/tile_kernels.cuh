@@ -36,16 +36,16 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   if (!op.prepare()) return;
   const int j = threadIdx.x;
   const long ntiles = (n + kTile - 1) / kTile;
+  const int sweep = red.sweep;
   TileInfo nxt{0, 0.0};
   if constexpr (kB) {
-    if (blockIdx.x < ntiles) nxt = op.tile_info(blockIdx.x);
+    if (blockIdx.x < ntiles) nxt = op.tile_info(tile_at(blockIdx.x, ntiles, sweep));
   }
-  const int sweep = kB ? 0 : red.sweep;
   for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
     const long t = tile_at(k, ntiles, sweep);
     if constexpr (kB) {
       const TileInfo cur = nxt;
-      if (k + gridDim.x < ntiles) nxt = op.tile_info(k + gridDim.x);
+      if (k + gridDim.x < ntiles) nxt = op.tile_info(tile_at(k + gridDim.x, ntiles, sweep));
       if (!cur.act) continue;
       op.begin_tile(cur);
     }
@@ -110,8 +110,7 @@ int resident_per_sm(int threads, int smem) {
 // (Measured on the 256^3 Poisson PCG: DRAM traffic per iteration 3217 ->
 // 3083 MB, time 538 -> 526 us, together with the streaming loads and stores
 // of the update and direction sweeps.)
-inline int next_sweep(celg_handle* h, bool batched, bool csr) {
-  if (batched) return 0;
+inline int next_sweep(celg_handle* h, bool csr) {
   const int s = h->sweep_rev;
   h->sweep_rev ^= 1;
   return csr ? (s | 2) : s;
@@ -123,7 +122,7 @@ template <class Op>
 int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
-  red.sweep = next_sweep(h, is_batched<Op>::value, false);
+  red.sweep = next_sweep(h, false);
   if (Op::NRED > 0) {
     int st = ensure_partials(h, nt, Op::NRED);
     if (st) return st;
@@ -147,7 +146,7 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
-  red.sweep = next_sweep(h, is_batched<Epi>::value, true);
+  red.sweep = next_sweep(h, true);
   const int smem = csr_smem_bytes(cap, (int)sizeof(VT), (int)sizeof(CT));
   auto kern = csr_tma_kernel<VT, Epi, CT>;
   CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -182,7 +181,7 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
-  red.sweep = next_sweep(h, false, false) & 1;
+  red.sweep = next_sweep(h, false);
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi>>(kLanes, 0)));
   jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
                                                     red);
