@@ -136,12 +136,10 @@ struct BEpiAp {
   __device__ void begin_tile(const TileInfo&) {}
   __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
-  struct Pre { VT p; };
-  __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
-  __device__ void row(long i, VT s, const Pre& g, double* acc) const {
+  __device__ void row(long i, VT s, double* acc) const {
     const VT vi = vadd(VT(0), s);
     v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(D(vi), D(g.p)));
+    acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
   }
   __device__ void finish_sys(int s, double* tot) const {
     const double sg = a.alpha[s] / tot[0];

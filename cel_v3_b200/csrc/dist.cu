@@ -133,13 +133,11 @@ struct DEpiAp {
   double* v;
   const double* p;
   DistArgs a;
-  struct Pre { double p; };
   __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
-  __device__ Pre pre(long i) const { return Pre{__ldg(p + i)}; }
-  __device__ void row(long i, double s, const Pre& g, double* acc) const {
+  __device__ void row(long i, double s, double* acc) const {
     const double vi = dadd(0.0, s);
     v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, g.p));
+    acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
   }
   __device__ void finish(double* tot) const { xch_store(a.st, a, 0.0, 0.0, 0.0, tot[0]); }
 };

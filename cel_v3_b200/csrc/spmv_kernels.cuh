@@ -44,13 +44,9 @@ __device__ __forceinline__ int entry_col(uint8_t c, long row, const int* dict) {
 }
 constexpr int kCsrHeader = 256;  // mbarriers, stage meta, fold scratch
 
-// An epilogue may declare `struct Pre` and `Pre pre(long row) const`: the
-// consumer then loads the row's epilogue operands before its x gathers (so
-// both latencies overlap) and calls row(i, s, pre, acc).
-template <class E, class = void>
-struct has_pre : std::false_type {};
-template <class E>
-struct has_pre<E, std::void_t<typename E::Pre>> : std::true_type {};
+// An epilogue's own vector loads belong in row(), after the row's gathers.
+// Issued before the gathers (tried for the p of p.v), they cost 23 us per
+// 256^3 sweep.
 
 template <int N>
 struct Acc {
@@ -198,10 +194,6 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
       const int fb = meta[2 * st + 1];
       const long row = s * kSub + j;
       if (row < n) {
-        [[maybe_unused]] auto pr = [&] {
-          if constexpr (has_pre<Epi>::value) return ep.pre(row);
-          else return 0;
-        }();
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
         if (!fb) {
@@ -225,8 +217,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
           for (int k = b; k < e; ++k)
             sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + entry_col(__ldg(ci + k), row, s_dict))));
         }
-        if constexpr (has_pre<Epi>::value) ep.row(row, sum, pr, acc.a);
-        else ep.row(row, sum, acc.a);
+        ep.row(row, sum, acc.a);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);
@@ -308,8 +299,7 @@ __global__ void __launch_bounds__(kLanes, 3)
     for (int k = 0; k < 4; ++k) {
       if (i[k] < n) {
         const long row = (long)__ldg(perm + i[k]);
-        if constexpr (has_pre<Epi>::value) epi.row(row, sum[k], epi.pre(row), acc.a);
-        else epi.row(row, sum[k], acc.a);
+        epi.row(row, sum[k], acc.a);
       }
     }
     if (NR > 0) {
