@@ -330,7 +330,7 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
         RuArgs a{sd, h->hist_d, hist_cap, p->iter_max, cond, h->err_d, 0};
         int s2 = ru_setup(h, m, b, x, p, a, r, pv, d);
         if (!s2)
-          s2 = capture_while(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d, true); });
+          s2 = capture_while2(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d, true); });
         if (!s2) s2 = ru_tail(h, m, b, x, a, d);
         return s2;
       }, &ge);
