@@ -600,7 +600,9 @@ def run_gpu(args):
     iters = last.iter_done
     value = world * args.steps / (ms / 1e3)
     ms_per_step = ms / args.steps
-    pcg_bytes = 12 * nnz + 4 * (n + 1) + 104 * n
+    # algorithmic bytes of one iteration: K1 (matrix, p gathered, v stored),
+    # K2 (r, v, J read, r stored), K3 (p, r, J, x read, p, x stored)
+    pcg_bytes = 12 * nnz + 4 * (n + 1) + 96 * n
 
     # ---- roofline: the CSR SpMV kernel alone ----
     y = torch.empty_like(b)

@@ -6,10 +6,11 @@
 //
 // Per iteration (reference lines in brackets):
 //   K1  v = 0 + A p, pv = v.p, sigma = alpha/pv          [:251-261]
-//   K2  x += sigma p, r += (-sigma) v, z = J r (not stored),
+//   K2  r += (-sigma) v, z = J r (not stored),
 //       rz = r.z, rr = r.r, beta = rz/alpha, alpha = rz,
-//       ||r|| = sqrt(rr), convergence test               [:263-277, :287, :247-249]
-//   K3  p = beta p + J r                                  [:282]
+//       ||r|| = sqrt(rr), convergence test               [:265-277, :287, :247-249]
+//   K3  x += sigma p (the iteration's x update, :263-264, moved here
+//       because K3 reads the old p anyway), then p = beta p + J r  [:282]
 // Set-up: x0, ||b|| and eps (Kpre); r = b - A x, p = J r, alpha = r.p,
 // ||r|| (Kinit) [:207-236].  After the loop one more sweep recomputes
 // ||b - A x|| in FP64 (verification; not part of the reference).
@@ -19,7 +20,9 @@
 // vector update is computed in double from the float operands and rounded
 // once, reductions and scalars are double.  For VT = double the arithmetic
 // is exactly the reference's.
-// Algorithmic bytes per FP64 CSR iteration: 12 nnz + 4 (n+1) + 104 n.
+// Algorithmic bytes per FP64 CSR iteration: 12 nnz + 4 (n+1) + 96 n (K1
+// 12 nnz + 4 (n+1) + 16 n, p gathered and v stored, the p of p.v coming
+// from L1/L2; K2 32 n; K3 48 n).
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -121,8 +124,8 @@ static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
       return s2;
     }
   }
-  if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.x, B.r, B.p, B.v, B.J, a, 0.0});
-  if (!s2) s2 = launch_tile(h, n, OpDirection<VT>{B.p, B.r, B.J, a, 0.0});
+  if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.r, B.v, B.J, a, 0.0});
+  if (!s2) s2 = launch_tile(h, n, OpDirectionX<VT>{B.p, B.r, B.J, B.x, a});
   return s2;
 }
 
@@ -285,7 +288,7 @@ int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const cel
   std::memset(&s, 0, sizeof(s));
   const int ret = pcg_run<double>(h, B, p, m, &s);
   h->last_iters = s.iter;
-  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 104.0 * n;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 96.0 * n;
   if (res) {
     res->iter_done = s.iter;
     res->final_norm2 = s.norm;

@@ -13,6 +13,7 @@ constexpr double kRealSmall = 1.1 * 2.220446049250313e-16;  // cel_real_small
 struct PcgState {
   double alpha, sigma, beta, norm, bnorm, eps, pvd, rz, vres;
   int iter, active, err, hist_len;
+  int xpend;  // K2 ran: K3 owes x += sigma p
 };
 
 struct PcgArgs {
@@ -109,6 +110,7 @@ struct OpPre {
     st->active = 1;
     st->alpha = st->sigma = st->beta = st->pvd = st->rz = 0.0;
     st->vres = 0.0;
+    st->xpend = 0;
   }
 };
 
@@ -183,14 +185,15 @@ struct EpiAp {
   }
 };
 
-// K2: x += sigma p; r += (-sigma) v; z = J r; rz, rr; scalars and stopping test
+// K2: r += (-sigma) v; z = J r; rz, rr; scalars and stopping test.  The
+// iteration's x += sigma p (:263-265) is left to K3, which reads the old p
+// anyway, so this sweep reads neither x nor p; K2 marks it pending.  Each x
+// element gets the same operation in the same iteration as before.
 template <typename VT>
 struct OpUpdate {
   static constexpr int NRED = 2;
-  struct Regs { VT x, r, p, v, J; };
-  VT* x;
+  struct Regs { VT r, v, J; };
   VT* r;
-  const VT* p;
   const VT* v;
   const VT* J;
   PcgArgs a;
@@ -203,17 +206,14 @@ struct OpUpdate {
     sg = a.st->sigma;
     return true;
   }
-  // x and v are not read again before the next update sweep: streamed
-  // (evict-first), so that L2 keeps r, p and J for the direction sweep
+  // v is not read again before the next update sweep: streamed (evict-first),
+  // so that L2 keeps r and J for the direction sweep
   __device__ void load(long i, Regs& g) const {
-    g.x = __ldcs(x + i);
     g.r = r[i];
-    g.p = __ldg(p + i);
     g.v = __ldcs(v + i);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
     const VT ri = R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     r[i] = ri;
     const double z = dmul(D(ri), D(g.J));
@@ -229,9 +229,50 @@ struct OpUpdate {
     st->iter += 1;
     if (a.hist && st->iter < a.hist_cap) a.hist[st->iter] = st->norm;
     st->hist_len = st->iter + 1;
+    st->xpend = 1;
     st->active = pcg_go(st, a.iter_max, a.errw);
     set_cond(a.cond, st->active);
   }
+};
+
+// K3 of the PCG: x += sigma p when K2 left it pending (also after K2 ended
+// the solve), then p = beta p + J r (:282) while the solve goes on.  The
+// last CTA clears the pending mark.
+template <typename VT>
+struct OpDirectionX {
+  static constexpr int NRED = 0;
+  static constexpr bool kFinishAlways = true;
+  struct Regs { VT p, r, J, x; };
+  VT* p;
+  const VT* r;
+  const VT* J;
+  VT* x;
+  PcgArgs a;
+  double bt = 0.0, sg = 0.0;
+  int xp = 0, act = 0;
+  __device__ bool prepare() {
+    xp = *(volatile int*)&a.st->xpend;
+    act = *(volatile int*)&a.st->active;
+    if (!xp && !act) return false;
+    bt = a.st->beta;
+    sg = a.st->sigma;
+    return true;
+  }
+  // r, J and x are streamed (evict-first), so that L2 keeps the new p for
+  // the next SpMV
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldcs(J + i);
+    }
+    if (xp) g.x = __ldcs(x + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (xp) __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+    if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish(double*) const { a.st->xpend = 0; }
 };
 
 // K3: p = beta p + J r
