@@ -15,7 +15,8 @@
 // are reduced with the single-vector order (lane j sums j, j+256, ...,
 // butterfly, warps in order).
 //
-// Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 104 n k.
+// Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 96 n k (SpMM 16 n k,
+// update sweep 32 n k, direction sweep 48 n k; J is n doubles, not counted).
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
@@ -33,6 +34,9 @@ constexpr int kMaxRhs = 32;
 struct MultiArgs {
   double *alpha, *sigma, *beta, *norm, *bnorm, *eps, *vres;
   int *iter, *active, *err, *n_active;
+  // columns whose update sweep ran and whose x += sigma p the direction
+  // sweep still owes (bit c = column c)
+  unsigned* xmask;
   int k;
   int iter_max;
   cudaGraphConditionalHandle cond;
@@ -689,7 +693,10 @@ struct MOpPre {
     a.active[c] = part ? (part[c] ? 1 : 0) : 1;
     a.vres[c] = 0.0;
   }
-  __device__ void finish_global() const { *a.n_active = part_count ? *part_count : a.k; }
+  __device__ void finish_global() const {
+    *a.n_active = part_count ? *part_count : a.k;
+    *a.xmask = 0u;
+  }
 };
 
 // r = b - (0 + A x); p = J r; alpha = r.p; ||r||  (columns set active by MOpPre)
@@ -764,14 +771,14 @@ struct MEpiAp {
   __device__ void finish_global() const {}
 };
 
-// K2: x += sigma p; r += (-sigma) v; rz, rr; per-column scalars and test
+// K2: r += (-sigma) v; rz, rr; per-column scalars and test.  The column's
+// x += sigma p is left to the direction sweep, which reads the old p anyway
+// (bit c of xmask), so this sweep reads neither X nor P.
 template <typename VT>
 struct MOpUpdate {
   static constexpr int NRED = 2;
-  struct Regs { VT x, r, p, v, J; };
-  VT* X;
+  struct Regs { VT r, v, J; };
   VT* R;
-  const VT* P;
   const VT* V;
   const VT* J;
   MultiArgs a;
@@ -779,17 +786,14 @@ struct MOpUpdate {
   __device__ bool prepare() { return true; }
   __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
   __device__ void begin_col(int c) { sg = a.sigma[c]; }
-  // x and v are not read again before the next update sweep: streamed
-  // (evict-first), so that L2 keeps r and p for the direction sweep
+  // v is not read again before the next update sweep: streamed
+  // (evict-first), so that L2 keeps r for the direction sweep
   __device__ void load(long e, long i, Regs& g) const {
-    g.x = __ldcs(X + e);
     g.r = R[e];
-    g.p = __ldg(P + e);
     g.v = __ldcs(V + e);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long e, long, Regs& g, double* acc) const {
-    __stcs(X + e, celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
     const VT ri = celg::R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     R[e] = ri;
     const double z = dmul(D(ri), D(g.J));
@@ -802,35 +806,54 @@ struct MOpUpdate {
     a.alpha[c] = tot[0];
     a.norm[c] = sqrt(tot[1]);
     a.iter[c] += 1;
+    atomicOr(a.xmask, 1u << c);
     a.settle(c);
   }
   __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
 };
 
-// K3: p = beta p + J r
+// K3: per column, x += sigma p when the update sweep left it pending (also
+// after that sweep stopped the column), then p = beta p + J r while the
+// column goes on.  The last CTA clears the pending mask.
 template <typename VT>
 struct MOpDirection {
   static constexpr int NRED = 0;
-  struct Regs { VT p, r, J; };
+  struct Regs { VT p, r, J, x; };
   VT* P;
   const VT* R;
   const VT* J;
+  VT* X;
   MultiArgs a;
-  double bt;
-  __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
-  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
-  __device__ void begin_col(int c) { bt = a.beta[c]; }
-  // r is streamed (evict-first), so that L2 keeps the new p for the SpMM
+  double bt = 0.0, sg = 0.0;
+  bool xp = false, act = false;
+  __device__ bool prepare() {
+    return *(volatile int*)a.n_active > 0 || *(volatile unsigned*)a.xmask != 0u;
+  }
+  __device__ bool col_active(int c) const {
+    return *(volatile int*)&a.active[c] != 0 || ((*(volatile unsigned*)a.xmask >> c) & 1u);
+  }
+  __device__ void begin_col(int c) {
+    bt = a.beta[c];
+    sg = a.sigma[c];
+    act = *(volatile int*)&a.active[c] != 0;
+    xp = ((*(volatile unsigned*)a.xmask >> c) & 1u) != 0;
+  }
+  // r and x are streamed (evict-first), so that L2 keeps the new p for the
+  // SpMM
   __device__ void load(long e, long i, Regs& g) const {
     g.p = P[e];
-    g.r = __ldcs(R + e);
-    g.J = __ldg(J + i);
+    if (act) {
+      g.r = __ldcs(R + e);
+      g.J = __ldg(J + i);
+    }
+    if (xp) g.x = __ldcs(X + e);
   }
   __device__ void compute(long e, long, Regs& g, double*) const {
-    P[e] = celg::R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+    if (xp) __stcs(X + e, celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+    if (act) P[e] = celg::R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
   __device__ void finish_col(int, double*) const {}
-  __device__ void finish_global() const {}
+  __device__ void finish_global() const { *a.xmask = 0u; }
 };
 
 // ||b - A x|| / ||b|| per column
@@ -1172,6 +1195,7 @@ static MultiArgs multi_args(double* ds, int* is, int k, int iter_max, cudaGraphC
   a.active = a.iter + kMaxRhs;
   a.err = a.active + kMaxRhs;
   a.n_active = a.err + kMaxRhs;
+  a.xmask = reinterpret_cast<unsigned*>(a.n_active + 1);
   a.k = k;
   a.iter_max = iter_max;
   a.errw = errw;
@@ -1200,7 +1224,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   }
   if (!mu->dstate) {
     CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 1)));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
   }
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
@@ -1219,6 +1243,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   a.active = a.iter + kMaxRhs;
   a.err = a.active + kMaxRhs;
   a.n_active = a.err + kMaxRhs;
+  a.xmask = reinterpret_cast<unsigned*>(a.n_active + 1);
   a.k = k;
   a.iter_max = p->iter_max;
   a.errw = h->err_d;
@@ -1239,8 +1264,8 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   };
   auto body = [&](const MultiArgs& ac) -> int {
     int s3 = launch_spmm(h, m->csr, k, P, MEpiAp<double>{V, P, k, ac}, cfg);
-    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate<double>{X, R, P, V, m->jacobi, ac, 0.0});
-    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection<double>{P, R, m->jacobi, ac, 0.0});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate<double>{R, V, m->jacobi, ac, 0.0});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection<double>{P, R, m->jacobi, X, ac});
     return s3;
   };
   auto tail = [&](const MultiArgs& ac) -> int {
@@ -1315,7 +1340,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     }
   }
   h->last_iters = iters;
-  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 104.0 * (double)nk;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 96.0 * (double)nk;
   return ret;
 }
 
@@ -1354,8 +1379,8 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
   if (!st)
     st = multi_run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
       int s2 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ai});
-      if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{D32, R32, P32, V32, J32, ai, 0.0});
-      if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, ai, 0.0});
+      if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{R32, V32, J32, ai, 0.0});
+      if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, D32, ai});
       return s2;
     });
   return st;
@@ -1381,7 +1406,7 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
   }
   if (!mu->dstate) {
     CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 1)));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
   }
   if (nk > mu->f32cap || !mu->f32) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
@@ -1394,7 +1419,7 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
   if (!mu->irs) {
     CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
     CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 1)));
+    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 2)));
   }
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
