@@ -275,34 +275,6 @@ struct OpDirectionX {
   __device__ void finish(double*) const { a.st->xpend = 0; }
 };
 
-// K3: p = beta p + J r
-template <typename VT>
-struct OpDirection {
-  static constexpr int NRED = 0;
-  struct Regs { VT p, r, J; };
-  VT* p;
-  const VT* r;
-  const VT* J;
-  PcgArgs a;
-  double bt;
-  __device__ bool prepare() {
-    if (*(volatile int*)&a.st->active == 0) return false;
-    bt = a.st->beta;
-    return true;
-  }
-  // r and J are streamed (evict-first), so that L2 keeps the new p for the
-  // next SpMV
-  __device__ void load(long i, Regs& g) const {
-    g.p = p[i];
-    g.r = __ldcs(r + i);
-    g.J = __ldcs(J + i);
-  }
-  __device__ void compute(long i, Regs& g, double*) const {
-    p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
-  }
-  __device__ void finish(double*) const {}
-};
-
 // verification: ||b - A x|| / ||b|| (residual not stored)
 struct EpiVerify {
   static constexpr int NRED = 1;

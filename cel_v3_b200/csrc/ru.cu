@@ -89,6 +89,7 @@ struct OpRuPre {
     r->delta = delta;
     r->update = 1;  // the set-up residual is a reliable update
     r->updates = 0;
+    r->s.xpend = 0;
   }
 };
 
@@ -134,13 +135,13 @@ struct EpiRuResidual {
   }
 };
 
-// d += sigma p ; r -= sigma v ; rz' = r.J r ; ||r||^2 ; update decision
+// r -= sigma v ; rz' = r.J r ; ||r||^2 ; update decision.  The iteration's
+// d += sigma p is left pending (s.xpend) for the flush or the direction
+// sweep, which read p anyway, so this sweep reads neither d nor p.
 struct OpRuStep {
   static constexpr int NRED = 2;
-  struct Regs { float d, r, p, v, J; };
-  float* d;
+  struct Regs { float r, v, J; };
   float* r;
-  const float* p;
   const float* v;
   const float* J;
   RuArgs a;
@@ -154,14 +155,11 @@ struct OpRuStep {
     return true;
   }
   __device__ void load(long i, Regs& g) const {
-    g.d = d[i];
     g.r = r[i];
-    g.p = __ldg(p + i);
-    g.v = __ldg(v + i);
+    g.v = __ldcs(v + i);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    d[i] = (float)dadd((double)g.d, dmul(sg, (double)g.p));
     const float ri = (float)dadd((double)g.r, dmul(-sg, (double)g.v));
     r[i] = ri;
     const double z = dmul((double)ri, (double)g.J);
@@ -177,6 +175,7 @@ struct OpRuStep {
     st->s.iter += 1;
     if (a.hist && st->s.iter < a.hist_cap) a.hist[st->s.iter] = st->s.norm;
     st->s.hist_len = min(st->s.iter + 1, a.hist_cap);
+    st->s.xpend = 1;
     const int upd = (st->s.norm < st->delta * st->maxr) || (st->s.norm <= st->s.eps) ||
                     (st->s.iter >= a.iter_max);
     st->update = upd;
@@ -193,21 +192,75 @@ struct OpRuStep {
   }
 };
 
-// x64 += (double) d ; d = 0   (pending update, or unconditionally at the end)
+// x64 += (double) d ; d = 0   (pending update, or unconditionally at the end).
+// A d += sigma p still pending from the step is applied first, with the
+// step's rounding, and the last CTA clears the mark.
 struct OpRuFlush {
   static constexpr int NRED = 0;
-  struct Regs { double x; float d; };
+  static constexpr bool kFinishAlways = true;
+  struct Regs { double x; float d, p; };
   double* x;
   float* d;
+  const float* p;
   RuArgs a;
   int always;
-  __device__ bool prepare() { return always || *(volatile int*)&a.st->update != 0; }
-  __device__ void load(long i, Regs& g) const { g.x = x[i]; g.d = d[i]; }
+  int dp = 0;
+  double sg = 0.0;
+  __device__ bool prepare() {
+    if (!(always || *(volatile int*)&a.st->update != 0)) return false;
+    dp = p != nullptr && *(volatile int*)&a.st->s.xpend;
+    sg = a.st->s.sigma;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const {
+    g.x = x[i];
+    g.d = d[i];
+    if (dp) g.p = __ldg(p + i);
+  }
   __device__ void compute(long i, Regs& g, double*) const {
-    x[i] = dadd(g.x, (double)g.d);
+    const float di = dp ? (float)dadd((double)g.d, dmul(sg, (double)g.p)) : g.d;
+    x[i] = dadd(g.x, (double)di);
     d[i] = 0.0f;
   }
-  __device__ void finish(double*) const {}
+  __device__ void finish(double*) const { a.st->s.xpend = 0; }
+};
+
+// K3: d += sigma p when the step left it pending (no reliable update in
+// between; also after the step stopped the solve), then p = beta p + J r
+// while the solve goes on.  The last CTA clears the mark.
+struct OpRuDirection {
+  static constexpr int NRED = 0;
+  static constexpr bool kFinishAlways = true;
+  struct Regs { float p, r, J, d; };
+  float* p;
+  const float* r;
+  const float* J;
+  float* d;
+  RuArgs a;
+  int dp = 0, act = 0;
+  double bt = 0.0, sg = 0.0;
+  __device__ bool prepare() {
+    dp = *(volatile int*)&a.st->s.xpend;
+    act = *(volatile int*)&a.st->s.active;
+    if (!dp && !act) return false;
+    bt = a.st->s.beta;
+    sg = a.st->s.sigma;
+    return true;
+  }
+  // r, J and d are streamed (evict-first), so that L2 keeps the new p
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldcs(J + i);
+    }
+    if (dp) g.d = __ldcs(d + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (dp) __stcs(d + i, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
+    if (act) p[i] = R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish(double*) const { a.st->s.xpend = 0; }
 };
 
 // final check ||b - A x|| / ||b|| in FP64
@@ -258,21 +311,21 @@ static int ru_body(celg_handle* h, celg_mat* m, const double* b, double* x, RuAr
   }
   PcgArgs pa = a.pcg();
   int st = launch_csr<float>(h, m->csr, m->csr.v32, pv, EpiAp<float>{v, pv, pa});
-  if (!st) st = launch_tile(h, n, OpRuStep{d, r, pv, v, m->jacobi32, a, 0.0});
+  if (!st) st = launch_tile(h, n, OpRuStep{r, v, m->jacobi32, a, 0.0});
   auto update = [&]() -> int {
-    int s2 = launch_tile(h, n, OpRuFlush{x, d, a, 0});
+    int s2 = launch_tile(h, n, OpRuFlush{x, d, pv, a, 0});
     if (!s2)
       s2 = launch_csr<double>(h, m->csr, m->csr.v, x,
                               EpiRuResidual{b, r, nullptr, m->jacobi32, a, 0});
     return s2;
   };
   if (!st) st = in_graph ? capture_if(h, a.cond_update, update) : update();
-  if (!st) st = launch_tile(h, n, OpDirection<float>{pv, r, m->jacobi32, pa, 0.0});
+  if (!st) st = launch_tile(h, n, OpRuDirection{pv, r, m->jacobi32, d, a});
   return st;
 }
 
 static int ru_tail(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* d) {
-  int st = launch_tile(h, m->csr.n, OpRuFlush{x, d, a, 1});
+  int st = launch_tile(h, m->csr.n, OpRuFlush{x, d, nullptr, a, 1});
   if (!st) st = launch_csr<double>(h, m->csr, m->csr.v, x, EpiRuVerify{b, a.st});
   return st;
 }
@@ -352,7 +405,7 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   else if (s.s.err) ret = s.s.err;
   else if (!(s.norm64 <= s.s.eps)) ret = CELG_ERR_NOCONV;
   h->last_iters = s.s.iter;
-  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 52.0 * n;
+  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 48.0 * n;
   if (res) {
     res->iter_done = s.s.iter;
     res->final_norm2 = s.norm64;
