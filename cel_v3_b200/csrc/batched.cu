@@ -28,6 +28,7 @@ namespace celg {
 struct BatchArgs {
   double *alpha, *sigma, *beta, *norm, *bnorm, *eps, *vres;
   int *iter, *active, *err, *n_active;
+  int* xpend;  // per system: the update sweep ran, the direction sweep owes x += sigma p
   BatchRed br;
   int nsys;
   int nlive;  // systems with rows (empty systems are never active)
@@ -75,6 +76,7 @@ struct BOpPre {
     acc[0] = dadd(acc[0], dmul(D(g.b), D(g.b)));
   }
   __device__ void finish_sys(int s, double* tot) const {
+    a.xpend[s] = 0;
     a.bnorm[s] = sqrt(tot[0]);
     double e = eps_abs;
     if (eps_rel > 0.0 && eps_rel * a.bnorm[s] > e) e = eps_rel * a.bnorm[s];
@@ -153,15 +155,15 @@ struct BEpiAp {
   __device__ void finish_global() const {}
 };
 
-// K2: x += sigma p; r += (-sigma) v; rz, rr; scalars and per-system test
+// K2: r += (-sigma) v; rz, rr; scalars and per-system test.  The system's
+// x += sigma p is left to the direction sweep, which reads the old p anyway
+// (xpend[s]), so this sweep reads neither x nor p.
 template <typename VT>
 struct BOpUpdate {
   static constexpr int NRED = 2;
   static constexpr bool kBatched = true;
-  struct Regs { VT x, r, p, v, J; };
-  VT* x;
+  struct Regs { VT r, v, J; };
   VT* r;
-  const VT* p;
   const VT* v;
   const VT* J;
   BatchArgs a;
@@ -175,14 +177,11 @@ struct BOpUpdate {
   __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
   __device__ void load(long i, Regs& g) const {
-    g.x = x[i];
     g.r = r[i];
-    g.p = __ldg(p + i);
-    g.v = __ldg(v + i);
+    g.v = __ldcs(v + i);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    x[i] = R<VT>(dadd(D(g.x), dmul(sg, D(g.p))));
     const VT ri = R<VT>(dadd(D(g.r), dmul(-sg, D(g.v))));
     r[i] = ri;
     const double z = dmul(D(ri), D(g.J));
@@ -194,37 +193,62 @@ struct BOpUpdate {
     a.alpha[s] = tot[0];
     a.norm[s] = sqrt(tot[1]);
     a.iter[s] += 1;
+    a.xpend[s] = 1;
     a.settle(s);
   }
   __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
 };
 
-// K3: p = beta p + J r
+// K3: per system, x += sigma p when the update sweep left it pending (also
+// after that sweep stopped the system), then p = beta p + J r while the
+// system goes on.  TileInfo.act: bit 0 active, bit 1 x pending; s = beta,
+// s2 = sigma.  The marks are cleared by clear_marks_kernel after the sweep.
 template <typename VT>
 struct BOpDirection {
   static constexpr int NRED = 0;
   static constexpr bool kBatched = true;
-  struct Regs { VT p, r, J; };
+  struct Regs { VT p, r, J, x; };
   VT* p;
   const VT* r;
   const VT* J;
+  VT* x;
   BatchArgs a;
-  double bt;
-  __device__ bool prepare() { return *(volatile int*)a.n_active > 0; }
+  double bt = 0.0, sg = 0.0;
+  int act = 0, xp = 0;
+  __device__ bool prepare() { return true; }
   __device__ TileInfo tile_info(long t) const {
     const int s = a.sys_of(t);
-    return TileInfo{*(volatile int*)&a.active[s], a.beta[s]};
+    const int f = (*(volatile int*)&a.active[s] != 0 ? 1 : 0) |
+                  (*(volatile int*)&a.xpend[s] != 0 ? 2 : 0);
+    return TileInfo{f, a.beta[s], a.sigma[s]};
   }
-  __device__ void begin_tile(const TileInfo& ti) { bt = ti.s; }
+  __device__ void begin_tile(const TileInfo& ti) {
+    act = ti.act & 1;
+    xp = ti.act & 2;
+    bt = ti.s;
+    sg = ti.s2;
+  }
   __device__ bool sys_active(int) const { return false; }
   __device__ const BatchRed& bred() const { return a.br; }
-  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldg(J + i);
+    }
+    if (xp) g.x = __ldcs(x + i);
+  }
   __device__ void compute(long i, Regs& g, double*) const {
-    p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+    if (xp) __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+    if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
   __device__ void finish_sys(int, double*) const {}
   __device__ void finish_global() const {}
 };
+
+__global__ void clear_marks_kernel(int* marks, int count) {
+  for (int s = threadIdx.x; s < count; s += blockDim.x) marks[s] = 0;
+}
 
 // ||b - A x|| / ||b|| per system
 struct BEpiVerify {
@@ -437,7 +461,7 @@ struct Batch {
   int* tile_arrays = nullptr;  // tile_sys[NT], sys_tile0[nsys], sys_ntiles[nsys]
   unsigned* sys_ticket = nullptr;
   double* dstate = nullptr;    // 7 x nsys doubles
-  int* istate = nullptr;       // 3 x nsys ints + n_active
+  int* istate = nullptr;       // 3 x nsys ints + n_active + nsys pending marks
   int nlive = 0;               // systems with at least one row
   std::vector<long> row_off;
   std::vector<int> n;
@@ -446,7 +470,7 @@ struct Batch {
   float* F = nullptr;          // 5 x N floats: B32 D32 R32 P32 V32
   int* irs = nullptr;          // part, done, status, outer, inner_total (nsys each), part_count
   double* dstate2 = nullptr;   // inner-solve scalars, 7 x nsys
-  int* istate2 = nullptr;      // inner-solve counters, 3 x nsys + 1
+  int* istate2 = nullptr;      // inner-solve counters, 4 x nsys + 1
 };
 
 namespace celg {
@@ -512,7 +536,7 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
   ok(cudaMalloc(&bt->tile_arrays, sizeof(int) * ((size_t)bt->NT + 2 * (size_t)count + 1)));
   ok(cudaMalloc(&bt->sys_ticket, sizeof(unsigned) * (size_t)count));
   ok(cudaMalloc(&bt->dstate, sizeof(double) * 7 * (size_t)count));
-  ok(cudaMalloc(&bt->istate, sizeof(int) * (3 * (size_t)count + 1)));
+  ok(cudaMalloc(&bt->istate, sizeof(int) * (4 * (size_t)count + 1)));
   if (e != cudaSuccess) {
     batch_free(bt);
     return cuda_status(e, "batch allocation");
@@ -581,6 +605,7 @@ static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle 
   a.active = a.iter + c;
   a.err = a.active + c;
   a.n_active = a.err + c;
+  a.xpend = a.n_active + 1;
   a.br.tile_sys = bt->tile_arrays;
   a.br.sys_tile0 = bt->tile_arrays + bt->NT;
   a.br.sys_ntiles = bt->tile_arrays + bt->NT + c;
@@ -604,6 +629,12 @@ static int batch_finish(celg_handle* h, const Batch* bt, const Op& op) {
   return CELG_OK;
 }
 
+static int clear_marks(celg_handle* h, const BatchArgs& a) {
+  clear_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.xpend, a.nsys);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
                           const celg_params* p, BatchArgs a) {
   const long N = bt->N;
@@ -618,7 +649,7 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
   const BOpPre<double> pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
   const BEpiInit<double> init{bt->B, bt->R, bt->P, bt->J, a};
   const BEpiAp<double> ap{bt->V, bt->P, a};
-  const BOpUpdate<double> upd{bt->X, bt->R, bt->P, bt->V, bt->J, a, 0.0};
+  const BOpUpdate<double> upd{bt->R, bt->V, bt->J, a, 0.0};
   int st = launch_tile(h, N, pre);
   if (!st) st = batch_finish(h, bt, pre);
   if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, init);
@@ -628,7 +659,8 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
     if (!s2) s2 = batch_finish(h, bt, ap);
     if (!s2) s2 = launch_tile(h, N, upd);
     if (!s2) s2 = batch_finish(h, bt, upd);
-    if (!s2) s2 = launch_tile(h, N, BOpDirection<double>{bt->P, bt->R, bt->J, a, 0.0});
+    if (!s2) s2 = launch_tile(h, N, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
+    if (!s2) s2 = clear_marks(h, a);
     return s2;
   };
   if (!st && a.cond) st = capture_while2(h, a.cond, body);
@@ -773,7 +805,7 @@ static int batch_ensure_f32(celg_handle* h, Batch* bt) {
   ok(cudaMalloc(&bt->F, sizeof(float) * N * 5));
   ok(cudaMalloc(&bt->irs, sizeof(int) * (5 * c + 1)));
   ok(cudaMalloc(&bt->dstate2, sizeof(double) * 7 * c));
-  ok(cudaMalloc(&bt->istate2, sizeof(int) * (3 * c + 1)));
+  ok(cudaMalloc(&bt->istate2, sizeof(int) * (4 * c + 1)));
   ok(cudaMemsetAsync(bt->F, 0, sizeof(float) * N * 5, h->stream));
   ok(cudaMemsetAsync(bt->A.v32 + NNZ, 0, sizeof(float) * 32, h->stream));
   if (e != cudaSuccess) return cuda_status(e, "batch FP32 allocation");
@@ -809,7 +841,7 @@ static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, Ba
   const BOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps_rel, ai, ir.part, ir.part_count};
   const BEpiInit<float> init{B32, R32, P32, bt->J32, ai};
   const BEpiAp<float> ap{V32, P32, ai};
-  const BOpUpdate<float> upd{D32, R32, P32, V32, bt->J32, ai, 0.0};
+  const BOpUpdate<float> upd{R32, V32, bt->J32, ai, 0.0};
   int st = launch_tile(h, N, pre);
   if (!st) st = batch_finish(h, bt, pre);
   if (!st) st = launch_csr<float>(h, bt->A, bt->A.v32, D32, init);
@@ -820,7 +852,8 @@ static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, Ba
       if (!s2) s2 = batch_finish(h, bt, ap);
       if (!s2) s2 = launch_tile(h, N, upd);
       if (!s2) s2 = batch_finish(h, bt, upd);
-      if (!s2) s2 = launch_tile(h, N, BOpDirection<float>{P32, R32, bt->J32, ai, 0.0});
+      if (!s2) s2 = launch_tile(h, N, BOpDirection<float>{P32, R32, bt->J32, D32, ai});
+      if (!s2) s2 = clear_marks(h, ai);
       return s2;
     });
   return st;

@@ -291,6 +291,7 @@ struct BatchRed {
 struct TileInfo {
   int act;
   double s;
+  double s2 = 0.0;
 };
 
 template <class T, class = void>
