@@ -600,9 +600,11 @@ def run_gpu(args):
     iters = last.iter_done
     value = world * args.steps / (ms / 1e3)
     ms_per_step = ms / args.steps
-    # algorithmic bytes of one iteration: K1 (matrix, p gathered, v stored),
-    # K2 (r, v, J read, r stored), K3 (p, r, J, x read, p, x stored)
-    pcg_bytes = 12 * nnz + 4 * (n + 1) + 96 * n
+    # algorithmic bytes of one iteration, as the library accounts them for the
+    # solve it ran: K1 (matrix, p gathered, v stored), K2 (r, v, J read, r
+    # stored), K3 (p, r, J, x read, p, x stored); the matrix is 9 bytes per
+    # non-zero with 1-byte column offsets, else 12
+    pcg_bytes = int(h.elm_performance()[2])
 
     # ---- roofline: the CSR SpMV kernel alone ----
     y = torch.empty_like(b)

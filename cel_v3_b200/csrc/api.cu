@@ -181,6 +181,12 @@ static int build_offset_dict(celg_handle* h, celg_mat* m) {
   return CELG_OK;
 }
 
+int ensure_offset_dict(celg_handle* h, celg_mat* m) {
+  if (m->csr.ci8 || m->dict_tried) return CELG_OK;
+  m->dict_tried = true;
+  return build_offset_dict(h, m);
+}
+
 void free_mat_arrays(celg_mat* m) {
   cudaFree(m->csr.rp);
   cudaFree(m->csr.ci);
@@ -599,7 +605,7 @@ extern "C" int celg_mat_make_fp32(celg_mat* m) {
     CELG_CUDA(cudaMemsetAsync(m->csr.v32 + m->csr.nnz, 0, sizeof(float) * 32, m->h->stream));
   }
   int st = launch_to_f32(m->h, m->csr.nnz, m->csr.v, m->csr.v32);
-  if (!st && !m->csr.ci8) st = build_offset_dict(m->h, m);
+  if (!st) st = ensure_offset_dict(m->h, m);
   if (!st && m->jacobi) {
     if (!m->jacobi32) CELG_CUDA(cudaMalloc(&m->jacobi32, sizeof(float) * std::max(1, m->csr.n)));
     st = launch_to_f32(m->h, m->csr.n, m->jacobi, m->jacobi32);

@@ -25,8 +25,9 @@ struct CsrDev {
   double* v = nullptr;
   float* v32 = nullptr;   // FP32 copy (refinement inner solve), nnz+32
   int cap = 0;            // staged entries per 256-row sub-tile
-  // FP32 copy's column indices as 1-byte indices into a dictionary of
-  // column offsets (col - row), when the matrix has at most 256 of them
+  // column indices as 1-byte indices into a dictionary of column offsets
+  // (col - row), when the matrix has at most 256 of them (FP32 copy and
+  // the FP64 PCG sweeps)
   uint8_t* ci8 = nullptr; // nnz+32
   int* dict = nullptr;    // ndict offsets, ascending
   int ndict = 0;
@@ -112,6 +113,7 @@ struct celg_mat {
   float* jacobi32 = nullptr;  // n
   double* scale = nullptr;    // sqrt|d| when row-scaled, else null
   double* bjinv = nullptr;    // n x bj_bs inverse diagonal blocks (block Jacobi)
+  bool dict_tried = false;    // the offset dictionary was attempted (csr.ci8 set if it fits)
   int bj_bs = 0;
   bool scaled = false;
 };
@@ -164,6 +166,9 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 int ensure_f32(celg_handle* h, size_t n);
 // api.cu: matrix storage (alloc_csr leaves row_ptr/cols/vals for the caller
 // to fill; finish_csr shifts to 0-based, validates and sets the staging cap)
+// Build the 1-byte column offsets of the matrix once (no-op when built,
+// attempted before, or the matrix has more than 256 column offsets).
+int ensure_offset_dict(celg_handle* h, celg_mat* m);
 int alloc_csr(celg_mat* m, int n, int nnz, int ncols);
 int finish_csr(celg_handle* h, celg_mat* m, int base);
 void free_mat_arrays(celg_mat* m);

@@ -42,6 +42,9 @@ struct PcgBind {
   const double* bj = nullptr;
   int bs = 0;
   double* z = nullptr;
+  // FP64 CSR sweeps read the 1-byte column offsets (A->ci8) instead of the
+  // int32 columns: 9 instead of 12 bytes per non-zero
+  bool dict = false;
 };
 
 // blockjacobi.cu: the block-Jacobi forms of the set-up and of K2/K3
