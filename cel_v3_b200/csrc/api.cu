@@ -205,16 +205,20 @@ void free_mat_arrays(celg_mat* m) {
   cudaFree(m->bjinv);
 }
 
-// Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.
+// Allocate the padded CSR arrays; the caller fills rp[0..n], ci, v.  The
+// SpMV's bulk copies round a sub-tile's entry range out to 16-byte units of
+// the narrowest column array: up to 3 entries past nnz with int32 columns,
+// up to 15 with the 1-byte offsets, so ci and v carry 32 zeroed entries.
+constexpr int kCsrPad = 32;
 int alloc_csr(celg_mat* m, int n, int nnz, int ncols) {
   m->csr.n = n;
   m->csr.nnz = nnz;
   m->csr.ncols = ncols;
   CELG_CUDA(cudaMalloc(&m->csr.rp, sizeof(int) * ((size_t)n + 1 + 8)));
-  CELG_CUDA(cudaMalloc(&m->csr.ci, sizeof(int) * ((size_t)nnz + 8)));
-  CELG_CUDA(cudaMalloc(&m->csr.v, sizeof(double) * ((size_t)nnz + 8)));
-  CELG_CUDA(cudaMemsetAsync(m->csr.ci + nnz, 0, sizeof(int) * 8, m->h->stream));
-  CELG_CUDA(cudaMemsetAsync(m->csr.v + nnz, 0, sizeof(double) * 8, m->h->stream));
+  CELG_CUDA(cudaMalloc(&m->csr.ci, sizeof(int) * ((size_t)nnz + kCsrPad)));
+  CELG_CUDA(cudaMalloc(&m->csr.v, sizeof(double) * ((size_t)nnz + kCsrPad)));
+  CELG_CUDA(cudaMemsetAsync(m->csr.ci + nnz, 0, sizeof(int) * kCsrPad, m->h->stream));
+  CELG_CUDA(cudaMemsetAsync(m->csr.v + nnz, 0, sizeof(double) * kCsrPad, m->h->stream));
   return CELG_OK;
 }
 
