@@ -196,7 +196,23 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
       if (row < n) {
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
-        if (!fb) {
+        if (kDict && sizeof(VT) == 4 && !fb) {
+          // FP32 with 1-byte column offsets: the gathers address x from the
+          // row's base (one dictionary lookup and one add per entry), and the
+          // values are read from the stage when they are added (store-only
+          // sweep at 256^3: 151 -> 140 us; the FP64 sweep is slower this way,
+          // 251 -> 278 us, and keeps the loop below)
+          const VT* xr = x + row;
+          for (int k = b - a0, ke = e - a0; k < ke; k += 8) {
+            VT xv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (k + u < ke) xv[u] = __ldg(xr + s_dict[cis[k + u]]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (k + u < ke) sum = vadd(sum, vmul(vs[k + u], xv[u]));
+          }
+        } else if (!fb) {
           // chunks of 8 entries: all gathers of a chunk are issued before the
           // first add, so a row of up to 8 entries costs one memory round trip;
           // the adds stay in stored order
