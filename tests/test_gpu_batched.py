@@ -70,6 +70,10 @@ def test_batched_with_empty_system_and_cap(gpu):
                           [x.data_ptr() for x in xs] + [0], eps_rel=1e-12, iter_max=5)
     for s in range(3):
         assert infos[s].iter_done == 5 and infos[s].status == celgpu.ERR_NOCONV
+        # the capped systems' x equal single solves capped the same way
+        xs1 = dev(torch, np.zeros(bs[s].numel()))
+        h.pcg_jacobi(mats[s], bs[s].data_ptr(), xs1.data_ptr(), eps_rel=1e-12, iter_max=5)
+        assert torch.equal(xs[s], xs1)
     assert infos[3].iter_done == 0 and infos[3].status == celgpu.OK
     for m in mats + [empty]:
         m.destroy()

@@ -123,6 +123,26 @@ def test_every_spmm_variant_is_bitexact(gpu, cfg, monkeypatch):
     assert [i.iter_done for i in infos] == list(ito)
 
 
+@pytest.mark.parametrize("iter_max", [1, 6])
+def test_multirhs_iteration_cap_bitexact(gpu, iter_max):
+    """Columns stopped by the iteration cap still get the last x update
+    (which the direction sweep applies after the update sweep stopped
+    them): X equals the mirror bit for bit, columns of different speed
+    included."""
+    celgpu, h, torch = gpu
+    rp, ci, v = synth.poisson7(11, 10, 9)
+    n, k = rp.size - 1, 8
+    B = np.random.default_rng(17).uniform(-1.0, 1.0, (n, k))
+    B[:, 2] = 0.0                            # stops at once (alpha = 0)
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-12, iter_max=iter_max)
+    Xo, ito, _ = mirror(rp, ci, v, B, 1e-12, iter_max)
+    m.destroy()
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == list(ito)
+
+
 def mirror_ir(rp, ci, v, B, eps_rel, inner_eps, inner_max, outer_max):
     """FP64 refinement of every column around an FP32 multi-column PCG,
     composed from oracle pieces in the multi-column reduction order."""

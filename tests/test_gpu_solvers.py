@@ -358,3 +358,23 @@ def test_fp32_reliable_update_bitexact_and_accurate(gpu, name):
                           red=R.RED_TREE, iter_max=5000)
     assert it <= 1.25 * i64["iter_done"] + 5
     m.destroy()
+
+
+@pytest.mark.parametrize("iter_max", [1, 9])
+def test_fp32_reliable_update_iteration_cap_bitexact(gpu, iter_max):
+    """Stopped by the iteration cap (which forces a reliable update), the
+    correction d += sigma p left pending by the last step is still applied
+    before x is flushed: x equals the composed oracle bit for bit."""
+    celgpu, h, torch = gpu
+    rp, ci, v, b = PROBS["diffusion"]
+    n = rp.size - 1
+    m = setup(h, rp, ci, v)
+    xd = dev(torch, np.zeros(n))
+    info = h.pcg_jacobi(m, dev(torch, b).data_ptr(), xd.data_ptr(), history=True,
+                        precision=celgpu.PREC_FP32_RU, eps_rel=1e-10, inner_eps_rel=1e-2,
+                        iter_max=iter_max)
+    xo, ho, it, updates = ru_oracle(rp, ci, v, b, iter_max=iter_max)
+    assert info.iter_done == it == iter_max
+    assert np.array_equal(xd.cpu().numpy(), xo)
+    assert np.array_equal(info.history, ho)
+    m.destroy()
