@@ -54,7 +54,7 @@ struct Acc {
 };
 
 template <typename VT, class Epi, typename CT = int>
-__global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT) == 1 ? 3 : 2))
     csr_tma_kernel(const int* __restrict__ rp, const CT* __restrict__ ci,
                    const VT* __restrict__ v, int n, int cap, const VT* __restrict__ x, Epi epi,
                    RedCtx red, int* err, const int* __restrict__ dict, int ndict) {
