@@ -15,8 +15,9 @@
 // are reduced with the single-vector order (lane j sums j, j+256, ...,
 // butterfly, warps in order).
 //
-// Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 96 n k (SpMM 16 n k,
-// update sweep 32 n k, direction sweep 48 n k; J is n doubles, not counted).
+// Algorithmic bytes per iteration: 12 nnz + 4 (n+1) + 80 n k + 16 n (SpMM
+// 16 n k: P gathered, V stored; update sweep 24 n k + 8 n: R, V, J read, R
+// stored; direction sweep 40 n k + 8 n: P, R, X, J read, P, X stored).
 #include <algorithm>
 #include <cstdlib>
 #include <cmath>
@@ -1340,7 +1341,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     }
   }
   h->last_iters = iters;
-  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 96.0 * (double)nk;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 80.0 * (double)nk + 16.0 * n;
   return ret;
 }
 

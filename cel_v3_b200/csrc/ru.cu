@@ -405,7 +405,10 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   else if (s.s.err) ret = s.s.err;
   else if (!(s.norm64 <= s.s.eps)) ret = CELG_ERR_NOCONV;
   h->last_iters = s.s.iter;
-  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 48.0 * n;
+  // K1 (matrix, p gathered, v stored: 8 n), K2 (r, v, J read, r stored:
+  // 16 n), K3 (p, r, J, d read, p, d stored: 24 n); 5 bytes per non-zero
+  // with the 1-byte column offsets, else 8
+  h->last_bytes_per_iter = (m->csr.ci8 ? 5.0 : 8.0) * m->csr.nnz + 4.0 * (n + 1) + 48.0 * n;
   if (res) {
     res->iter_done = s.s.iter;
     res->final_norm2 = s.norm64;
