@@ -142,7 +142,7 @@ __global__ void offset_index_kernel(int n, const int* __restrict__ rp, const int
   }
 }
 
-// Build ci8/dict for the FP32 copy; leaves them unset when the matrix has
+// Build ci8/dict (1-byte column offsets col - row); leaves them unset when the matrix has
 // more than kDictMax distinct offsets.
 static int build_offset_dict(celg_handle* h, celg_mat* m) {
   CsrDev& A = m->csr;

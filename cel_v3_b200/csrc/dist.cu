@@ -258,6 +258,15 @@ static int dist_check(const celg_dist* d) {
   return CELG_OK;
 }
 
+// SpMV phase of the block: 1-byte column offsets when the block has them
+// (same values in the same order, so the same sums), else int32 columns.
+template <class Epi>
+static int dist_csr(celg_dist* d, const double* x, const Epi& epi) {
+  const CsrDev& A = d->m->csr;
+  if (A.ci8) return launch_csr_ct<double, uint8_t>(d->h, A, A.v, A.ci8, A.cap_dict, x, epi);
+  return launch_csr<double>(d->h, A, A.v, x, epi);
+}
+
 extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* p, void* state_d,
                                 double* hist_d, int hist_cap, celg_dist** out) {
   if (!h || !m || !p || !out || m->h != h || hist_cap < 0 || (hist_cap > 0 && !hist_d))
@@ -271,6 +280,9 @@ extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* 
   if (state_d && (reinterpret_cast<uintptr_t>(state_d) & 15)) return CELG_ERR_ARG;
   *out = nullptr;
   CELG_CUDA(cudaSetDevice(h->device));
+  // 1-byte column offsets for the block's SpMV phases when its columns (halo
+  // included) use at most 256 distinct offsets col - row
+  if (const int st = ensure_offset_dict(h, m)) return st;
   celg_dist* d = new celg_dist();
   d->h = h;
   d->m = m;
@@ -324,7 +336,7 @@ extern "C" int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double*
   CELG_CUDA(cudaSetDevice(d->h->device));
   const CsrDev& A = d->m->csr;
   DEpiInit epi{b_d, r_d, p_ext_d, d->m->jacobi, d->p.eps_abs, d->p.eps_rel, d->args()};
-  return launch_csr<double>(d->h, A, A.v, x_ext_d, epi);
+  return dist_csr(d, x_ext_d, epi);
 }
 
 extern "C" int celg_dist_pcg_start(celg_dist* d) {
@@ -339,7 +351,7 @@ extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
   const CsrDev& A = d->m->csr;
-  return launch_csr<double>(d->h, A, A.v, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
+  return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
 }
 
 extern "C" int celg_dist_pcg_update(celg_dist* d, double* x_ext_d, double* r_d,
@@ -361,7 +373,7 @@ extern "C" int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const doubl
   if (dist_check(d) || !b_d || !x_ext_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
   const CsrDev& A = d->m->csr;
-  return launch_csr<double>(d->h, A, A.v, x_ext_d, DEpiVerify{b_d, d->args()});
+  return dist_csr(d, x_ext_d, DEpiVerify{b_d, d->args()});
 }
 
 static int dist_fetch(celg_dist* d) {
