@@ -146,8 +146,8 @@ def _load():
         "celg_dist_pcg_init": (i, [vp, vp, vp, vp, vp]),
         "celg_dist_pcg_start": (i, [vp]),
         "celg_dist_pcg_ap": (i, [vp, vp, vp]),
-        "celg_dist_pcg_update": (i, [vp, vp, vp, vp, vp]),
-        "celg_dist_pcg_direction": (i, [vp, vp, vp]),
+        "celg_dist_pcg_update": (i, [vp, vp, vp]),
+        "celg_dist_pcg_direction": (i, [vp, vp, vp, vp]),
         "celg_dist_pcg_poll": (i, [vp, ip, ip]),
         "celg_dist_pcg_verify": (i, [vp, vp, vp]),
         "celg_dist_pcg_result": (i, [vp, ctypes.POINTER(Result)]),
@@ -253,11 +253,11 @@ class Dist:
     def ap(self, p_ext_d, v_d):
         self._call("celg_dist_pcg_ap", p_ext_d, v_d)
 
-    def update(self, x_ext_d, r_d, p_ext_d, v_d):
-        self._call("celg_dist_pcg_update", x_ext_d, r_d, p_ext_d, v_d)
+    def update(self, r_d, v_d):
+        self._call("celg_dist_pcg_update", r_d, v_d)
 
-    def direction(self, r_d, p_ext_d):
-        self._call("celg_dist_pcg_direction", r_d, p_ext_d)
+    def direction(self, x_ext_d, r_d, p_ext_d):
+        self._call("celg_dist_pcg_direction", x_ext_d, r_d, p_ext_d)
 
     def poll(self):
         a, it = ctypes.c_int(), ctypes.c_int()

@@ -142,14 +142,14 @@ struct DEpiAp {
   __device__ void finish(double* tot) const { xch_store(a.st, a, 0.0, 0.0, 0.0, tot[0]); }
 };
 
-// update (after the p.v reduction): sigma = alpha / p.v; x += sigma p;
-// r += (-sigma) v; local r.z and r.r with z = J r
+// update (after the p.v reduction): sigma = alpha / p.v;
+// r += (-sigma) v; local r.z and r.r with z = J r.  x += sigma p is left to
+// the direction phase, which reads p anyway: an update that ran (active, sigma
+// finite) always leaves the loop active, so a direction phase follows it.
 struct DOpUpdate {
   static constexpr int NRED = 2;
-  struct Regs { double x, r, p, v, J; };
-  double* x;
+  struct Regs { double r, v, J; };
   double* r;
-  const double* p;
   const double* v;
   const double* J;
   DistArgs a;
@@ -162,16 +162,14 @@ struct DOpUpdate {
     ok = isfinite(sg) && st->xch[X_ERR] == 0.0;
     return true;
   }
+  // v is not read again before the next update: streamed (evict-first)
   __device__ void load(long i, Regs& g) const {
-    g.x = x[i];
     g.r = r[i];
-    g.p = __ldg(p + i);
-    g.v = __ldg(v + i);
+    g.v = __ldcs(v + i);
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
     if (!ok) return;
-    x[i] = dadd(g.x, dmul(sg, g.p));
     const double ri = dadd(g.r, dmul(-sg, g.v));
     r[i] = ri;
     const double z = dmul(ri, g.J);
@@ -189,26 +187,37 @@ struct DOpUpdate {
   }
 };
 
-// direction (after the r.z / r.r reduction): beta = r.z / alpha;
-// p = beta p + J r; then alpha = r.z, ||r||, iteration count and the test
-// (by the last CTA, after every CTA has read the old alpha)
+// direction (after the r.z / r.r reduction): x += sigma p with the old p
+// (the update phase's step); beta = r.z / alpha; p = beta p + J r; then
+// alpha = r.z, ||r||, iteration count and the test (by the last CTA, after
+// every CTA has read the old alpha)
 struct DOpDirection {
   static constexpr int NRED = 0;
   static constexpr bool kFinishAlways = true;
-  struct Regs { double p, r, J; };
+  struct Regs { double p, r, J, x; };
   double* p;
   const double* r;
   const double* J;
+  double* x;
   DistArgs a;
-  double bt;
+  double bt, sg;
   __device__ bool prepare() {
     const DistState* st = a.st;
     if (*(volatile const int*)&st->active == 0) return false;
     bt = st->xch[X_RZ] / st->alpha;
+    sg = st->sigma;
     return true;
   }
-  __device__ void load(long i, Regs& g) const { g.p = p[i]; g.r = __ldg(r + i); g.J = __ldg(J + i); }
+  // r, J and x are streamed (evict-first), so that L2 keeps the new p for
+  // the next SpMV
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    g.r = __ldcs(r + i);
+    g.J = __ldcs(J + i);
+    g.x = __ldcs(x + i);
+  }
   __device__ void compute(long i, Regs& g, double*) const {
+    __stcs(x + i, dadd(g.x, dmul(sg, g.p)));
     p[i] = dadd(dmul(bt, g.p), dmul(g.r, g.J));
   }
   __device__ void finish(double*) const {
@@ -354,18 +363,18 @@ extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
 }
 
-extern "C" int celg_dist_pcg_update(celg_dist* d, double* x_ext_d, double* r_d,
-                                    const double* p_ext_d, const double* v_d) {
-  if (dist_check(d) || !x_ext_d || !r_d || !p_ext_d || !v_d) return CELG_ERR_ARG;
+extern "C" int celg_dist_pcg_update(celg_dist* d, double* r_d, const double* v_d) {
+  if (dist_check(d) || !r_d || !v_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  DOpUpdate op{x_ext_d, r_d, p_ext_d, v_d, d->m->jacobi, d->args(), 0.0, true};
+  DOpUpdate op{r_d, v_d, d->m->jacobi, d->args(), 0.0, true};
   return launch_tile(d->h, d->m->csr.n, op);
 }
 
-extern "C" int celg_dist_pcg_direction(celg_dist* d, const double* r_d, double* p_ext_d) {
-  if (dist_check(d) || !r_d || !p_ext_d) return CELG_ERR_ARG;
+extern "C" int celg_dist_pcg_direction(celg_dist* d, double* x_ext_d, const double* r_d,
+                                       double* p_ext_d) {
+  if (dist_check(d) || !x_ext_d || !r_d || !p_ext_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  DOpDirection op{p_ext_d, r_d, d->m->jacobi, d->args(), 0.0};
+  DOpDirection op{p_ext_d, r_d, d->m->jacobi, x_ext_d, d->args(), 0.0, 0.0};
   return launch_tile(d->h, d->m->csr.n, op);
 }
 

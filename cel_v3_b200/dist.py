@@ -195,10 +195,10 @@ class GpuRank:
         self.d.ap(self.p_ext.data_ptr(), self.v.data_ptr())
 
     def update(self):
-        self.d.update(self.x_ext.data_ptr(), self.r.data_ptr(), self.p_ext.data_ptr(), self.v.data_ptr())
+        self.d.update(self.r.data_ptr(), self.v.data_ptr())
 
     def direction(self):
-        self.d.direction(self.r.data_ptr(), self.p_ext.data_ptr())
+        self.d.direction(self.x_ext.data_ptr(), self.r.data_ptr(), self.p_ext.data_ptr())
 
     def poll(self):
         return self.d.poll()[0]

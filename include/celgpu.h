@@ -314,9 +314,9 @@ int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double* x_ext_d, d
                        double* p_ext_d);                                              /* [R] */
 int celg_dist_pcg_start(celg_dist* d);
 int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d);               /* [R] */
-int celg_dist_pcg_update(celg_dist* d, double* x_ext_d, double* r_d, const double* p_ext_d,
-                         const double* v_d);                                          /* [R] */
-int celg_dist_pcg_direction(celg_dist* d, const double* r_d, double* p_ext_d);
+int celg_dist_pcg_update(celg_dist* d, double* r_d, const double* v_d);               /* [R] */
+/* applies the preceding update's x += sigma p (old p), then p = beta p + J r */
+int celg_dist_pcg_direction(celg_dist* d, double* x_ext_d, const double* r_d, double* p_ext_d);
 /* synchronises the stream; active = 0 once the loop has ended */
 int celg_dist_pcg_poll(celg_dist* d, int* active, int* iter);
 int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const double* x_ext_d);      /* [R] */

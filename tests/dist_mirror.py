@@ -68,6 +68,7 @@ class CpuRank:
         else:
             xe[:n] = self.x0
         self.err, self.iter, self.active, self.alpha, self.norm = 0, 0, 1, 0.0, 0.0
+        self.sigma = 0.0
         self._store(tdot(self.b, self.b))
 
     def init(self):
@@ -106,9 +107,8 @@ class CpuRank:
         sg = self.alpha / float(self.xch[3])
         rz = rr = 0.0
         flagged = float(self.xch[4]) != 0.0
+        self.sigma = sg
         if np.isfinite(sg) and not flagged:
-            xe, pe = self._xe(), self._pe()
-            xe[:n] = xe[:n] + sg * pe[:n]
             self.r = self.r + (-sg) * self.v
             z = self.r * self.J
             rz, rr = tdot(self.r, z), tdot(self.r, self.r)
@@ -123,7 +123,8 @@ class CpuRank:
             return
         n = self.block.n
         bt = float(self.xch[1]) / self.alpha
-        pe = self._pe()
+        xe, pe = self._xe(), self._pe()
+        xe[:n] = xe[:n] + self.sigma * pe[:n]  # the update's step, old p
         pe[:n] = bt * pe[:n] + self.r * self.J
         self.alpha = float(self.xch[1])
         self.norm = float(np.sqrt(float(self.xch[2])))
