@@ -146,6 +146,9 @@ def _load():
         "celg_dist_pcg_init": (i, [vp, vp, vp, vp, vp]),
         "celg_dist_pcg_start": (i, [vp]),
         "celg_dist_pcg_ap": (i, [vp, vp, vp]),
+        "celg_dist_pcg_ap_interior": (i, [vp, vp, vp]),
+        "celg_dist_pcg_ap_boundary": (i, [vp, vp, vp]),
+        "celg_dist_interior_rows": (i, [vp, ip, ip]),
         "celg_dist_pcg_update": (i, [vp, vp, vp]),
         "celg_dist_pcg_direction": (i, [vp, vp, vp, vp]),
         "celg_dist_pcg_poll": (i, [vp, ip, ip]),
@@ -252,6 +255,19 @@ class Dist:
 
     def ap(self, p_ext_d, v_d):
         self._call("celg_dist_pcg_ap", p_ext_d, v_d)
+
+    def ap_interior(self, p_ext_d, v_d):
+        self._call("celg_dist_pcg_ap_interior", p_ext_d, v_d)
+
+    def ap_boundary(self, p_ext_d, v_d):
+        self._call("celg_dist_pcg_ap_boundary", p_ext_d, v_d)
+
+    def interior_rows(self):
+        """[lo, hi): the rows the interior half of the split SpMV covers."""
+        lo, hi = ctypes.c_int(), ctypes.c_int()
+        _check(lib.celg_dist_interior_rows(self.ptr, ctypes.byref(lo), ctypes.byref(hi)),
+               "celg_dist_interior_rows")
+        return lo.value, hi.value
 
     def update(self, r_d, v_d):
         self._call("celg_dist_pcg_update", r_d, v_d)

@@ -42,11 +42,26 @@ struct RedCtx {
   // tile is reduced on its own and the tile partials are combined in index
   // order.
   int sweep = 0;
+  // Tile window of a CSR sweep split in two launches (the rows that read no
+  // halo value, then the others): the launch visits nvisit tiles (-1: all),
+  // its k-th visited tile being k, plus win_shift once k reaches win_a.
+  // finish = false leaves the tile partials to the second launch, whose last
+  // CTA combines all ntiles of them in index order.
+  long nvisit = -1;
+  long win_a = 0x3fffffffffffffffL;
+  long win_shift = 0;
+  bool finish = true;
 };
 
 // Tile index of the k-th tile a sweep visits.
 __device__ __forceinline__ long tile_at(long k, long ntiles, int sweep) {
   return (sweep & 1) ? ntiles - 1 - k : k;
+}
+
+// Tile index of the k-th tile a windowed sweep visits (nvis tiles in all).
+__device__ __forceinline__ long tile_of(const RedCtx& red, long k, long nvis) {
+  const long t = tile_at(k, nvis, red.sweep);
+  return t >= red.win_a ? t + red.win_shift : t;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <vector>
 
 #include "pcg_internal.cuh"
 
@@ -233,6 +234,16 @@ struct DOpDirection {
   }
 };
 
+// Tiles whose rows read a halo column (a column index >= n): flags[t] = 1.
+__global__ void halo_tile_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 int* __restrict__ flags) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    bool halo = false;
+    for (int k = rp[i], e = rp[i + 1]; k < e; ++k) halo = halo || ci[k] >= n;
+    if (halo) flags[i / kTile] = 1;
+  }
+}
+
 // verify (after the halo of x): local ||b - A x||^2
 struct DEpiVerify {
   static constexpr int NRED = 1;
@@ -259,6 +270,10 @@ struct celg_dist {
   int hist_cap = 0;
   celg_params p{};
   DistState* host = nullptr;  // pinned mirror for poll/result
+  // interior tiles [win_lo, win_hi): the longest run of tiles that read no
+  // halo value; part: the tile partials of the split SpMV phase
+  long win_lo = 0, win_hi = 0;
+  double* part = nullptr;
   DistArgs args() const { return DistArgs{st, hist, hist_cap, p.iter_max, h->err_d}; }
 };
 
@@ -270,10 +285,43 @@ static int dist_check(const celg_dist* d) {
 // SpMV phase of the block: 1-byte column offsets when the block has them
 // (same values in the same order, so the same sums), else int32 columns.
 template <class Epi>
-static int dist_csr(celg_dist* d, const double* x, const Epi& epi) {
+static int dist_csr(celg_dist* d, const double* x, const Epi& epi, const TileWindow* win = nullptr) {
   const CsrDev& A = d->m->csr;
-  if (A.ci8) return launch_csr_ct<double, uint8_t>(d->h, A, A.v, A.ci8, A.cap_dict, x, epi);
-  return launch_csr<double>(d->h, A, A.v, x, epi);
+  if (A.ci8) return launch_csr_ct<double, uint8_t>(d->h, A, A.v, A.ci8, A.cap_dict, x, epi, win);
+  return launch_csr_ct<double, int>(d->h, A, A.v, A.ci, A.cap, x, epi, win);
+}
+
+// The interior window of the block and the partials of the split SpMV.
+static int dist_find_interior(celg_dist* d) {
+  celg_handle* h = d->h;
+  const CsrDev& A = d->m->csr;
+  const long nt = ntiles_of(A.n);
+  if (nt == 0) return CELG_OK;
+  CELG_CUDA(cudaMalloc(&d->part, sizeof(double) * (size_t)nt));
+  int* flags = nullptr;
+  CELG_CUDA(cudaMalloc(&flags, sizeof(int) * (size_t)nt));
+  std::vector<int> f((size_t)nt);
+  cudaError_t e = cudaMemsetAsync(flags, 0, sizeof(int) * (size_t)nt, h->stream);
+  if (e == cudaSuccess) {
+    const int grid = (int)std::max(1L, std::min(((long)A.n + 255) / 256, (long)h->sms * 16));
+    halo_tile_kernel<<<grid, 256, 0, h->stream>>>(A.n, A.rp, A.ci, flags);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f.data(), flags, sizeof(int) * (size_t)nt, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(flags);
+  if (e != cudaSuccess) return cuda_status(e, "celg_dist_create");
+  for (long t = 0; t < nt;) {
+    if (f[t]) { ++t; continue; }
+    long u = t;
+    while (u < nt && !f[u]) ++u;
+    if (u - t > d->win_hi - d->win_lo) {
+      d->win_lo = t;
+      d->win_hi = u;
+    }
+    t = u;
+  }
+  return CELG_OK;
 }
 
 extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* p, void* state_d,
@@ -313,6 +361,10 @@ extern "C" int celg_dist_create(celg_handle* h, celg_mat* m, const celg_params* 
     delete d;
     return cuda_status(e, "celg_dist_create");
   }
+  if (const int st = dist_find_interior(d)) {
+    celg_dist_destroy(d);
+    return st;
+  }
   *out = d;
   return CELG_OK;
 }
@@ -323,6 +375,7 @@ extern "C" int celg_dist_destroy(celg_dist* d) {
   cudaStreamSynchronize(d->h->stream);
   if (d->own_state) cudaFree(d->st);
   cudaFreeHost(d->host);
+  cudaFree(d->part);
   delete d;
   return CELG_OK;
 }
@@ -361,6 +414,28 @@ extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d
   CELG_CUDA(cudaSetDevice(d->h->device));
   const CsrDev& A = d->m->csr;
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
+}
+
+extern "C" int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, double* v_d) {
+  if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  const TileWindow w{d->win_lo, d->win_hi, true, d->part};
+  return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);
+}
+
+extern "C" int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d) {
+  if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
+  CELG_CUDA(cudaSetDevice(d->h->device));
+  const TileWindow w{d->win_lo, d->win_hi, false, d->part};
+  return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);
+}
+
+extern "C" int celg_dist_interior_rows(celg_dist* d, int* row_lo, int* row_hi) {
+  if (dist_check(d) || !row_lo || !row_hi) return CELG_ERR_ARG;
+  const long n = d->m->csr.n;
+  *row_lo = (int)std::min(n, d->win_lo * kTile);
+  *row_hi = (int)std::min(n, d->win_hi * kTile);
+  return CELG_OK;
 }
 
 extern "C" int celg_dist_pcg_update(celg_dist* d, double* r_d, const double* v_d) {

@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
 
   if (!epi.active()) return;
   const long nsub = ((long)n + kSub - 1) / kSub;
-  const long ntiles = ((long)n + kTile - 1) / kTile;
+  const long nvis = red.nvisit >= 0 ? red.nvisit : ((long)n + kTile - 1) / kTile;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -96,21 +96,21 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
     long k = blockIdx.x;
     int it = 0;
     int bnd = 0;  // lane q (0..4) holds rp at sub-tile boundary q of tile t
-    if (k < ntiles && lane <= kSubPerTile)
-      bnd = __ldg(rp + min(tile_at(k, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
+    if (k < nvis && lane <= kSubPerTile)
+      bnd = __ldg(rp + min(tile_of(red, k, nvis) * kTile + (long)lane * kSub, (long)n));
     TileInfo nxt{0, 0.0};
     if constexpr (kB) {
-      if (k < ntiles) nxt = epi.tile_info(tile_at(k, ntiles, sweep));
+      if (k < nvis) nxt = epi.tile_info(tile_of(red, k, nvis));
     }
-    for (; k < ntiles; k += gridDim.x) {
-      const long t = tile_at(k, ntiles, sweep);
+    for (; k < nvis; k += gridDim.x) {
+      const long t = tile_of(red, k, nvis);
       const int cur = bnd;
       const long kn = k + gridDim.x;
-      if (kn < ntiles && lane <= kSubPerTile)
-        bnd = __ldg(rp + min(tile_at(kn, ntiles, sweep) * kTile + (long)lane * kSub, (long)n));
+      if (kn < nvis && lane <= kSubPerTile)
+        bnd = __ldg(rp + min(tile_of(red, kn, nvis) * kTile + (long)lane * kSub, (long)n));
       if constexpr (kB) {
         const TileInfo ti = nxt;
-        if (kn < ntiles) nxt = epi.tile_info(tile_at(kn, ntiles, sweep));
+        if (kn < nvis) nxt = epi.tile_info(tile_of(red, kn, nvis));
         if (!ti.act) continue;
       }
       for (int q = 0; q < kSubPerTile; ++q) {
@@ -168,13 +168,13 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   Epi ep = epi;
   TileInfo nxt{0, 0.0};
   if constexpr (kB) {
-    if (blockIdx.x < ntiles) nxt = ep.tile_info(tile_at(blockIdx.x, ntiles, sweep));
+    if (blockIdx.x < nvis) nxt = ep.tile_info(tile_of(red, blockIdx.x, nvis));
   }
-  for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
-    const long t = tile_at(k, ntiles, sweep);
+  for (long k = blockIdx.x; k < nvis; k += gridDim.x) {
+    const long t = tile_of(red, k, nvis);
     if constexpr (kB) {
       const TileInfo ti = nxt;
-      if (k + gridDim.x < ntiles) nxt = ep.tile_info(tile_at(k + gridDim.x, ntiles, sweep));
+      if (k + gridDim.x < nvis) nxt = ep.tile_info(tile_of(red, k + gridDim.x, nvis));
       if (!ti.act) continue;
       ep.begin_tile(ti);
     }
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   }
   if constexpr (!kB && NR > 0) {
     double tot[NR > 0 ? NR : 1];
-    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);
+    if (red.finish && grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);
   }
 }
 

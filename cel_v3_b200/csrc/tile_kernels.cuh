@@ -135,12 +135,39 @@ int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
   return CELG_OK;
 }
 
+// One half of a CSR sweep split in two launches: the tiles [lo, hi)
+// (inside = true; their partials are left for the other half) or all tiles
+// but those (inside = false; its last CTA combines every tile's partials).
+// partials: NRED x ntiles doubles shared by the two halves.
+struct TileWindow {
+  long lo = 0, hi = 0;
+  bool inside = true;
+  double* partials = nullptr;
+};
+
 template <typename VT, typename CT, class Epi>
 int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* cols, int cap,
-                  const VT* x, const Epi& epi) {
+                  const VT* x, const Epi& epi, const TileWindow* win = nullptr) {
   const long nt = ntiles_of(A.n);
   RedCtx red{nullptr, h->ticket, nt};
-  if (Epi::NRED > 0) {
+  long nvis = nt;
+  if (win) {
+    const long len = win->hi - win->lo;
+    if (win->lo < 0 || len < 0 || win->hi > nt || (Epi::NRED > 0 && !win->partials)) return CELG_ERR_ARG;
+    if (win->inside) {
+      red.win_a = 0;
+      red.win_shift = win->lo;
+      nvis = len;
+      red.finish = false;
+    } else {
+      red.win_a = win->lo;
+      red.win_shift = len;
+      nvis = nt - len;
+    }
+    red.nvisit = nvis;
+    red.partials = win->partials;
+    if (win->inside && nvis == 0) return CELG_OK;
+  } else if (Epi::NRED > 0) {
     int st = ensure_partials(h, nt, Epi::NRED);
     if (st) return st;
     red.partials = h->partials;
@@ -153,7 +180,7 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
   per_sm = std::max(1, per_sm);
-  const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * per_sm));
+  const int grid = (int)std::max(1L, std::min(nvis, (long)h->sms * per_sm));
   kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, cols, vals, A.n, cap, x, epi, red, h->err_d,
                                                sizeof(CT) == 1 ? A.dict : nullptr,
                                                sizeof(CT) == 1 ? A.ndict : 0);

@@ -18,6 +18,12 @@ scalar per dot product (src/fop/cel_fop_vec_distr_module.f90:419-832).  Here:
   * `TorchComm` runs the exchanges with torch.distributed (NCCL for CUDA
     tensors, gloo for CPU tensors) -- point-to-point halo transfers and a sum
     all-reduce of the exchange buffer -- on torch's current stream;
+  * with `overlap=True`, the halo of p goes out on a side stream while the
+    SpMV of the rows that read no halo value runs, and the other rows follow
+    once it has arrived (cel_fop_mv_axy_distr,
+    src/fop/cel_fop_mv_module.f90:28-87, has the master thread exchange the
+    halo while the workers multiply the local block).  Same results either
+    way;
   * `GpuRank` is one rank's device side (libcelgpu.so phases); `run_pcg`
     sequences phases and exchanges for a list of ranks held by this process
     (one rank per process in a distributed run).
@@ -130,6 +136,12 @@ class TorchComm:
             for w in self.td.batch_isend_irecv(ops):
                 w.wait()
 
+    def halo_begin(self, vecs, blocks):
+        _side_begin(self, vecs, blocks)
+
+    def halo_end(self):
+        _side_end(self)
+
 
 class LocalComm:
     """All ranks in this process (one device or host): the all-reduce sums
@@ -150,6 +162,36 @@ class LocalComm:
                 src = blocks[q].send[r]
                 vecs[r][blk.n + off:blk.n + off + cnt] = vecs[q].index_select(
                     0, torch.as_tensor(src, device=vecs[q].device))
+
+    def halo_begin(self, vecs, blocks):
+        _side_begin(self, vecs, blocks)
+
+    def halo_end(self):
+        _side_end(self)
+
+
+def _side_begin(comm, vecs, blocks):
+    """Start comm.halo(vecs, blocks) on a side stream that first waits for
+    the work queued so far (CUDA tensors); CPU tensors exchange at once."""
+    import torch
+    comm._side_busy = False
+    if not vecs[0].is_cuda:
+        comm.halo(vecs, blocks)
+        return
+    if getattr(comm, "_side", None) is None:
+        comm._side = torch.cuda.Stream(device=vecs[0].device)
+    comm._side.wait_stream(torch.cuda.current_stream(vecs[0].device))
+    with torch.cuda.stream(comm._side):
+        comm.halo(vecs, blocks)
+    comm._side_busy = True
+
+
+def _side_end(comm):
+    """Make the current stream wait for the halo started by _side_begin."""
+    import torch
+    if getattr(comm, "_side_busy", False):
+        torch.cuda.current_stream(comm._side.device).wait_stream(comm._side)
+        comm._side_busy = False
 
 
 class GpuRank:
@@ -194,6 +236,15 @@ class GpuRank:
     def ap(self):
         self.d.ap(self.p_ext.data_ptr(), self.v.data_ptr())
 
+    def ap_interior(self):
+        self.d.ap_interior(self.p_ext.data_ptr(), self.v.data_ptr())
+
+    def ap_boundary(self):
+        self.d.ap_boundary(self.p_ext.data_ptr(), self.v.data_ptr())
+
+    def interior_rows(self):
+        return self.d.interior_rows()
+
     def update(self):
         self.d.update(self.r.data_ptr(), self.v.data_ptr())
 
@@ -217,12 +268,21 @@ class GpuRank:
         self.mat.destroy()
 
 
-def iterate(ranks, comm, count):
-    """`count` PCG iterations (each a no-op once the solve has stopped)."""
+def iterate(ranks, comm, count, overlap=False):
+    """`count` PCG iterations (each a no-op once the solve has stopped).
+    overlap: the halo of p travels while the interior rows' SpMV runs."""
     for _ in range(count):
-        comm.halo([r.p_ext for r in ranks], [r.block for r in ranks])
-        for r in ranks:
-            r.ap()
+        if overlap:
+            comm.halo_begin([r.p_ext for r in ranks], [r.block for r in ranks])
+            for r in ranks:
+                r.ap_interior()
+            comm.halo_end()
+            for r in ranks:
+                r.ap_boundary()
+        else:
+            comm.halo([r.p_ext for r in ranks], [r.block for r in ranks])
+            for r in ranks:
+                r.ap()
         comm.allreduce([r.xch for r in ranks])
         for r in ranks:
             r.update()
@@ -231,11 +291,11 @@ def iterate(ranks, comm, count):
             r.direction()
 
 
-def run_pcg(ranks, comm, check_every=8):
+def run_pcg(ranks, comm, check_every=8, overlap=False):
     """Distributed Jacobi-PCG over `ranks` (this process's ranks, each with
     the phase methods of GpuRank) with `comm` for the exchanges; polls the
-    stopping flag every `check_every` iterations.  Returns the ranks'
-    results."""
+    stopping flag every `check_every` iterations; overlap as in iterate.
+    Returns the ranks' results."""
     blocks = [r.block for r in ranks]
     for r in ranks:
         r.begin()
@@ -247,7 +307,7 @@ def run_pcg(ranks, comm, check_every=8):
     for r in ranks:
         r.start()
     while ranks[0].poll():
-        iterate(ranks, comm, check_every)
+        iterate(ranks, comm, check_every, overlap)
     comm.halo([r.x_ext for r in ranks], blocks)
     for r in ranks:
         r.verify()

@@ -314,6 +314,14 @@ int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double* x_ext_d, d
                        double* p_ext_d);                                              /* [R] */
 int celg_dist_pcg_start(celg_dist* d);
 int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d);               /* [R] */
+/* celg_dist_pcg_ap in two launches with the same results: the interior rows
+ * (the longest run of 1024-row tiles that read no halo column) need only the
+ * local part of p, so they may run while the halo of p is in flight; the
+ * boundary launch (after the halo) does the other rows and the p.v partial
+ * sums.  interior_rows gives that row range [row_lo, row_hi). */
+int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, double* v_d);
+int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d);
+int celg_dist_interior_rows(celg_dist* d, int* row_lo, int* row_hi);
 int celg_dist_pcg_update(celg_dist* d, double* r_d, const double* v_d);               /* [R] */
 /* applies the preceding update's x += sigma p (old p), then p = beta p + J r */
 int celg_dist_pcg_direction(celg_dist* d, double* x_ext_d, const double* r_d, double* p_ext_d);

@@ -100,6 +100,13 @@ class CpuRank:
         self.v = 0.0 + self._spmv(self._pe())
         self._store(0.0, 0.0, 0.0, tdot(self.v, self._pe()[:n]))
 
+    # the split SpMV phase: every row in the second half (same sums)
+    def ap_interior(self):
+        pass
+
+    def ap_boundary(self):
+        self.ap()
+
     def update(self):
         if not self.active:
             return

@@ -103,6 +103,21 @@ def test_mirror_ranks_converge_like_one(world):
     assert rw[0]["verified_relres"] <= 1e-8
 
 
+def test_mirror_split_spmv_phase_same_bits():
+    """The driver's overlapped sequence (halo_begin, interior half, halo_end,
+    boundary half) gives the bits of the plain sequence."""
+    rp, ci, v, b = poisson()
+    bounds = D.partition(rp.size - 1, 3, GRID[0] * GRID[1])
+    out = []
+    for overlap in (False, True):
+        ranks = [M.CpuRank(D.RowBlock(rp, ci, v, bounds, q), b[bounds[q]:bounds[q + 1]],
+                           eps_rel=1e-10, iter_max=500) for q in range(3)]
+        res = D.run_pcg(ranks, D.LocalComm(), check_every=3, overlap=overlap)
+        out.append((np.concatenate([r.x() for r in ranks]), res[0]["history"]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 def test_mirror_reference_start_and_iteration_cap():
     rp, ci, v, b = random_spd()
     x, res = run_mirror(rp, ci, v, b, 3, eps_rel=1e-14, iter_max=7, x0_mode=M.X0_ONES)
@@ -119,7 +134,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _gloo_worker(rank, world, port, out_dir):
+def _gloo_worker(rank, world, port, out_dir, overlap=False):
     import torch.distributed as td
     from datetime import timedelta
     td.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
@@ -129,20 +144,21 @@ def _gloo_worker(rank, world, port, out_dir):
         bounds = D.partition(rp.size - 1, world, GRID[0] * GRID[1])
         blk = D.RowBlock(rp, ci, v, bounds, rank)
         rk = M.CpuRank(blk, b[blk.r0:blk.r1], eps_rel=1e-10, iter_max=500)
-        (res,) = D.run_pcg([rk], D.TorchComm(), check_every=4)
+        (res,) = D.run_pcg([rk], D.TorchComm(), check_every=4, overlap=overlap)
         np.savez(os.path.join(out_dir, f"rank{rank}.npz"), x=rk.x(), iters=res["iter_done"],
                  hist=res["history"], vres=res["verified_relres"])
     finally:
         td.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_match_in_process_emulation(world, tmp_path):
+@pytest.mark.parametrize("world,overlap", [(2, False), (3, False), (2, True)])
+def test_gloo_ranks_match_in_process_emulation(world, overlap, tmp_path):
     """The exchanges over torch.distributed (gloo, one process per rank)
-    give the same bits as the in-process emulation."""
+    give the same bits as the in-process emulation, also with the SpMV
+    phase split around the halo exchange."""
     import torch.multiprocessing as mp
-    mp.start_processes(_gloo_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world,
-                       start_method="spawn", join=True)
+    mp.start_processes(_gloo_worker, args=(world, _free_port(), str(tmp_path), overlap),
+                       nprocs=world, start_method="spawn", join=True)
     parts = [np.load(tmp_path / f"rank{q}.npz") for q in range(world)]
     rp, ci, v, b = poisson()
     x_emul, res = run_mirror(rp, ci, v, b, world, align=GRID[0] * GRID[1], eps_rel=1e-10,

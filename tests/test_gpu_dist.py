@@ -37,10 +37,12 @@ def blocks_of(rp, ci, v, world, align):
     return [D.RowBlock(rp, ci, v, bounds, q) for q in range(world)]
 
 
-def run_gpu(h, blocks, b, comm=None, **kw):
+def run_gpu(h, blocks, b, comm=None, overlap=False, windows=None, **kw):
     ranks = [D.GpuRank(h, blk, b[blk.r0:blk.r1], history=True, **kw) for blk in blocks]
     try:
-        res = D.run_pcg(ranks, comm or D.LocalComm(), check_every=5)
+        if windows is not None:
+            windows.extend(r.interior_rows() for r in ranks)
+        res = D.run_pcg(ranks, comm or D.LocalComm(), check_every=5, overlap=overlap)
         x = np.concatenate([r.x().cpu().numpy() for r in ranks])
     finally:
         for r in ranks:
@@ -71,12 +73,13 @@ def test_one_rank_equals_single_system_solve(gpu):
     assert res.verified_relres == info.verified_relres
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("world", [2, 3, 4])
-def test_emulated_slab_ranks_match_cpu_mirror(gpu, world):
+def test_emulated_slab_ranks_match_cpu_mirror(gpu, world, overlap):
     celgpu, h, torch = gpu
     rp, ci, v, b = poisson()
     blocks = blocks_of(rp, ci, v, world, GRID[0] * GRID[1])
-    x, res = run_gpu(h, blocks, b, eps_rel=1e-8, iter_max=1000)
+    x, res = run_gpu(h, blocks, b, overlap=overlap, eps_rel=1e-8, iter_max=1000)
     xc, rc = run_cpu(blocks, b, eps_rel=1e-8, iter_max=1000)
     assert all(r.status == celgpu.OK for r in res)
     assert len({r.iter_done for r in res}) == 1
@@ -85,6 +88,31 @@ def test_emulated_slab_ranks_match_cpu_mirror(gpu, world):
     assert np.array_equal(x, xc)
     assert res[0].verified_relres == rc[0]["verified_relres"]
     assert res[0].verified_relres <= 1.5e-8
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_split_spmv_phase_interior_windows_and_bits(gpu, world):
+    """The SpMV phase in two launches around the halo (interior tiles while
+    the halo copies run on a side stream, then the rest): on z-slabs of
+    32x32x24 every 1024-row tile is one plane, the interior window leaves
+    out exactly the planes next to a neighbour, and the solve has the bits
+    of the one-launch phase and of the CPU mirror."""
+    celgpu, h, torch = gpu
+    rp, ci, v = synth.poisson7(32, 32, 24)
+    b = R.spmv_csr(rp, ci, v, np.random.default_rng(13).random(rp.size - 1))
+    blocks = blocks_of(rp, ci, v, world, 32 * 32)
+    win = []
+    x1, r1 = run_gpu(h, blocks, b, overlap=True, windows=win, eps_rel=1e-8, iter_max=1000)
+    x0, r0 = run_gpu(h, blocks, b, eps_rel=1e-8, iter_max=1000)
+    xc, rc = run_cpu(blocks, b, eps_rel=1e-8, iter_max=1000)
+    for q, (blk, (lo, hi)) in enumerate(zip(blocks, win)):
+        assert lo == (1024 if q > 0 else 0)
+        assert hi == blk.n - (1024 if q < world - 1 else 0)
+    assert all(r.status == celgpu.OK for r in r1)
+    assert r1[0].iter_done == r0[0].iter_done == rc[0]["iter_done"]
+    assert np.array_equal(r1[0].history, r0[0].history)
+    assert np.array_equal(x1, x0)
+    assert np.array_equal(x1, xc)
 
 
 def test_emulated_general_partition_user_start(gpu):
@@ -101,10 +129,18 @@ def test_emulated_general_partition_user_start(gpu):
     x = np.concatenate([r.x().cpu().numpy() for r in ranks])
     for r in ranks:
         r.close()
+    ranks = [D.GpuRank(h, blk, b[blk.r0:blk.r1], x0=x0[blk.r0:blk.r1], history=True, **kw)
+             for blk in blocks]
+    res_o = D.run_pcg(ranks, D.LocalComm(), check_every=4, overlap=True)
+    x_o = np.concatenate([r.x().cpu().numpy() for r in ranks])
+    for r in ranks:
+        r.close()
     xc, rc = run_cpu(blocks, b, x0=x0, **kw)
     assert all(r.status == celgpu.ERR_NOCONV and r.iter_done == 12 for r in res)
     assert np.array_equal(x, xc)
+    assert np.array_equal(x_o, xc)
     assert np.array_equal(res[0].history, rc[0]["history"])
+    assert np.array_equal(res_o[0].history, rc[0]["history"])
 
 
 def test_nccl_world_one(gpu):
