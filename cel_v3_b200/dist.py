@@ -99,7 +99,36 @@ class RowBlock:
         return sorted(set(self.send) | set(self.recv))
 
 
-class TorchComm:
+class _SideHalo:
+    """halo_begin / halo_end: the halo exchange of `halo` on a side stream
+    that first waits for the work queued so far (CUDA tensors), so that
+    kernels queued in between overlap it; CPU tensors exchange at once."""
+
+    _side = None
+    _side_busy = False
+
+    def halo_begin(self, vecs, blocks):
+        import torch
+        self._side_busy = False
+        if not vecs[0].is_cuda:
+            self.halo(vecs, blocks)
+            return
+        if self._side is None:
+            self._side = torch.cuda.Stream(device=vecs[0].device)
+        self._side.wait_stream(torch.cuda.current_stream(vecs[0].device))
+        with torch.cuda.stream(self._side):
+            self.halo(vecs, blocks)
+        self._side_busy = True
+
+    def halo_end(self):
+        """The current stream waits for the halo started by halo_begin."""
+        import torch
+        if self._side_busy:
+            torch.cuda.current_stream(self._side.device).wait_stream(self._side)
+            self._side_busy = False
+
+
+class TorchComm(_SideHalo):
     """Exchanges over torch.distributed for the single rank of this process:
     halo transfers with isend/irecv (lower rank's send first within each
     pair, as every rank walks its neighbours in ascending order) and a sum
@@ -136,14 +165,8 @@ class TorchComm:
             for w in self.td.batch_isend_irecv(ops):
                 w.wait()
 
-    def halo_begin(self, vecs, blocks):
-        _side_begin(self, vecs, blocks)
 
-    def halo_end(self):
-        _side_end(self)
-
-
-class LocalComm:
+class LocalComm(_SideHalo):
     """All ranks in this process (one device or host): the all-reduce sums
     the ranks' buffers in rank order, the halo copies between the ranks'
     vectors.  Used to run several ranks' kernels on one GPU in turn."""
@@ -162,36 +185,6 @@ class LocalComm:
                 src = blocks[q].send[r]
                 vecs[r][blk.n + off:blk.n + off + cnt] = vecs[q].index_select(
                     0, torch.as_tensor(src, device=vecs[q].device))
-
-    def halo_begin(self, vecs, blocks):
-        _side_begin(self, vecs, blocks)
-
-    def halo_end(self):
-        _side_end(self)
-
-
-def _side_begin(comm, vecs, blocks):
-    """Start comm.halo(vecs, blocks) on a side stream that first waits for
-    the work queued so far (CUDA tensors); CPU tensors exchange at once."""
-    import torch
-    comm._side_busy = False
-    if not vecs[0].is_cuda:
-        comm.halo(vecs, blocks)
-        return
-    if getattr(comm, "_side", None) is None:
-        comm._side = torch.cuda.Stream(device=vecs[0].device)
-    comm._side.wait_stream(torch.cuda.current_stream(vecs[0].device))
-    with torch.cuda.stream(comm._side):
-        comm.halo(vecs, blocks)
-    comm._side_busy = True
-
-
-def _side_end(comm):
-    """Make the current stream wait for the halo started by _side_begin."""
-    import torch
-    if getattr(comm, "_side_busy", False):
-        torch.cuda.current_stream(comm._side.device).wait_stream(comm._side)
-        comm._side_busy = False
 
 
 class GpuRank:
