@@ -214,8 +214,9 @@ def distributed_form(h, celgpu, torch, stream, rp, ci, v, b, reps=2):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         # the SpMV phase split around the halo (interior tiles, then the
-        # rest and the p.v sums): at world size 1 every tile is interior,
-        # so this measures the cost of the second launch
+        # rest and the p.v sums), as run_pcg(overlap=True) drives it: at
+        # world size 1 every tile is interior and the interior half is the
+        # whole one-launch phase
         e0.record(stream)
         for _ in range(reps):
             (res_s,) = D.run_pcg([rk], comm, check_every=8, overlap=True)

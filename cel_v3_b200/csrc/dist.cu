@@ -416,15 +416,23 @@ extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
 }
 
+// A block that reads no halo value (every tile interior) runs the whole
+// one-launch phase as its interior half and nothing as its boundary half.
+static bool dist_all_interior(const celg_dist* d) {
+  return d->win_lo == 0 && d->win_hi == ntiles_of(d->m->csr.n);
+}
+
 extern "C" int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, double* v_d) {
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
+  if (dist_all_interior(d)) return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
   const TileWindow w{d->win_lo, d->win_hi, true, d->part};
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);
 }
 
 extern "C" int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d) {
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
+  if (dist_all_interior(d)) return CELG_OK;
   CELG_CUDA(cudaSetDevice(d->h->device));
   const TileWindow w{d->win_lo, d->win_hi, false, d->part};
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);

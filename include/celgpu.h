@@ -318,7 +318,8 @@ int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d);         
  * (the longest run of 1024-row tiles that read no halo column) need only the
  * local part of p, so they may run while the halo of p is in flight; the
  * boundary launch (after the halo) does the other rows and the p.v partial
- * sums.  interior_rows gives that row range [row_lo, row_hi). */
+ * sums.  interior_rows gives that row range [row_lo, row_hi).  A block with
+ * no halo reads does all of ap in the interior half. */
 int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, double* v_d);
 int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d);
 int celg_dist_interior_rows(celg_dist* d, int* row_lo, int* row_hi);
