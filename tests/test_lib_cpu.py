@@ -55,3 +55,28 @@ def test_params_default_without_gpu(lib):
 def test_build_is_sm100a():
     from cel_v3_b200 import build
     assert "arch=compute_100a,code=sm_100a" in build.ARCH
+
+
+def test_null_arguments_return_status_without_gpu():
+    """Every entry point that takes a handle, matrix or solver object
+    returns a status for NULL arguments (ERR_ARG, or ERR_STATE for the
+    ELM-mirroring calls with no assembly in progress) before any CUDA call;
+    the destroy calls accept NULL as a no-op."""
+    from cel_v3_b200 import celgpu
+    scalar = (ctypes.c_int, ctypes.c_long, ctypes.c_size_t, ctypes.c_double, ctypes.c_float,
+              ctypes.c_int64)
+    no_status = {"celg_params_default", "celg_status_string"}
+    seen = 0
+    for name in declared_functions():
+        if name in no_status:
+            continue
+        f = getattr(celgpu.lib, name)
+        assert f.argtypes is not None, name  # every entry point has a ctypes signature
+        args = [t(0) if t in scalar else None for t in f.argtypes]
+        st = f(*args)
+        if name.endswith("_destroy"):
+            assert st == 0, name
+        else:
+            assert st in (1, 6), (name, st)
+        seen += 1
+    assert seen >= 60
