@@ -16,8 +16,9 @@
 // Exchange buffer: CELG_DIST_NEXCH doubles at the start of the state.  Every
 // phase that produces partial sums overwrites all of them (its own sums, 0
 // elsewhere; the last one is this rank's error flag), so the caller's rule is
-// uniform: after begin, init, ap, update and verify, sum-all-reduce the whole
-// buffer.  The scalars of the recurrence are computed from the reduced values
+// uniform: after begin, init, ap (or ap_boundary), update and verify,
+// sum-all-reduce the whole buffer.  ap_interior writes no exchange value: it
+// only runs the rows that read no halo value ahead of the halo's arrival.  The scalars of the recurrence are computed from the reduced values
 // identically on every rank, so every rank takes the same number of steps.
 #include <algorithm>
 #include <cmath>

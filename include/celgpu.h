@@ -293,6 +293,8 @@ int celg_diffusion7_face_grad(celg_handle* h, int nx, int ny, int nz, const doub
  *   begin [R]; halo(x); init [R]; start;
  *   repeat: halo(p); ap [R]; update [R]; direction;    (until poll says done)
  *   halo(x); verify [R]; result.
+ * With the halo of p overlapped: start halo(p) on another stream, then
+ * ap_interior; wait for the halo; ap_boundary [R] (in place of ap).
  * Iterations queued after convergence do no work (their exchanges still run,
  * identically on every rank).  Every rank reaches the same decisions because
  * they are taken from the reduced values only; a bounded-wait timeout on any
@@ -321,7 +323,7 @@ int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d);         
  * sums.  interior_rows gives that row range [row_lo, row_hi).  A block with
  * no halo reads does all of ap in the interior half. */
 int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, double* v_d);
-int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d);
+int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, double* v_d);      /* [R] */
 int celg_dist_interior_rows(celg_dist* d, int* row_lo, int* row_hi);
 int celg_dist_pcg_update(celg_dist* d, double* r_d, const double* v_d);               /* [R] */
 /* applies the preceding update's x += sigma p (old p), then p = beta p + J r */
