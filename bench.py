@@ -699,10 +699,9 @@ def run_gpu(args):
         "forms": forms,
         # one solve: 2 set-up sweeps, 3 per iteration and 1 verification; the
         # graph's loop body holds two iterations (an odd count ends with one
-        # body of 3 kernels that return at once); the distributed phases run
-        # 8 iterations between polls, plus a start kernel
-        "gpu_launches": args.steps * (3 + 3 * (iters + iters % 2) if world == 1 else
-                                      world * (4 + 3 * 8 * ((iters + 7) // 8))),
+        # body of 3 kernels that return at once); every rank runs its own
+        # replica of the solve, so the whole job launches world times that
+        "gpu_launches": world * args.steps * (3 + 3 * (iters + iters % 2)),
         "clocks": clk,
     }
     if cpu is not None:
