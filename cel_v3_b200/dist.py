@@ -98,6 +98,27 @@ class RowBlock:
     def neighbours(self):
         return sorted(set(self.send) | set(self.recv))
 
+    def interior_rows(self, tile=1024):
+        """[lo, hi): the longest run of `tile`-row tiles (the first of equal
+        runs) whose rows read no halo column -- the rows the interior half of
+        the split SpMV phase covers (celg_dist_interior_rows)."""
+        rows = np.repeat(np.arange(self.n), np.diff(self.rp))
+        nt = -(-self.n // tile)
+        halo = np.zeros(nt, dtype=bool)
+        halo[rows[self.ci >= self.n] // tile] = True
+        best, t = (0, 0), 0
+        while t < nt:
+            if halo[t]:
+                t += 1
+                continue
+            u = t
+            while u < nt and not halo[u]:
+                u += 1
+            if u - t > best[1] - best[0]:
+                best = (t, u)
+            t = u
+        return min(self.n, best[0] * tile), min(self.n, best[1] * tile)
+
 
 class _SideHalo:
     """halo_begin / halo_end: the halo exchange of `halo` on a side stream

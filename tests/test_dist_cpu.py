@@ -103,6 +103,39 @@ def test_mirror_ranks_converge_like_one(world):
     assert rw[0]["verified_relres"] <= 1e-8
 
 
+def test_interior_rows_of_slabs_and_general_blocks():
+    """The interior window: on z-slabs of 32x32x24 (one plane per 1024-row
+    tile) every plane but those next to a neighbour; on general blocks, a
+    run of tiles with no halo column that no other such run outgrows."""
+    rp, ci, v = synth.poisson7(32, 32, 24)
+    for world in (1, 2, 3):
+        bounds = D.partition(rp.size - 1, world, 32 * 32)
+        for q in range(world):
+            blk = D.RowBlock(rp, ci, v, bounds, q)
+            assert blk.interior_rows() == (1024 if q > 0 else 0,
+                                           blk.n - (1024 if q < world - 1 else 0))
+    # a banded unstructured matrix (columns within 100 of the row), cut at
+    # unaligned bounds: the halo reads sit near the block ends
+    rng = np.random.default_rng(5)
+    n = 5000
+    cols = [np.unique(np.clip(i + rng.integers(-100, 101, 6), 0, n - 1)) for i in range(n)]
+    rp = np.concatenate([[0], np.cumsum([c.size for c in cols])])
+    ci = np.concatenate(cols)
+    rp, ci, v = spd_from_pattern(rp, ci, rng.random(ci.size))
+    bounds = D.partition(n, 3)
+    for q in range(3):
+        blk = D.RowBlock(rp, ci, v, bounds, q)
+        lo, hi = blk.interior_rows(tile=64)
+        assert hi - lo >= 1024
+        assert lo % 64 == 0 and lo <= hi <= blk.n
+        assert (blk.ci[blk.rp[lo]:blk.rp[hi]] < blk.n).all()
+        # the run cannot grow: the tiles on either side read the halo
+        if lo >= 64:
+            assert (blk.ci[blk.rp[lo - 64]:blk.rp[lo]] >= blk.n).any()
+        if hi < blk.n:
+            assert (blk.ci[blk.rp[hi]:blk.rp[min(blk.n, hi + 64)]] >= blk.n).any()
+
+
 def test_mirror_split_spmv_phase_same_bits():
     """The driver's overlapped sequence (halo_begin, interior half, halo_end,
     boundary half) gives the bits of the plain sequence."""
