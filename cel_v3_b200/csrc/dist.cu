@@ -17,9 +17,14 @@
 // phase that produces partial sums overwrites all of them (its own sums, 0
 // elsewhere; the last one is this rank's error flag), so the caller's rule is
 // uniform: after begin, init, ap (or ap_boundary), update and verify,
-// sum-all-reduce the whole buffer.  ap_interior writes no exchange value: it
-// only runs the rows that read no halo value ahead of the halo's arrival.  The scalars of the recurrence are computed from the reduced values
-// identically on every rank, so every rank takes the same number of steps.
+// sum-all-reduce the whole buffer.  ap_interior runs the rows that read no
+// halo value ahead of the halo's arrival and writes no exchange value, except
+// for a block that reads no halo value at all: its ap_interior is the whole
+// one-launch ap phase (exchange values included) and ap_boundary does
+// nothing, so the caller's rule stays the same (all-reduce after
+// ap_boundary).  The scalars of the recurrence are computed from the reduced
+// values identically on every rank, so every rank takes the same number of
+// steps.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -427,7 +432,7 @@ extern "C" int celg_dist_pcg_ap_interior(celg_dist* d, const double* p_ext_d, do
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
   if (dist_all_interior(d)) return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
-  const TileWindow w{d->win_lo, d->win_hi, true, d->part};
+  const TileWindow w{d->win_lo, d->win_hi, true, d->part, ntiles_of(d->m->csr.n)};
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);
 }
 
@@ -435,7 +440,7 @@ extern "C" int celg_dist_pcg_ap_boundary(celg_dist* d, const double* p_ext_d, do
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
   if (dist_all_interior(d)) return CELG_OK;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  const TileWindow w{d->win_lo, d->win_hi, false, d->part};
+  const TileWindow w{d->win_lo, d->win_hi, false, d->part, ntiles_of(d->m->csr.n)};
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()}, &w);
 }
 

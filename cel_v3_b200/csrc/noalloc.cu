@@ -21,9 +21,13 @@
 //     different streams, or from different threads) race on it and their
 //     results are undefined.  Calls ordered on one stream are safe; the
 //     ticket is cleared by each call before its kernel starts.
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture.
+//   * each call outside a stream capture looks up the array's device
+//     address on the current device (cudaGetSymbolAddress, with that device
+//     current) and caches it; a call on a capturing stream uses the cached
+//     address, so make one call on the device before any stream capture.
+//     Looking the address up again on every uncaptured call keeps it valid
+//     across a cudaDeviceReset, which recreates the device's context and
+//     with it the array.
 #include <mutex>
 
 #include "tile_kernels.cuh"
@@ -42,12 +46,15 @@ std::mutex g_mutex;
 void* g_addr[kMaxDevices] = {};
 int g_sms[kMaxDevices] = {};
 
-// Device address of the scratch array on `dev` (looked up once per device,
-// with that device current).
-int scratch_for_device(int dev, void** addr, int* sms) {
+// Device address of the scratch array on `dev`, with that device current:
+// looked up again unless the stream is capturing (then the address cached by
+// an earlier call is used).
+int scratch_for_device(int dev, cudaStream_t stream, void** addr, int* sms) {
   if (dev < 0 || dev >= kMaxDevices) return CELG_ERR_ARG;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  CELG_CUDA(cudaStreamIsCapturing(stream, &cap));
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone || !g_addr[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) return celg::cuda_status(e, "cudaGetSymbolAddress(noalloc scratch)");
@@ -75,9 +82,9 @@ extern "C" int celg_dot_noalloc(int n, const double* a_d, const double* b_d, dou
   CELG_CUDA(cudaGetDevice(&dev));
   void* base = nullptr;
   int sms = 0;
-  int st = scratch_for_device(dev, &base, &sms);
-  if (st) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st = scratch_for_device(dev, s, &base, &sms);
+  if (st) return st;
   unsigned* ticket = static_cast<unsigned*>(base);
   double* partials = reinterpret_cast<double*>(static_cast<unsigned char*>(base) + kHeader);
   CELG_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));

@@ -138,11 +138,14 @@ int launch_tile(celg_handle* h, long n, const Op& op, int blocks_per_sm = 8) {
 // One half of a CSR sweep split in two launches: the tiles [lo, hi)
 // (inside = true; their partials are left for the other half) or all tiles
 // but those (inside = false; its last CTA combines every tile's partials).
-// partials: NRED x ntiles doubles shared by the two halves.
+// partials: NRED x ntiles doubles shared by the two halves; partials_cap is
+// the buffer's length in doubles (a launch whose epilogue needs more is
+// rejected with CELG_ERR_ARG).
 struct TileWindow {
   long lo = 0, hi = 0;
   bool inside = true;
   double* partials = nullptr;
+  long partials_cap = 0;
 };
 
 template <typename VT, typename CT, class Epi>
@@ -153,7 +156,9 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   long nvis = nt;
   if (win) {
     const long len = win->hi - win->lo;
-    if (win->lo < 0 || len < 0 || win->hi > nt || (Epi::NRED > 0 && !win->partials)) return CELG_ERR_ARG;
+    if (win->lo < 0 || len < 0 || win->hi > nt) return CELG_ERR_ARG;
+    if (Epi::NRED > 0 && (!win->partials || win->partials_cap < (long)Epi::NRED * nt))
+      return CELG_ERR_ARG;
     if (win->inside) {
       red.win_a = 0;
       red.win_shift = win->lo;

@@ -341,8 +341,10 @@ int celg_dist_pcg_result(celg_dist* d, celg_result* res);
  * keeps its reduction scratch in a fixed file-scope device array of the
  * library.  out_d[0] = a.b in the same order as celg_dot.  n may not exceed
  * CELG_NOALLOC_MAX_ROWS (CELG_ERR_ARG otherwise).  Calls share the array:
- * calls whose kernels overlap on the GPU race.  The first call on a device
- * resolves the array's address; make it before any stream capture.
+ * calls whose kernels overlap on the GPU race.  A call outside a stream
+ * capture looks the array's device address up again (so it stays valid
+ * across a cudaDeviceReset); a call on a capturing stream uses the address
+ * an earlier call found, so make one call on the device before capturing.
  * stream: a cudaStream_t of the current device, NULL for the default stream. */
 #define CELG_NOALLOC_MAX_ROWS 67108864
 int celg_dot_noalloc(int n, const double* a_d, const double* b_d, double* out_d, void* stream);

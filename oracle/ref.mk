@@ -2,7 +2,10 @@
 # they lie, into oracle/_ref/ref_poisson (test infrastructure: it produces
 # the known-answer Poisson fixtures under tests/golden/).  Nothing is copied
 # out of the reference tree.  Usage: make -f oracle/ref.mk REF=/path/to/cel_v3
-REF ?= /root/reference
+# (REF is the root of a hpcdkhab/cel_v3 checkout; it has no default)
+ifeq ($(strip $(REF)),)
+$(error REF is not set: make -f oracle/ref.mk REF=/path/to/cel_v3)
+endif
 OUT := $(dir $(lastword $(MAKEFILE_LIST)))_ref
 SRC := $(REF)/src/base
 REF_SOURCES := $(SRC)/cel_sparce_matrix_coo_interface.c $(SRC)/cel_discretisation.c \

@@ -47,7 +47,10 @@ def coo_to_csr(n, rows, cols, vals):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CEL_REFERENCE_DIR")
+    if not ref:
+        raise SystemExit("usage: make_golden.py REFERENCE_TREE (or set CEL_REFERENCE_DIR): "
+                         "the root of a hpcdkhab/cel_v3 checkout")
     subprocess.check_call(["make", "-s", "-f", os.path.join(REPO, "oracle", "ref.mk"), f"REF={ref}"])
     exe = os.path.join(REPO, "oracle", "_ref", "ref_poisson")
     for nx, ny, nz in GRIDS:

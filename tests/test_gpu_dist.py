@@ -143,6 +143,38 @@ def test_emulated_general_partition_user_start(gpu):
     assert np.array_equal(res_o[0].history, rc[0]["history"])
 
 
+def banded_spd(n=40000, half_width=300, seed=5):
+    """An unstructured banded SPD matrix: 6 random columns within
+    half_width of each row, symmetrised."""
+    rng = np.random.default_rng(seed)
+    cols = [np.unique(np.clip(i + rng.integers(-half_width, half_width + 1, 6), 0, n - 1))
+            for i in range(n)]
+    rp = np.concatenate([[0], np.cumsum([c.size for c in cols])])
+    rp, ci, v = spd_from_pattern(rp, np.concatenate(cols), rng.random(int(rp[-1])))
+    return rp, ci, v, rng.uniform(-1, 1, n)
+
+
+def test_interior_window_matches_host_restatement_on_unaligned_blocks(gpu):
+    """The library's interior window (celg_dist_interior_rows) equals the
+    host restatement (RowBlock.interior_rows: longest run of halo-free
+    1024-row tiles, the first of equal runs) on unaligned blocks of an
+    unstructured banded matrix, and the split SpMV phase over that window
+    keeps the bits of the CPU mirror."""
+    celgpu, h, torch = gpu
+    rp, ci, v, b = banded_spd()
+    blocks = blocks_of(rp, ci, v, 3, 1)
+    assert any(blk.r0 % 1024 for blk in blocks)            # bounds cut tiles
+    win = []
+    x1, r1 = run_gpu(h, blocks, b, overlap=True, windows=win, eps_rel=1e-8, iter_max=400)
+    for blk, w in zip(blocks, win):
+        assert tuple(w) == blk.interior_rows()
+        assert w[1] - w[0] >= 8 * 1024                    # halo reads only near the ends
+    xc, rc = run_cpu(blocks, b, eps_rel=1e-8, iter_max=400)
+    assert r1[0].iter_done == rc[0]["iter_done"]
+    assert np.array_equal(r1[0].history, rc[0]["history"])
+    assert np.array_equal(x1, xc)
+
+
 def test_nccl_world_one(gpu):
     """One rank over torch.distributed with NCCL: the collectives queue on
     torch's stream between the phases; same bits as the single solve."""
