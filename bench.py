@@ -20,7 +20,11 @@ Also reported on the same line:
                 batched uneven systems, 32 right-hand sides on 128^3, and the
                 adjoint gradients of a batch of 8 128^3 diffusion solves
   cpu_baseline  the C restatement of the reference's MPI+OpenMP PCG (oracle/)
-                on the host cores, on a bounded sample of iterations
+                on the host cores: one complete solve of the same system
+  summary       last on the line: one number per form, and the parity of the
+                headline solve against that oracle solve (b = A x_true and the
+                JAD permutation bit for bit; residual history and solution
+                within 1e-10 relative, iterations +-1)
 
 --impl reference times that CPU restatement alone (the Fortran reference
 cannot be built here: no Fortran compiler or MPI), each step a bounded sample
@@ -128,6 +132,11 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
+def rel_err(x, ref):
+    """max |x - ref| / max |ref| of two device vectors."""
+    return float((x - ref).abs().max() / ref.abs().max())
+
+
 def build_problem():
     from cel_v3_b200 import synth
     rp, ci, v, x_true = synth.plain(SIDE, SEED)
@@ -158,7 +167,9 @@ def plain_large_form(h, celgpu, torch, stream, m, b, x, iters_csr):
         rp, ci, v = synth.poisson7(side)
         n, nnz = rp.size - 1, int(rp[-1])
         mm = m if side == 256 else h.matrix_from_csr(rp, ci, v)
-        mm.to_jad()
+        perm = mm.to_jad()
+        if side == 256:
+            out["jad_perm"] = perm
         xs = torch.from_numpy(np.random.default_rng(1).random(n)).cuda()
         ys = torch.zeros(n, dtype=torch.float64, device="cuda")
         row = {}
@@ -249,6 +260,7 @@ def precision_form(h, celgpu, torch, stream, side=256, reps=2):
     x = torch.zeros_like(b)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"rows": n, "nnz": nnz, "rel_res": 1e-10}
+    x64 = None
     for name, kw in (("fp64_pcg", dict()),
                      ("fp32_ir", dict(precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4)),
                      ("fp32_ru", dict(precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2))):
@@ -264,6 +276,10 @@ def precision_form(h, celgpu, torch, stream, side=256, reps=2):
         out[name] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
                      "inner_iters": inf.arnoldi_steps, "verified_relres": inf.verified_relres,
                      "status": inf.status}
+        if x64 is None:
+            x64 = x.clone()
+        else:
+            out[name]["err_vs_fp64"] = rel_err(x, x64)
     base = out["fp64_pcg"]["solves_per_s"]
     for k in ("fp32_ir", "fp32_ru"):
         out[k]["speedup_vs_fp64"] = out[k]["solves_per_s"] / base
@@ -281,7 +297,10 @@ def precision_form(h, celgpu, torch, stream, side=256, reps=2):
     fms = e0.elapsed_time(e1) / reps
     out["fp64_pcg_block_jacobi8"] = {"solves_per_s": 1e3 / fms, "ms": fms, "iters": inf.iter_done,
                                      "verified_relres": inf.verified_relres, "status": inf.status,
-                                     "speedup_vs_fp64": 1e3 / fms / base}
+                                     "speedup_vs_fp64": 1e3 / fms / base,
+                                     "err_vs_fp64": rel_err(x, x64)}
+    out["err_vs_fp64"] = ("max |x - x_fp64| / max |x_fp64|, x_fp64 = the plain FP64 PCG "
+                          "solution of the same system (rel-res 1e-10)")
     m.destroy()
     return out
 
@@ -312,6 +331,7 @@ def batch_form(h, celgpu, torch, stream):
         return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p32)
 
     out = {}
+    x64 = None
     for name, fn in (("one_by_one", one_by_one), ("batched", batched),
                      ("batched_fp32_ir", batched_fp32_ir)):
         fn()
@@ -328,6 +348,10 @@ def batch_form(h, celgpu, torch, stream):
                      "sum_iters": sum(i.iter_done for i in infos),
                      "worst_verified_relres": max(i.verified_relres for i in infos),
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
+        if name == "batched":
+            x64 = [x.clone() for x in xs]
+        elif name == "batched_fp32_ir":
+            out[name]["worst_err_vs_fp64"] = max(rel_err(x, y) for x, y in zip(xs, x64))
     out["speedup_batched_vs_one_by_one"] = out["batched"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_batched_fp32_ir_vs_one_by_one"] = (out["batched_fp32_ir"]["solves_per_s"] /
                                                     out["one_by_one"]["solves_per_s"])
@@ -371,6 +395,10 @@ def multirhs_form(h, celgpu, torch, stream):
                      "max_iters": max(i.iter_done for i in infos),
                      "worst_verified_relres": max(i.verified_relres for i in infos),
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
+        if name == "multirhs":
+            X64 = Xd.clone()
+        elif name == "multirhs_fp32_ir":
+            out[name]["worst_err_vs_fp64"] = max(rel_err(Xd[:, c], X64[:, c]) for c in range(k))
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_multirhs_fp32_ir_vs_one_by_one"] = (out["multirhs_fp32_ir"]["solves_per_s"] /
                                                      out["one_by_one"]["solves_per_s"])
@@ -469,35 +497,93 @@ def differentiation_form(h, celgpu, torch, stream, side=128, batch=8, fd_dirs=64
                          "scale": "max(|fd|, max|dL/dg|)"}}
 
 
-def cpu_sample(rp, ci, v, b, iters_per_solve, target_s=12.0, red_seq=True):
-    """Time the oracle's reference-order PCG on the host cores for a bounded
-    number of iterations and scale to solves/s."""
+def forms_summary(forms, value):
+    """One number per form: each speed-up against its plain FP64 GPU
+    counterpart, the FP32 forms' errors against the FP64 solutions."""
+    def g(*keys):
+        d = forms
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return float(f"{d:.4g}") if isinstance(d, float) else d
+
+    out = {
+        "fp32_ru_x": g("precision_diffusion256", "fp32_ru", "speedup_vs_fp64"),
+        "fp32_ir_x": g("precision_diffusion256", "fp32_ir", "speedup_vs_fp64"),
+        "fp32_ru_err": g("precision_diffusion256", "fp32_ru", "err_vs_fp64"),
+        "fp32_ir_err": g("precision_diffusion256", "fp32_ir", "err_vs_fp64"),
+        "fp64_diffusion_solves_s": g("precision_diffusion256", "fp64_pcg", "solves_per_s"),
+        "batched_x": g("batched_64", "speedup_batched_vs_one_by_one"),
+        "batched_fp32_ir_x": g("batched_64", "speedup_batched_fp32_ir_vs_one_by_one"),
+        "multirhs_x": g("multirhs_128_k32", "speedup_multirhs_vs_one_by_one"),
+        "multirhs_fp32_ir_x": g("multirhs_128_k32", "speedup_multirhs_fp32_ir_vs_one_by_one"),
+        "grad_per_s": g("differentiation_128_b8", "gradients_per_s"),
+        "grad_fd_err": g("differentiation_128_b8", "fd_check", "max_rel_err_dLdg"),
+        "jad_pcg_solves_s": g("plain_large_256", "pcg_jad_256", "solves_per_s"),
+        "gmres30_solves_s": g("plain_large_256", "gmres30_csr_256", "solves_per_s"),
+        "spmv256_csr_frac": g("plain_large_256", "spmv_sweep", "256^3", "csr", "frac_of_measured"),
+        "spmv256_jad_frac": g("plain_large_256", "spmv_sweep", "256^3", "jad", "frac_of_measured"),
+    }
+    dist = g("distributed_phases_256", "solves_per_s")
+    if dist is not None:
+        out["dist_world1_x"] = float(f"{dist / value:.4g}")
+    return {k: v for k, v in out.items() if v is not None}
+
+
+def cpu_baseline_and_parity(h, celgpu, torch, m, rp, ci, v, x_true, b, p, perm_gpu):
+    """The CPU baseline and the parity of the headline solve.
+
+    Baseline: one complete solve of the oracle's reference-order Jacobi-PCG
+    (the C restatement of cel_cgalg_jacobi with the reference's thread model:
+    an idle master plus one OpenMP worker per other host core), timed on the
+    host cores; plus a bounded sample with one worker.
+
+    Parity, against that same oracle solve and the oracle's row sums: the
+    GPU's b = A x_true bit for bit, the JAD permutation bit for bit, and the
+    GPU solve's residual history and solution within 1e-10 relative at the
+    same iteration count +-1."""
     from oracle import celref as R
     cores = os.cpu_count() or 1
-    workers = max(1, cores - 1)  # reference thread model: 1 idle master + workers
+    workers = max(1, cores - 1)
+    n = rp.size - 1
+    b_ref = R.spmv_csr(rp, ci, v, x_true, nworkers=workers)
+    b_host = b.cpu().numpy()
+    perm_ref, _ = R.jad_perm(rp)
+    if perm_gpu is None:
+        perm_gpu = m.to_jad()
+    xg = torch.zeros(n, dtype=torch.float64, device="cuda")
+    info = h.pcg_jacobi(m, b.data_ptr(), xg.data_ptr(), p, history=True)
+    x_gpu = xg.cpu().numpy()
     A = R.Matrix(rp, ci, v)
     J = R.jacobi(R.diag(rp, ci, v))
-    red = R.RED_SEQ if red_seq else R.RED_TREE
     t0 = time.perf_counter()
-    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=2, red=red, nworkers=workers)
-    probe = time.perf_counter() - t0
-    k = max(3, min(400, int(target_s / max(probe / 2.0, 1e-3))))
+    xs, io = R.pcg_jacobi(A, J, b_ref, eps_rel=EPS_REL, iter_max=5000, red=R.RED_SEQ,
+                          nworkers=workers)
+    t_full = time.perf_counter() - t0
     t0 = time.perf_counter()
-    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=k, red=red, nworkers=workers)
-    t = time.perf_counter() - t0
-    per_iter = t / (k + 1)  # set-up sweep ~ one iteration
-    # the deterministic one-worker setting (the oracle's sequential order)
-    t0 = time.perf_counter()
-    R.pcg_jacobi(A, J, b, eps_rel=0.0, eps_abs=0.0, iter_max=4, red=red, nworkers=1)
+    R.pcg_jacobi(A, J, b_ref, eps_rel=0.0, eps_abs=0.0, iter_max=4, red=R.RED_SEQ, nworkers=1)
     t1 = time.perf_counter() - t0
-    return {"value": 1.0 / (per_iter * iters_per_solve), "unit": UNIT, "cores": cores,
-            "threads": workers + 1, "kind": "port",
-            "sample": f"oracle Jacobi-PCG (reference order, {workers} workers + idle master) on the "
-                      f"256^3 system: {k} iterations in {t:.2f} s, scaled by {iters_per_solve} "
-                      f"iterations per solve",
-            "one_worker": {"value": 1.0 / (t1 / 5 * iters_per_solve), "unit": UNIT, "threads": 1,
-                           "sample": f"4 iterations + set-up in {t1:.2f} s, scaled by "
-                                     f"{iters_per_solve} iterations per solve"}}
+    k = min(len(io["history"]), len(info.history))
+    hist_rel = float(np.max(np.abs(info.history[:k] - io["history"][:k]) / io["history"][:k]))
+    x_rel = float(np.abs(x_gpu - xs).max() / np.abs(xs).max())
+    parity = {"spmv_256_bitexact": bool(np.array_equal(b_host, b_ref)),
+              "jad_perm_256_bitexact": bool(np.array_equal(perm_gpu, perm_ref)),
+              "iters_gpu": info.iter_done, "iters_ref": io["iter_done"],
+              "pcg_256_hist_max_rel": hist_rel, "pcg_256_x_max_rel": x_rel,
+              "pass": bool(np.array_equal(b_host, b_ref) and np.array_equal(perm_gpu, perm_ref)
+                           and abs(info.iter_done - io["iter_done"]) <= 1 and hist_rel < 1e-10
+                           and x_rel < 1e-10),
+              "ref": f"oracle reference order, {workers} workers"}
+    cpu = {"value": 1.0 / t_full, "unit": UNIT, "cores": cores, "threads": workers + 1,
+           "kind": "port",
+           "sample": f"one complete oracle Jacobi-PCG solve (reference order, {workers} workers + "
+                     f"idle master) of the 256^3 system: {io['iter_done']} iterations in "
+                     f"{t_full:.2f} s",
+           "one_worker": {"value": 1.0 / (t1 / 5 * io["iter_done"]), "unit": UNIT, "threads": 1,
+                          "sample": f"4 iterations + set-up in {t1:.2f} s, scaled by "
+                                    f"{io['iter_done']} iterations per solve"}}
+    return cpu, parity
 
 
 def run_reference(args):
@@ -670,9 +756,11 @@ def run_gpu(args):
     h.elm_destroy()
     assert ierr == 0, ierr
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_sample(rp, ci, v, b.cpu().numpy(), iters)
+        perm_gpu = forms.get("plain_large_256", {}).pop("jad_perm", None)
+        cpu, parity = cpu_baseline_and_parity(h, celgpu, torch, m, rp, ci, v, x_true, b, p,
+                                              perm_gpu)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -706,6 +794,8 @@ def run_gpu(args):
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    # last on the line, so that a reader of only its tail sees them
+    line["summary"] = {"forms": forms_summary(forms, value), "parity": parity}
     if rank == 0:
         print(json.dumps(line), flush=True)
     m.destroy()
