@@ -32,7 +32,9 @@ of iterations of the same solve, scaled to solves/s.
 
 Multi-GPU (torchrun, N > 1): every rank solves its own copy of the system
 (independent replicas, no collective on the data path); value = all ranks'
-solves / max-over-ranks time.
+solves / max-over-ranks time.  Reported beside it (forms.distributed_256):
+the row-block solve of one 256^3 system over all N GPUs (z-slabs, halo and
+all-reduces over NCCL inside the library call), max-over-ranks time.
 """
 import argparse
 import json
@@ -195,54 +197,41 @@ def plain_large_form(h, celgpu, torch, stream, m, b, x, iters_csr):
     return out
 
 
-def distributed_form(h, celgpu, torch, stream, rp, ci, v, b, reps=2):
-    """The distributed PCG (celg_dist_* phases driven by cel_v3_b200.dist over
-    torch.distributed / NCCL) at world size 1 on the 256^3 system: the cost
-    of the phase API and its exchanges against the single-graph solve."""
-    import socket
-    import torch.distributed as td
+def distributed_form(h, celgpu, torch, stream, rp, ci, v, b_host, rank, world, local,
+                     max_over_ranks, barrier, reps=2):
+    """The row-block Jacobi-PCG of one 256^3 system over all ranks: z-slabs,
+    one per GPU (strong scaling), each rank's whole solve one library call
+    (celg_dist_pcg_solve_nccl: per iteration the halo of p and two
+    all-reduces of 5 doubles over the library's own NCCL communicator).  At
+    world size 1 it is the cost of that path against the single-graph solve.
+    Also timed with the halo of p overlapped with the interior rows' SpMV."""
     from cel_v3_b200 import dist as D
-    own = not td.is_initialized()
-    if own:
-        with socket.socket() as s:
-            s.bind(("127.0.0.1", 0))
-            port = s.getsockname()[1]
-        import datetime
-        td.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
-                              timeout=datetime.timedelta(seconds=120))
+    n = rp.size - 1
+    blk = D.RowBlock(rp, ci, v, D.partition(n, world, SIDE * SIDE), rank)
+    rk = D.GpuRank(h, blk, b_host[blk.r0:blk.r1], eps_rel=EPS_REL, iter_max=5000)
+    comm = D.nccl_communicator(rank, world, local)
+    out = {"world": world, "rows_per_rank": blk.n, "scaling": "strong", "poll_every": 8,
+           "api": "celg_dist_pcg_solve_nccl"}
     try:
-        n = rp.size - 1
-        blk = D.RowBlock(rp, ci, v, [0, n], 0)
-        rk = D.GpuRank(h, blk, b.cpu().numpy(), eps_rel=EPS_REL, iter_max=5000)
-        comm = D.TorchComm()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        D.run_pcg([rk], comm, check_every=8)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(reps):
-            (res,) = D.run_pcg([rk], comm, check_every=8)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        # the SpMV phase split around the halo (interior tiles, then the
-        # rest and the p.v sums), as run_pcg(overlap=True) drives it: at
-        # world size 1 every tile is interior and the interior half is the
-        # whole one-launch phase
-        e0.record(stream)
-        for _ in range(reps):
-            (res_s,) = D.run_pcg([rk], comm, check_every=8, overlap=True)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms_s = e0.elapsed_time(e1) / reps
-        rk.close()
-        assert res_s.iter_done == res.iter_done and res_s.verified_relres == res.verified_relres
-        return {"world": 1, "solves_per_s": 1e3 / ms, "ms": ms, "iters": res.iter_done,
-                "verified_relres": res.verified_relres, "status": res.status,
-                "exchanges_per_iteration": "1 halo (empty at world 1) + 2 all-reduces of 5 doubles",
-                "poll_every": 8, "split_spmv_solves_per_s": 1e3 / ms_s}
+        for overlap in (False, True):
+            rk.solve_nccl(comm, poll_every=8, overlap=overlap)
+            barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(reps):
+                res = rk.solve_nccl(comm, poll_every=8, overlap=overlap)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = max_over_ranks(e0.elapsed_time(e1) / reps)
+            key = "overlap" if overlap else "plain"
+            out[key] = {"solves_per_s": 1e3 / ms, "ms": ms, "iters": res.iter_done,
+                        "verified_relres": res.verified_relres, "status": res.status}
+        out["solves_per_s"] = max(out["plain"]["solves_per_s"], out["overlap"]["solves_per_s"])
     finally:
-        if own:
-            td.destroy_process_group()
+        rk.close()
+        celgpu.nccl_comm_destroy(comm)
+    return out
 
 
 def precision_form(h, celgpu, torch, stream, side=256, reps=2):
@@ -525,9 +514,12 @@ def forms_summary(forms, value):
         "spmv256_csr_frac": g("plain_large_256", "spmv_sweep", "256^3", "csr", "frac_of_measured"),
         "spmv256_jad_frac": g("plain_large_256", "spmv_sweep", "256^3", "jad", "frac_of_measured"),
     }
-    dist = g("distributed_phases_256", "solves_per_s")
+    dist = g("distributed_world1_256", "solves_per_s")
     if dist is not None:
         out["dist_world1_x"] = float(f"{dist / value:.4g}")
+    dist = g("distributed_256", "solves_per_s")
+    if dist is not None:
+        out["dist_solves_s"] = dist
     return {k: v for k, v in out.items() if v is not None}
 
 
@@ -728,8 +720,13 @@ def run_gpu(args):
         forms["batched_64"] = batch_form(h, celgpu, torch, stream)
         forms["multirhs_128_k32"] = multirhs_form(h, celgpu, torch, stream)
         forms["differentiation_128_b8"] = differentiation_form(h, celgpu, torch, stream)
-        forms["distributed_phases_256"] = distributed_form(h, celgpu, torch, stream, rp, ci, v, b)
         forms["plain_large_256"] = plain_large_form(h, celgpu, torch, stream, m, b, x, iters)
+
+    # ---- the distributed row-block solve of the same system over all ranks ----
+    if not args.quick:
+        dist_key = "distributed_256" if world > 1 else "distributed_world1_256"
+        forms[dist_key] = distributed_form(h, celgpu, torch, stream, rp, ci, v, b.cpu().numpy(),
+                                           rank, world, local, max_over_ranks, barrier)
 
     # ---- e2e through the ELM interface with host buffers ----
     h.elm_init(n, n, 1, (7, 0))

@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
          "-I", INCLUDE, "--expt-relaxed-constexpr"]
 SOURCES = ["api.cu", "spmv.cu", "blas1.cu", "pcg.cu", "krylov.cu", "ir.cu", "ru.cu", "elm.cu", "noalloc.cu",
-           "batched.cu", "selftest.cu", "multirhs.cu", "adjoint.cu", "dist.cu", "assemble.cu",
+           "batched.cu", "selftest.cu", "multirhs.cu", "adjoint.cu", "dist.cu", "dist_solve.cu", "assemble.cu",
            "blockjacobi.cu"]
 
 
@@ -71,7 +71,7 @@ def build(verbose=False, ptxas_info=False):
     if failed:
         raise RuntimeError("nvcc failed for: " + ", ".join(failed))
     if _newer(LIB, objs) or jobs:
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)

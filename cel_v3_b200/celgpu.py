@@ -36,6 +36,7 @@ ERR_BREAKDOWN = 3
 ERR_NOCONV = 4
 ERR_TIMEOUT = 5
 ERR_STATE = 6
+ERR_COMM = 7
 
 FMT_CSR = 0
 FMT_JAD = 1
@@ -76,6 +77,16 @@ class Result(ctypes.Structure):
         ("arnoldi_steps", ctypes.c_int), ("history", ctypes.POINTER(ctypes.c_double)),
         ("history_cap", ctypes.c_int), ("history_len", ctypes.c_int),
     ]
+
+
+# celg_dist_comm: the caller's exchange callbacks of celg_dist_pcg_solve
+ALLREDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                ctypes.c_void_p)
+HALO_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class DistComm(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("allreduce_sum", ALLREDUCE_FN), ("halo", HALO_FN)]
 
 
 def _load():
@@ -154,6 +165,12 @@ def _load():
         "celg_dist_pcg_poll": (i, [vp, ip, ip]),
         "celg_dist_pcg_verify": (i, [vp, vp, vp]),
         "celg_dist_pcg_result": (i, [vp, ctypes.POINTER(Result)]),
+        "celg_dist_pcg_solve": (i, [vp, ctypes.POINTER(DistComm), vp, vp, i, ctypes.POINTER(Result)]),
+        "celg_dist_set_exchange": (i, [vp, i, vp, vp, vp, vp, vp]),
+        "celg_nccl_unique_id": (i, [vp]),
+        "celg_nccl_comm_create": (i, [vp, i, i, i, ctypes.POINTER(vp)]),
+        "celg_nccl_comm_destroy": (i, [vp]),
+        "celg_dist_pcg_solve_nccl": (i, [vp, vp, vp, vp, i, i, ctypes.POINTER(Result)]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -294,10 +311,93 @@ class Dist:
         _check(st, "celg_dist_pcg_result", allow=(ERR_NOCONV, ERR_BREAKDOWN))
         return _info(res, hist, st)
 
+    def _result_buffers(self, history):
+        res = Result()
+        hist = None
+        if history:
+            hist = np.zeros(self.iter_max + 1)
+            res.history = hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            res.history_cap = hist.size
+        return res, hist
+
+    def solve(self, allreduce_sum, halo, b_d, x_ext_d, poll_every=8, history=False):
+        """celg_dist_pcg_solve: the whole solve with the exchanges done by the
+        Python callables allreduce_sum(buf_d, count, stream) and
+        halo(vec_ext_d, stream) (device pointers as ints; return None or 0)."""
+        errors = []
+
+        def guarded(fn, *a):
+            try:
+                return int(fn(*a) or 0)
+            except BaseException as e:  # noqa: BLE001 - re-raised after the call
+                errors.append(e)
+                return 1
+
+        def ar(ctx, buf, count, stream):
+            return guarded(allreduce_sum, buf, count, stream)
+
+        def hl(ctx, vec, stream):
+            return guarded(halo, vec, stream)
+
+        comm = DistComm(None, ALLREDUCE_FN(ar), HALO_FN(hl))
+        res, hist = self._result_buffers(history)
+        st = lib.celg_dist_pcg_solve(self.ptr, ctypes.byref(comm), ctypes.c_void_p(b_d),
+                                     ctypes.c_void_p(x_ext_d), int(poll_every), ctypes.byref(res))
+        if errors:
+            raise errors[0]
+        _check(st, "celg_dist_pcg_solve", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return _info(res, hist, st)
+
+    def set_exchange(self, peers, send_rows, recv):
+        """celg_dist_set_exchange: peers[q] with send_rows[q] (local rows, any
+        int array) and recv[q] = (halo start, count)."""
+        peers = np.asarray(peers, np.int32)
+        counts = np.asarray([len(r) for r in send_rows], np.int32)
+        rows = (np.concatenate([np.asarray(r, np.int32) for r in send_rows])
+                if len(send_rows) else np.zeros(0, np.int32)).astype(np.int32)
+        starts = np.asarray([r[0] for r in recv], np.int32)
+        rcount = np.asarray([r[1] for r in recv], np.int32)
+        _check(lib.celg_dist_set_exchange(self.ptr, int(peers.size), _host_ptr(peers),
+                                          _host_ptr(counts), _host_ptr(rows), _host_ptr(starts),
+                                          _host_ptr(rcount)), "celg_dist_set_exchange")
+
+    def solve_nccl(self, nccl_comm, b_d, x_ext_d, poll_every=8, overlap=False, history=False):
+        """celg_dist_pcg_solve_nccl: the whole solve, exchanges over NCCL."""
+        res, hist = self._result_buffers(history)
+        st = lib.celg_dist_pcg_solve_nccl(self.ptr, ctypes.c_void_p(nccl_comm), ctypes.c_void_p(b_d),
+                                          ctypes.c_void_p(x_ext_d), int(poll_every), int(overlap),
+                                          ctypes.byref(res))
+        _check(st, "celg_dist_pcg_solve_nccl", allow=(ERR_NOCONV, ERR_BREAKDOWN))
+        return _info(res, hist, st)
+
     def destroy(self):
         if self.ptr:
             lib.celg_dist_destroy(self.ptr)
             self.ptr = ctypes.c_void_p()
+
+
+NCCL_ID_BYTES = 128
+
+
+def nccl_unique_id():
+    """celg_nccl_unique_id: 128 bytes, made on one rank, broadcast by the caller."""
+    buf = (ctypes.c_ubyte * NCCL_ID_BYTES)()
+    _check(lib.celg_nccl_unique_id(buf), "celg_nccl_unique_id")
+    return bytes(buf)
+
+
+def nccl_comm_create(uid, nranks, rank, device):
+    """celg_nccl_comm_create (collective over the nranks ranks): the
+    communicator as an int."""
+    buf = (ctypes.c_ubyte * NCCL_ID_BYTES).from_buffer_copy(bytes(uid))
+    out = ctypes.c_void_p()
+    _check(lib.celg_nccl_comm_create(buf, int(nranks), int(rank), int(device), ctypes.byref(out)),
+           "celg_nccl_comm_create")
+    return out.value
+
+
+def nccl_comm_destroy(comm):
+    _check(lib.celg_nccl_comm_destroy(ctypes.c_void_p(comm)), "celg_nccl_comm_destroy")
 
 
 class SolveInfo(dict):

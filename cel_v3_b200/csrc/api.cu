@@ -343,6 +343,7 @@ extern "C" const char* celg_status_string(int s) {
     case CELG_ERR_NOCONV: return "iteration limit reached";
     case CELG_ERR_TIMEOUT: return "device wait timed out";
     case CELG_ERR_STATE: return "call out of order";
+    case CELG_ERR_COMM: return "an exchange between ranks failed";
     default: return "unknown status";
   }
 }
@@ -414,6 +415,9 @@ extern "C" int celg_destroy(celg_handle* h) {
   cudaFree(h->ru_state_d);
   cudaFreeHost(h->ru_state_h);
   cudaFree(h->hist_d);
+  cudaFree(h->gm_work);
+  cudaFree(h->gm_state_d);
+  cudaFreeHost(h->gm_state_h);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);

@@ -64,6 +64,7 @@ struct BOpPre {
   BatchArgs a;
   const int* part = nullptr;
   const int* part_count = nullptr;
+  const double* eps_rel_sys = nullptr;  // per-system eps_rel (refinement inner solves)
   __device__ bool prepare() { return true; }
   __device__ TileInfo tile_info(long) const { return TileInfo{1, 0.0}; }
   __device__ void begin_tile(const TileInfo&) {}
@@ -79,7 +80,8 @@ struct BOpPre {
     a.xpend[s] = 0;
     a.bnorm[s] = sqrt(tot[0]);
     double e = eps_abs;
-    if (eps_rel > 0.0 && eps_rel * a.bnorm[s] > e) e = eps_rel * a.bnorm[s];
+    const double er = eps_rel_sys ? eps_rel_sys[s] : eps_rel;
+    if (er > 0.0 && er * a.bnorm[s] > e) e = er * a.bnorm[s];
     a.eps[s] = e;
     a.err[s] = 0;
     a.iter[s] = 0;
@@ -138,10 +140,18 @@ struct BEpiAp {
   __device__ void begin_tile(const TileInfo&) {}
   __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
+  static constexpr bool kDiagX = true;
   __device__ void row(long i, VT s, double* acc) const {
     const VT vi = vadd(VT(0), s);
     v[i] = vi;
     acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
+  }
+  // p(i) from the diagonal entry's gather (the sweep runs on x = p)
+  __device__ void row_x(long i, VT s, bool have, VT xi, const VT* x, double* acc) const {
+    const VT vi = vadd(VT(0), s);
+    v[i] = vi;
+    const VT pi = (have && x == p) ? xi : __ldg(p + i);
+    acc[0] = dadd(acc[0], dmul(D(vi), D(pi)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     const double sg = a.alpha[s] / tot[0];
@@ -285,6 +295,8 @@ struct IrState {
   int* inner_total;  // inner iterations over all outer steps
   int* part_count;
   int outer_max;
+  double* tau_sys;   // inner tolerance of the system's next inner solve
+  double tau;        // inner_eps_rel
 };
 
 // r = b - (0 + A x) in FP64, ||r|| per system; the system's outer decision
@@ -319,6 +331,7 @@ struct BEpiIrResidual {
       ir.status[s] = st;
     } else {
       ir.part[s] = 1;
+      ir.tau_sys[s] = ir_step_tolerance(rn, a.eps[s], ir.tau);
       atomicAdd(ir.part_count, 1);
     }
   }
@@ -469,6 +482,7 @@ struct Batch {
   float* J32 = nullptr;
   float* F = nullptr;          // 5 x N floats: B32 D32 R32 P32 V32
   int* irs = nullptr;          // part, done, status, outer, inner_total (nsys each), part_count
+  double* irtau = nullptr;     // inner tolerance per system
   double* dstate2 = nullptr;   // inner-solve scalars, 7 x nsys
   int* istate2 = nullptr;      // inner-solve counters, 4 x nsys + 1
 };
@@ -490,6 +504,7 @@ void batch_free(Batch* b) {
   cudaFree(b->J32);
   cudaFree(b->F);
   cudaFree(b->irs);
+  cudaFree(b->irtau);
   cudaFree(b->dstate2);
   cudaFree(b->istate2);
   delete b;
@@ -804,6 +819,7 @@ static int batch_ensure_f32(celg_handle* h, Batch* bt) {
   ok(cudaMalloc(&bt->J32, sizeof(float) * N));
   ok(cudaMalloc(&bt->F, sizeof(float) * N * 5));
   ok(cudaMalloc(&bt->irs, sizeof(int) * (5 * c + 1)));
+  ok(cudaMalloc(&bt->irtau, sizeof(double) * c));
   ok(cudaMalloc(&bt->dstate2, sizeof(double) * 7 * c));
   ok(cudaMalloc(&bt->istate2, sizeof(int) * (4 * c + 1)));
   ok(cudaMemsetAsync(bt->F, 0, sizeof(float) * N * 5, h->stream));
@@ -830,15 +846,15 @@ static int run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int*
   return CELG_OK;
 }
 
-static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, BatchArgs ai,
-                                double inner_eps_rel) {
+static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, BatchArgs ai) {
   const long N = bt->N;
   float* B32 = bt->F;
   float* D32 = B32 + N;
   float* R32 = D32 + N;
   float* P32 = R32 + N;
   float* V32 = P32 + N;
-  const BOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps_rel, ai, ir.part, ir.part_count};
+  const BOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, ir.tau, ai, ir.part, ir.part_count,
+                          ir.tau_sys};
   const BEpiInit<float> init{B32, R32, P32, bt->J32, ai};
   const BEpiAp<float> ap{V32, P32, ai};
   const BOpUpdate<float> upd{R32, V32, bt->J32, ai, 0.0};
@@ -879,6 +895,8 @@ static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, cons
   ir.inner_total = ir.outer + c;
   ir.part_count = ir.inner_total + c;
   ir.outer_max = p->outer_max > 0 ? p->outer_max : 20;
+  ir.tau_sys = bt->irtau;
+  ir.tau = inner_eps;
   const BatchArgs a = batch_args(bt, p->iter_max, 0, h->err_d);
   CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
   for (int s = 0; s < c; ++s) {
@@ -920,14 +938,13 @@ static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, cons
       GraphEntry* ge = graph_cache_find(h, gkey);
       if (!ge) {
         st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
-          return record_batched_inner(h, bt, ir, batch_args(bt, inner_max, cond, h->err_d, true),
-                                      inner_eps);
+          return record_batched_inner(h, bt, ir, batch_args(bt, inner_max, cond, h->err_d, true));
         }, &ge);
         if (st) break;
       }
       CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
     } else {
-      st = record_batched_inner(h, bt, ir, ai_host, inner_eps);
+      st = record_batched_inner(h, bt, ir, ai_host);
       if (st) break;
     }
     ir_count_kernel<<<(c + 127) / 128, 128, 0, h->stream>>>(c, ir, ai_host.iter, ai_host.err);

@@ -193,6 +193,31 @@ __device__ __forceinline__ double group_fold256(double v, double* scratch, int t
   return tot;
 }
 
+// group_fold256 of M values at once (each in the same order as alone), with
+// two barriers in all; `scratch` holds 8 M doubles.  The results are in
+// v[] of thread 0.
+template <int M>
+__device__ __forceinline__ void group_fold256_n(double (&v)[M], double* scratch, int tid,
+                                                int bar_id) {
+#pragma unroll
+  for (int i = 0; i < M; ++i) v[i] = warp_fold(v[i]);
+  if ((tid & 31) == 0) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) scratch[(tid >> 5) * M + i] = v[i];
+  }
+  named_bar_sync(bar_id, kLanes);
+  if (tid == 0) {
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      double tot = scratch[i];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) tot = dadd(tot, scratch[w * M + i]);
+      v[i] = tot;
+    }
+  }
+  named_bar_sync(bar_id, kLanes);
+}
+
 // The 256-lane order computed by one warp: lane l plays the virtual lanes
 // l + 32 g (g = 0..7) -- virtual lane j sums p[j], p[j+256], ... from 0.0;
 // each group of 32 virtual lanes folds with the butterfly; the 8 group sums
@@ -277,6 +302,29 @@ struct finishes_always : std::false_type {};
 template <class T>
 struct finishes_always<T, std::void_t<decltype(T::kFinishAlways)>>
     : std::integral_constant<bool, T::kFinishAlways> {};
+
+// ---- FP32 refinement: inner tolerance of an outer step ----------------------
+//
+// tau (inner_eps_rel) is the tightest relative tolerance an inner FP32 solve
+// is asked for.  At an outer step with residual norm rn and outer tolerance
+// tol, the goal g = tol / (2 rn) is the reduction still needed (with a margin
+// of 2).  If one inner solve at tau reaches it (tau <= g), the step asks for
+// g itself; if two do (tau^2 <= g), for sqrt(g), so that the remaining two
+// steps share the reduction; otherwise for tau.  A step then never does more
+// than the remaining steps need, and the last one does not end just short of
+// tol, which would cost a further restart of the Krylov space.  Only a
+// division and a square root are used, correctly rounded on the host and on
+// the GPU alike, so every form of the refinement takes the same decisions.
+__host__ __device__ inline double ir_step_tolerance(double rn, double tol, double tau) {
+  if (!(tol > 0.0) || !(rn > tol) || !(tau > 0.0 && tau < 1.0) || !(rn < 1.0e308)) return tau;
+  const double g = tol / (2.0 * rn);
+  if (tau <= g) return g;
+  if (tau * tau <= g) {
+    const double r = sqrt(g);
+    return r > tau ? r : tau;
+  }
+  return tau;
+}
 
 // ---- batched solves --------------------------------------------------------
 //

@@ -95,6 +95,11 @@ struct celg_handle {
   struct Batch* batch = nullptr;
   // work vectors and per-column state of multi-right-hand-side solves
   struct Multi* multi = nullptr;
+  // GMRES(m) work space (V, Z, H) and device state, kept between solves
+  double* gm_work = nullptr;
+  size_t gm_cap = 0;          // doubles
+  void* gm_state_d = nullptr;
+  void* gm_state_h = nullptr; // pinned
   // last solve timing
   float last_ms = 0.f;
   int last_iters = 0;
@@ -176,6 +181,9 @@ void free_mat_arrays(celg_mat* m);
 int coo_to_mat_device(celg_handle* h, int n, int ncols, int nnz, const int* rows_d,
                       const int* cols_d, const double* vals_d, int row_base, int col_base,
                       celg_mat** out);
+// dist.cu / dist_solve.cu: the one-call distributed solve's data on a celg_dist
+int dist_internals(celg_dist* d, celg_handle** h, int* n, int* ncols, void*** solve_slot);
+void dist_solve_free(void* solve);
 void batch_free(::Batch* b);
 void multi_free(::Multi* m);
 void multi_forget_matrix(::Multi* m, const void* mat);

@@ -141,10 +141,18 @@ struct DEpiAp {
   const double* p;
   DistArgs a;
   __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
+  static constexpr bool kDiagX = true;
   __device__ void row(long i, double s, double* acc) const {
     const double vi = dadd(0.0, s);
     v[i] = vi;
     acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
+  }
+  // p(i) from the diagonal entry's gather (the sweep runs on x = p)
+  __device__ void row_x(long i, double s, bool have, double xi, const double* x,
+                        double* acc) const {
+    const double vi = dadd(0.0, s);
+    v[i] = vi;
+    acc[0] = dadd(acc[0], dmul(vi, (have && x == p) ? xi : __ldg(p + i)));
   }
   __device__ void finish(double* tot) const { xch_store(a.st, a, 0.0, 0.0, 0.0, tot[0]); }
 };
@@ -280,8 +288,21 @@ struct celg_dist {
   // halo value; part: the tile partials of the split SpMV phase
   long win_lo = 0, win_hi = 0;
   double* part = nullptr;
+  // work vectors and exchange plan of celg_dist_pcg_solve (dist_solve.cu)
+  void* solve = nullptr;
   DistArgs args() const { return DistArgs{st, hist, hist_cap, p.iter_max, h->err_d}; }
 };
+
+namespace celg {
+int dist_internals(celg_dist* d, celg_handle** h, int* n, int* ncols, void*** solve_slot) {
+  if (!d || !d->h || !d->m) return CELG_ERR_ARG;
+  *h = d->h;
+  *n = d->m->csr.n;
+  *ncols = d->m->csr.ncols;
+  *solve_slot = &d->solve;
+  return CELG_OK;
+}
+}  // namespace celg
 
 static int dist_check(const celg_dist* d) {
   if (!d || !d->h || !d->m) return CELG_ERR_ARG;
@@ -382,6 +403,7 @@ extern "C" int celg_dist_destroy(celg_dist* d) {
   if (d->own_state) cudaFree(d->st);
   cudaFreeHost(d->host);
   cudaFree(d->part);
+  dist_solve_free(d->solve);
   delete d;
   return CELG_OK;
 }
@@ -402,7 +424,6 @@ extern "C" int celg_dist_pcg_init(celg_dist* d, const double* b_d, const double*
                                   double* r_d, double* p_ext_d) {
   if (dist_check(d) || !b_d || !x_ext_d || !r_d || !p_ext_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  const CsrDev& A = d->m->csr;
   DEpiInit epi{b_d, r_d, p_ext_d, d->m->jacobi, d->p.eps_abs, d->p.eps_rel, d->args()};
   return dist_csr(d, x_ext_d, epi);
 }
@@ -418,7 +439,6 @@ extern "C" int celg_dist_pcg_start(celg_dist* d) {
 extern "C" int celg_dist_pcg_ap(celg_dist* d, const double* p_ext_d, double* v_d) {
   if (dist_check(d) || !p_ext_d || !v_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  const CsrDev& A = d->m->csr;
   return dist_csr(d, p_ext_d, DEpiAp{v_d, p_ext_d, d->args()});
 }
 
@@ -470,7 +490,6 @@ extern "C" int celg_dist_pcg_direction(celg_dist* d, double* x_ext_d, const doub
 extern "C" int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const double* x_ext_d) {
   if (dist_check(d) || !b_d || !x_ext_d) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(d->h->device));
-  const CsrDev& A = d->m->csr;
   return dist_csr(d, x_ext_d, DEpiVerify{b_d, d->args()});
 }
 

@@ -3,12 +3,16 @@
 //   x = x0;  for k = 0, 1, ...:
 //     r = b - A x,  ||r||            (FP64 matrix, FP64 vectors, on the GPU)
 //     stop when ||r|| <= max(eps_abs, eps_rel ||b||)
-//     d = PCG_fp32(A32, r/||r||)      (inner tolerance inner_eps_rel)
+//     d = PCG_fp32(A32, r/||r||)      (inner tolerance tau_k, below)
 //     x = x + ||r|| d                 (FP64)
 // The outer residual, update and stopping test stay in binary64, so the
 // reported accuracy is the FP64-verified ||b - A x|| / ||b||.  The inner
 // solve reads 8 bytes per non-zero (float value + int32 column) and float
 // vectors instead of 12 bytes and doubles.
+//
+// Each refinement step asks its inner solve for ir_step_tolerance(||r||, eps,
+// inner_eps_rel) (celg_device.cuh): never tighter than inner_eps_rel, looser
+// when one or two more steps at inner_eps_rel would more than finish.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -99,7 +103,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   std::memcpy(&ip, p, sizeof(ip));
   ip.x0_mode = CELG_X0_ZERO;
   ip.eps_abs = 0.0;
-  ip.eps_rel = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-4;
+  const double tau = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-4;
   ip.iter_max = p->inner_iter_max > 0 ? p->inner_iter_max : 1000;
 
   PcgBind<float> B;
@@ -151,6 +155,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
     if (outer >= outer_max) break;
     st = launch_tile(h, n, OpToF32{r, b32, 1.0 / rn});
     if (st) break;
+    ip.eps_rel = ir_step_tolerance(rn, tol, tau);
     PcgState s;
     const int ist = pcg_run<float>(h, B, &ip, m, &s);
     inner_total += s.iter;

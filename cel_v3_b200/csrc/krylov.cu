@@ -1,13 +1,17 @@
 // krylov.cu -- unpreconditioned CG (cel_cgalg) and restarted GMRES(m) with
 // right Jacobi preconditioning (cel_gmresalg_2jacobi).  The vector sweeps
-// run on the device with the fixed-order reductions; the scalar recurrences
-// (CG step lengths, GMRES Hessenberg column, Givens rotations and back
-// substitution) run on the host in IEEE binary64, in the reference's order.
+// run on the device with the fixed-order reductions.  CG's scalar recurrence
+// runs on the host; GMRES runs entirely on the device: the Hessenberg column,
+// the Givens rotations, the convergence test, the back substitution and the
+// restart decisions are one-thread kernels between the sweeps, in the
+// reference's operation order, so that a whole solve is one CUDA graph (a
+// WHILE node over restart cycles) with no host synchronisation inside.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
+#include "graph.cuh"
 #include "pcg_internal.cuh"
 
 namespace celg {
@@ -59,8 +63,12 @@ struct OpV1 {
   double* v;
   double* z;
   const double* J;
-  double inv;
-  __device__ bool prepare() { return true; }
+  const double* rn;   // ||r|| (device): v = r * (1 / ||r||)
+  double inv = 0.0;
+  __device__ bool prepare() {
+    inv = 1.0 / *(volatile const double*)rn;
+    return true;
+  }
   __device__ void load(long i, Regs& g) const { g.r = __ldg(r + i); g.J = __ldg(J + i); }
   __device__ void compute(long i, Regs& g, double*) const {
     const double vi = dmul(g.r, inv);
@@ -78,8 +86,14 @@ struct OpVNext {
   double* v;
   double* z;
   const double* J;
-  double hdiv;
-  __device__ bool prepare() { return true; }
+  const double* hd;   // h(j+1, j) before the rotations (device)
+  const int* act;     // the cycle's Arnoldi steps go on (device)
+  double hdiv = 0.0;
+  __device__ bool prepare() {
+    if (!*(volatile const int*)act) return false;
+    hdiv = *hd;
+    return true;
+  }
   __device__ void load(long i, Regs& g) const { g.w = __ldg(w + i); g.J = __ldg(J + i); }
   __device__ void compute(long i, Regs& g, double*) const {
     const double vi = __ddiv_rn(g.w, hdiv);
@@ -100,8 +114,13 @@ struct OpMgs {
   const double* vnext;  // null: norm of w
   const double* hij;
   double* out;
-  double h;
-  __device__ bool prepare() { h = *hij; return true; }
+  const int* act;     // the cycle's Arnoldi steps go on (device)
+  double h = 0.0;
+  __device__ bool prepare() {
+    if (!*(volatile const int*)act) return false;
+    h = *hij;
+    return true;
+  }
   __device__ void load(long i, Regs& g) const {
     g.w = w[i];
     g.v = __ldg(vi + i);
@@ -115,16 +134,166 @@ struct OpMgs {
   __device__ void finish(double* tot) const { *out = vnext ? tot[0] : sqrt(tot[0]); }
 };
 
-// x = x + sum_i al_i z_i, terms added in order i = 0..k-1 (:755-760, :799-803)
-constexpr int kMaxRestart = 128;
-struct ZList {
-  const double* z[kMaxRestart];
-  double al[kMaxRestart];
+// v_0 . w -> h(0, j), skipped when the cycle has ended
+struct OpDotIf {
+  static constexpr int NRED = 1;
+  struct Regs { double a, b; };
+  const double* a;
+  const double* b;
+  double* out;
+  const int* act;
+  __device__ bool prepare() { return *(volatile const int*)act != 0; }
+  __device__ void load(long i, Regs& r) const { r.a = __ldg(a + i); r.b = __ldg(b + i); }
+  __device__ void compute(long, Regs& r, double* acc) const { acc[0] = dadd(acc[0], dmul(r.a, r.b)); }
+  __device__ void finish(double* tot) const { *out = tot[0]; }
 };
-__global__ void x_update_kernel(long n, double* __restrict__ x, ZList zl, int k) {
+
+// w = 0 + A z_j, skipped when the cycle has ended
+struct EpiStoreIf {
+  static constexpr int NRED = 0;
+  double* y;
+  const int* act;
+  __device__ bool active() const { return *(volatile const int*)act != 0; }
+  __device__ void row(long r, double s, double*) const { y[r] = dadd(0.0, s); }
+  __device__ void finish(double*) const {}
+};
+
+// ---- GMRES device state and its one-thread kernels -----------------------------
+
+constexpr int kMaxRestart = 128;
+
+struct GmState {
+  double eps, bnorm, resnorm, local;
+  int iter, steps, restart, hpos, jdone, conv, act, go;
+  double hn[kMaxRestart];   // h(j+1, j) before the rotations: v_{j+1} = w / hn[j]
+  double cc[kMaxRestart], ss[kMaxRestart], gam[kMaxRestart + 1], al[kMaxRestart];
+};
+
+struct GmArgs {
+  GmState* st;
+  double* H;     // (M+1) x M Hessenberg, column-major: H(i, j) = H[j (M+1) + i]
+  int M;
+  double* hist;  // |gamma| history (device, hist_cap entries) or null
+  int hist_cap;
+  int iter_max;
+  int literal;   // the reference's unrotated Givens update (:722-727)
+  cudaGraphConditionalHandle cond;
+  const int* errw;
+  __device__ double& h(int i, int j) const { return H[(size_t)j * (M + 1) + i]; }
+  __device__ void push_hist(double v) const {
+    if (hist && st->hpos < hist_cap) hist[st->hpos] = v;
+    st->hpos += 1;
+  }
+};
+
+// after ||b||: the tolerance and the counters of the first outer iteration
+__global__ void gm_setup_kernel(GmArgs a, double eps_abs, double eps_rel) {
+  GmState* s = a.st;
+  double e = eps_abs;
+  if (eps_rel > 0.0 && eps_rel * s->bnorm > e) e = eps_rel * s->bnorm;
+  s->eps = e;
+  s->iter = 1;  // the outer loop's first ++iter (:643)
+  s->steps = 0;
+  s->restart = 0;
+  s->hpos = 0;
+  s->conv = 0;
+  s->act = 0;
+  s->go = 1;
+}
+
+// after the first residual: its norm opens the history
+__global__ void gm_begin_kernel(GmArgs a) {
+  GmState* s = a.st;
+  a.push_hist(s->resnorm);
+  s->local = s->resnorm;
+}
+
+// a restart cycle begins: gamma_0 = ||r|| (:669-672)
+__global__ void gm_cycle_start_kernel(GmArgs a) {
+  GmState* s = a.st;
+  s->gam[0] = s->resnorm;
+  s->jdone = a.M;
+  s->act = 1;
+}
+
+// Arnoldi step j after the Gram-Schmidt sweeps left the raw column
+// h(0..j+1, j): the previous rotations, the new rotation, gamma and the
+// convergence test (:722-737), in the host restatement's operation order.
+__global__ void gm_givens_kernel(GmArgs a, int j) {
+  GmState* s = a.st;
+  if (!s->act) return;
+  s->steps += 1;
+  for (int i = 0; i < j; ++i) {
+    if (a.literal) {
+      const double t = dadd(dmul(a.h(i, j), s->cc[i]), dmul(a.h(i + 1, j), s->ss[i]));
+      a.h(i, j) = dadd(dmul(-t, s->ss[i]), dmul(a.h(i + 1, j), s->cc[i]));
+    } else {
+      const double top = dadd(dmul(a.h(i, j), s->cc[i]), dmul(a.h(i + 1, j), s->ss[i]));
+      const double bot = dadd(dmul(-a.h(i, j), s->ss[i]), dmul(a.h(i + 1, j), s->cc[i]));
+      a.h(i, j) = top;
+      a.h(i + 1, j) = bot;
+    }
+  }
+  const double hjj = a.h(j, j), hn = a.h(j + 1, j);
+  s->hn[j] = hn;
+  const double beta = sqrt(dadd(dmul(hjj, hjj), dmul(hn, hn)));
+  s->ss[j] = hn / beta;
+  s->cc[j] = hjj / beta;
+  a.h(j, j) = beta;
+  s->gam[j + 1] = dmul(-s->ss[j], s->gam[j]);
+  s->gam[j] = dmul(s->cc[j], s->gam[j]);
+  const double g = fabs(s->gam[j + 1]);
+  a.push_hist(g);
+  if (g <= s->eps) {
+    s->jdone = j + 1;
+    s->conv = 1;
+    s->act = 0;
+  }
+}
+
+// al = H^-1 gamma over the cycle's jdone steps (:739-747, :784-792)
+__global__ void gm_backsub_kernel(GmArgs a) {
+  GmState* s = a.st;
+  const int k = s->jdone;
+  for (int i = k - 1; i >= 0; --i) {
+    double acc = 0.0;
+    for (int t = i + 1; t < k; ++t) acc = dadd(acc, dmul(a.h(i, t), s->al[t]));
+    s->al[i] = dmul(1.0 / a.h(i, i), __dsub_rn(s->gam[i], acc));
+  }
+  s->act = 0;
+}
+
+// after the cycle's residual: the restart and outer-loop decisions
+// (:643, :664-668, :824-830); sets the WHILE node's condition
+__global__ void gm_cycle_end_kernel(GmArgs a) {
+  GmState* s = a.st;
+  s->local = s->resnorm;
+  s->restart += 1;
+  int go = 1;
+  if (s->conv || *(volatile const int*)a.errw) {
+    go = 0;
+  } else if (s->restart > a.M) {
+    // the inner while ends; the outer one goes on while iter <= iter_max
+    // (its residual is the one just computed, x being unchanged)
+    if (s->iter <= a.iter_max) {
+      s->iter += 1;
+      s->restart = 0;
+    } else {
+      go = 0;
+    }
+  }
+  s->go = go;
+  if (a.cond) cudaGraphSetConditional(a.cond, (unsigned)go);
+}
+
+// x = x + sum_i al_i z_i over the cycle's steps, terms added in order
+// i = 0..k-1 (:755-760, :799-803)
+__global__ void x_update_kernel(long n, double* __restrict__ x, const double* __restrict__ Z,
+                                size_t nn, const GmState* __restrict__ st) {
+  const int k = st->jdone;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     double xi = x[i];
-    for (int t = 0; t < k; ++t) xi = dadd(xi, dmul(zl.al[t], __ldg(zl.z[t] + i)));
+    for (int t = 0; t < k; ++t) xi = dadd(xi, dmul(st->al[t], __ldg(Z + nn * (size_t)t + i)));
     x[i] = xi;
   }
 }
@@ -244,140 +413,196 @@ int cg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 
 // ---- GMRES(m): cel_gmresalg_2jacobi, src/fcgalg/cel_gmresalg_module.f90:570-851 -------
 
+// The work space of a GMRES(M) solve on n rows, kept by the handle:
+// V[0..M], Z[0..M-1] and H ((M+1) x M), plus the device state.
+static int ensure_gmres_work(celg_handle* h, size_t nn, int M) {
+  const size_t need = nn * (size_t)(2 * M + 1) + (size_t)(M + 1) * M + 8;
+  if (!h->gm_state_d) {
+    CELG_CUDA(cudaMalloc(&h->gm_state_d, sizeof(GmState)));
+    CELG_CUDA(cudaMallocHost(&h->gm_state_h, sizeof(GmState)));
+  }
+  if (need <= h->gm_cap && h->gm_work) return CELG_OK;
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  graph_cache_clear(h);
+  cudaFree(h->gm_work);
+  h->gm_work = nullptr;
+  h->gm_cap = 0;
+  CELG_CUDA(cudaMalloc(&h->gm_work, sizeof(double) * need));
+  h->gm_cap = need;
+  return CELG_OK;
+}
+
+struct GmPlan {
+  celg_mat* m;
+  int fmt;
+  long n;
+  size_t nn;
+  const double* b;
+  double* x;
+  const celg_params* p;
+  double* V;
+  double* Z;
+  double* r;
+  double* w;
+  GmArgs a;
+  double* Vp(int i) const { return V + nn * (size_t)i; }
+  double* Zp(int i) const { return Z + nn * (size_t)i; }
+  double* Hp(int i, int j) const { return a.H + (size_t)j * (a.M + 1) + i; }
+};
+
+static int gm_spmv(celg_handle* h, const GmPlan& g, const double* x, double* y) {
+  const EpiStoreIf epi{y, &g.a.st->act};
+  if (g.fmt == CELG_FMT_JAD) return launch_jad(h, g.m->csr, g.m->jad, x, epi);
+  return launch_csr<double>(h, g.m->csr, g.m->csr.v, x, epi);
+}
+
+// x0, ||b||, the tolerance and the first residual
+static int gm_record_setup(celg_handle* h, const GmPlan& g) {
+  int st = set_x0(h, g.n, g.p->x0_mode, g.x);
+  if (!st) st = launch_dot(h, g.n, g.b, g.b, &g.a.st->bnorm, 1);
+  if (st) return st;
+  gm_setup_kernel<<<1, 1, 0, h->stream>>>(g.a, g.p->eps_abs, g.p->eps_rel);
+  CELG_CUDA(cudaGetLastError());
+  st = launch_residual(h, g.m, g.fmt, g.b, g.x, g.r, &g.a.st->resnorm);
+  if (st) return st;
+  gm_begin_kernel<<<1, 1, 0, h->stream>>>(g.a);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
+// One restart cycle: M Arnoldi steps (the kernels of the steps after
+// convergence return at once), back substitution, x update, the new
+// residual and the loop decision.
+static int gm_record_cycle(celg_handle* h, const GmPlan& g) {
+  const int M = g.a.M;
+  const int* act = &g.a.st->act;
+  const double* J = g.m->jacobi;
+  gm_cycle_start_kernel<<<1, 1, 0, h->stream>>>(g.a);
+  CELG_CUDA(cudaGetLastError());
+  // v_0 = r * (1/||r||); z_0 = J v_0 (:669, :683)
+  int st = launch_tile(h, g.n, OpV1{g.r, g.Vp(0), g.Zp(0), J, &g.a.st->local});
+  for (int j = 0; !st && j < M; ++j) {
+    // w = 0 + A z_j (:680-697)
+    st = gm_spmv(h, g, g.Zp(j), g.w);
+    // h_0j = v_0 . w, then modified Gram-Schmidt with the next coefficient fused
+    if (!st) st = launch_tile(h, g.n, OpDotIf{g.Vp(0), g.w, g.Hp(0, j), act});
+    for (int i = 0; !st && i <= j; ++i) {
+      const bool last = i == j;
+      st = launch_tile(h, g.n, OpMgs{g.w, g.Vp(i), last ? nullptr : g.Vp(i + 1), g.Hp(i, j),
+                                     last ? g.Hp(j + 1, j) : g.Hp(i + 1, j), act});
+    }
+    if (st) break;
+    gm_givens_kernel<<<1, 1, 0, h->stream>>>(g.a, j);
+    CELG_CUDA(cudaGetLastError());
+    // v_{j+1} = w / h(j+1,j); z_{j+1} = J v_{j+1}
+    if (j + 1 < M)
+      st = launch_tile(h, g.n, OpVNext{g.w, g.Vp(j + 1), g.Zp(j + 1), J, &g.a.st->hn[j], act});
+  }
+  if (st) return st;
+  gm_backsub_kernel<<<1, 1, 0, h->stream>>>(g.a);
+  CELG_CUDA(cudaGetLastError());
+  if (g.n > 0) {
+    const int grid = (int)std::max(1L, std::min((g.n + 255) / 256, (long)h->sms * 16));
+    x_update_kernel<<<grid, 256, 0, h->stream>>>(g.n, g.x, g.Z, g.nn, g.a.st);
+    CELG_CUDA(cudaGetLastError());
+  }
+  // r = b - A x ; ||r|| (:808-824)
+  st = launch_residual(h, g.m, g.fmt, g.b, g.x, g.r, &g.a.st->resnorm);
+  if (st) return st;
+  gm_cycle_end_kernel<<<1, 1, 0, h->stream>>>(g.a);
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 int gmres_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg_params* p,
                 celg_result* res) {
   const long n = m->csr.n;
   const int fmt = p->fmt;
   const int M = p->restart;
   if (M <= 0 || M > kMaxRestart) return CELG_ERR_ARG;
+  if (p->iter_max < 0) return CELG_ERR_ARG;
   if (!m->jacobi) return CELG_ERR_STATE;
   if (fmt == CELG_FMT_JAD && m->jad.mmax < 0) return CELG_ERR_STATE;
+  const size_t nn = (size_t)std::max(1L, n);
   int st = ensure_work(h, (size_t)n);
+  if (!st) st = ensure_gmres_work(h, nn, M);
+  if (!st) st = ensure_partials(h, ntiles_of(n), 2);
+  const int hist_cap = (res && res->history && res->history_cap > 0) ? res->history_cap : 0;
+  if (!st && hist_cap) st = ensure_state(h, hist_cap);
   if (st) return st;
   if (res) res->history_len = 0;
-  // V[0..M], Z[0..M-1], w, r ; H raw coefficients (M+1) x M on the device
-  const size_t nn = (size_t)std::max(1L, n);
-  double* base = nullptr;
-  CELG_CUDA(cudaMalloc(&base, sizeof(double) * (nn * (size_t)(2 * M + 1) + (size_t)(M + 1) * M + 8)));
-  double* V = base;
-  double* Z = V + nn * (size_t)(M + 1);
-  double* Hd = Z + nn * (size_t)M;
-  double* w = h->wv;
-  double* r = h->wr;
-  double* sd = h->scal_d;
-  const double* J = m->jacobi;
-  auto Vp = [&](int i) { return V + nn * (size_t)i; };
-  auto Zp = [&](int i) { return Z + nn * (size_t)i; };
-  std::vector<double> H((size_t)(M + 1) * M, 0.0), cc(M + 1), ss(M + 1), gam(M + 2), al(M + 1);
-  auto Hh = [&](int i, int j) -> double& { return H[(size_t)j * (M + 1) + i]; };
-  auto Hdev = [&](int i, int j) { return Hd + (size_t)j * (M + 1) + i; };
-
-  cudaEventRecord(h->ev0, h->stream);
-  double bnorm = 0.0, resnorm = 0.0;
-  int iter = 0, steps = 0, hpos = 0;
-  bool converged = false;
-  do {
-    if ((st = launch_dot(h, n, b, b, sd, 1)) || (st = read_scalar(h, sd, &bnorm))) break;
-    double eps = p->eps_abs;
-    if (p->eps_rel > 0.0 && p->eps_rel * bnorm > eps) eps = p->eps_rel * bnorm;
-    if ((st = set_x0(h, n, p->x0_mode, x))) break;
-    while (iter <= p->iter_max && !converged && !st) {
-      ++iter;
-      // r = b - A x ; ||r|| (:643-663)
-      if ((st = launch_residual(h, m, fmt, b, x, r, sd)) || (st = read_scalar(h, sd, &resnorm))) break;
-      if (hpos == 0) store_hist(res, hpos++, resnorm);
-      double local_res = resnorm;
-      int restart = 0;
-      while (restart <= M && !converged && !st) {
-        // v1 = r * (1/||r||); z1 = J v1 (:669, :683)
-        if ((st = launch_tile(h, n, OpV1{r, Vp(0), Zp(0), J, 1.0 / local_res}))) break;
-        gam[0] = resnorm;
-        int jdone = M;
-        for (int j = 0; j < M; ++j) {
-          // w = 0 + A z_j (:680-697)
-          if ((st = spmv_fmt(h, m, fmt, Zp(j), w))) break;
-          ++steps;
-          // h_0j = v_0 . w, then MGS with the next coefficient fused
-          if ((st = launch_dot(h, n, Vp(0), w, Hdev(0, j), 0))) break;
-          for (int i = 0; i <= j; ++i) {
-            const bool last = i == j;
-            st = launch_tile(h, n, OpMgs{w, Vp(i), last ? nullptr : Vp(i + 1), Hdev(i, j),
-                                         last ? Hdev(j + 1, j) : Hdev(i + 1, j), 0.0});
-            if (st) break;
-          }
-          if (st) break;
-          CELG_CUDA(cudaMemcpyAsync(&Hh(0, j), Hdev(0, j), sizeof(double) * (size_t)(j + 2),
-                                    cudaMemcpyDeviceToHost, h->stream));
-          CELG_CUDA(cudaStreamSynchronize(h->stream));
-          // previous rotations on column j (:722-727; corrected unless literal)
-          for (int i = 0; i < j; ++i) {
-            if (p->literal_ref_bugs) {
-              Hh(i, j) = Hh(i, j) * cc[i] + Hh(i + 1, j) * ss[i];
-              Hh(i, j) = -Hh(i, j) * ss[i] + Hh(i + 1, j) * cc[i];
-            } else {
-              const double top = Hh(i, j) * cc[i] + Hh(i + 1, j) * ss[i];
-              const double bot = -Hh(i, j) * ss[i] + Hh(i + 1, j) * cc[i];
-              Hh(i, j) = top;
-              Hh(i + 1, j) = bot;
-            }
-          }
-          // new rotation (:728-733)
-          const double hn = Hh(j + 1, j);
-          const double beta = std::sqrt(Hh(j, j) * Hh(j, j) + Hh(j + 1, j) * Hh(j + 1, j));
-          ss[j] = Hh(j + 1, j) / beta;
-          cc[j] = Hh(j, j) / beta;
-          Hh(j, j) = beta;
-          gam[j + 1] = -ss[j] * gam[j];
-          gam[j] = cc[j] * gam[j];
-          store_hist(res, hpos++, std::fabs(gam[j + 1]));
-          if (std::fabs(gam[j + 1]) <= eps) {
-            jdone = j + 1;
-            converged = true;
-            break;
-          }
-          // v_{j+1} = w / h(j+1,j); z_{j+1} = J v_{j+1}
-          if (j + 1 < M) {
-            if ((st = launch_tile(h, n, OpVNext{w, Vp(j + 1), Zp(j + 1), J, hn}))) break;
-          }
-        }
-        if (st) break;
-        // back substitution (:739-747, :784-792)
-        for (int i = jdone - 1; i >= 0; --i) {
-          double acc = 0.0;
-          for (int k = i + 1; k < jdone; ++k) acc = acc + Hh(i, k) * al[k];
-          al[i] = (1.0 / Hh(i, i)) * (gam[i] - acc);
-        }
-        ZList zl;
-        for (int i = 0; i < jdone; ++i) {
-          zl.z[i] = Zp(i);
-          zl.al[i] = al[i];
-        }
-        if (n > 0) {
-          const int grid = (int)std::max(1L, std::min((n + 255) / 256, (long)h->sms * 16));
-          x_update_kernel<<<grid, 256, 0, h->stream>>>(n, x, zl, jdone);
-          if (cudaGetLastError() != cudaSuccess) { st = CELG_ERR_CUDA; break; }
-        }
-        // r = b - A x ; ||r|| (:808-824)
-        if ((st = launch_residual(h, m, fmt, b, x, r, sd)) || (st = read_scalar(h, sd, &resnorm))) break;
-        local_res = resnorm;
-        ++restart;
-      }
+  GmPlan g;
+  g.m = m;
+  g.fmt = fmt;
+  g.n = n;
+  g.nn = nn;
+  g.b = b;
+  g.x = x;
+  g.p = p;
+  g.V = h->gm_work;
+  g.Z = g.V + nn * (size_t)(M + 1);
+  g.r = h->wr;
+  g.w = h->wv;
+  GmState* sd = static_cast<GmState*>(h->gm_state_d);
+  g.a = GmArgs{sd, g.Z + nn * (size_t)M, M, hist_cap ? h->hist_d : nullptr, hist_cap, p->iter_max,
+               p->literal_ref_bugs, 0, h->err_d};
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  if (!graphs_enabled()) {
+    // host-driven (profiling): one poll of the loop flag per restart cycle
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = gm_record_setup(h, g);
+    GmState* sh = static_cast<GmState*>(h->gm_state_h);
+    while (!st) {
+      st = gm_record_cycle(h, g);
+      if (st) break;
+      CELG_CUDA(cudaMemcpyAsync(&sh->go, &sd->go, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      CELG_CUDA(cudaStreamSynchronize(h->stream));
+      if (!sh->go) break;
     }
-  } while (0);
-  cudaEventRecord(h->ev1, h->stream);
-  cudaEventSynchronize(h->ev1);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    char kb[512];
+    std::snprintf(kb, sizeof(kb), "gmres|%p|%d|%d|%p|%p|%d|%d|%d|%.17g|%.17g|%d|%d", (const void*)m,
+                  m->csr.n, fmt, (const void*)b, (const void*)x, M, p->x0_mode, p->literal_ref_bugs,
+                  p->eps_abs, p->eps_rel, p->iter_max, hist_cap);
+    const std::string key(kb);
+    GraphEntry* ge = graph_cache_find(h, key);
+    if (!ge) {
+      st = graph_build(h, key, [&](cudaGraphConditionalHandle cond) -> int {
+        GmPlan gc = g;
+        gc.a.cond = cond;
+        int s2 = gm_record_setup(h, gc);
+        if (!s2) s2 = capture_while(h, cond, [&]() -> int { return gm_record_cycle(h, gc); });
+        return s2;
+      }, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  }
+  GmState* sh = static_cast<GmState*>(h->gm_state_h);
+  CELG_CUDA(cudaMemcpyAsync(sh, sd, sizeof(GmState), cudaMemcpyDeviceToHost, h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(h->scal_h + 8, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  std::memcpy(&err_word, h->scal_h + 8, sizeof(int));
   cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
-  cudaFree(base);
-  if (st) return st;
-  h->last_iters = steps;
-  const int ret = converged ? CELG_OK : CELG_ERR_NOCONV;
+  h->last_iters = sh->steps;
+  int ret = sh->conv ? CELG_OK : CELG_ERR_NOCONV;
+  if (err_word) ret = err_word;
   if (res) {
-    res->iter_done = iter;
-    res->final_norm2 = resnorm;
-    res->bnorm = bnorm;
-    res->verified_relres = bnorm > 0 ? resnorm / bnorm : resnorm;
+    res->iter_done = sh->iter;
+    res->final_norm2 = sh->resnorm;
+    res->bnorm = sh->bnorm;
+    res->verified_relres = sh->bnorm > 0 ? sh->resnorm / sh->bnorm : sh->resnorm;
     res->err = ret;
-    res->arnoldi_steps = steps;
+    res->arnoldi_steps = sh->steps;
+    if (hist_cap) {
+      st = copy_history(h, std::min(sh->hpos, hist_cap), res);
+      if (st) return st;
+    }
   }
   return ret;
 }

@@ -675,6 +675,7 @@ struct MOpPre {
   MultiArgs a;
   const int* part = nullptr;
   const int* part_count = nullptr;
+  const double* eps_rel_col = nullptr;  // per-column eps_rel (refinement inner solves)
   __device__ bool prepare() { return true; }
   __device__ bool col_active(int) const { return true; }
   __device__ void begin_col(int) {}
@@ -687,7 +688,8 @@ struct MOpPre {
   __device__ void finish_col(int c, double* tot) const {
     a.bnorm[c] = sqrt(tot[0]);
     double e = eps_abs;
-    if (eps_rel > 0.0 && eps_rel * a.bnorm[c] > e) e = eps_rel * a.bnorm[c];
+    const double er = eps_rel_col ? eps_rel_col[c] : eps_rel;
+    if (er > 0.0 && er * a.bnorm[c] > e) e = er * a.bnorm[c];
     a.eps[c] = e;
     a.err[c] = 0;
     a.iter[c] = 0;
@@ -892,6 +894,8 @@ struct MultiIr {
   int* inner_total;
   int* part_count;
   int outer_max;
+  double* tau_col;   // inner tolerance of the column's next inner solve
+  double tau;        // inner_eps_rel
 };
 
 // r = b - (0 + A x) in FP64, ||r|| per column and the column's outer decision
@@ -927,6 +931,7 @@ struct MEpiIrResidual {
       ir.status[c] = st;
     } else {
       ir.part[c] = 1;
+      ir.tau_col[c] = ir_step_tolerance(rn, a.eps[c], ir.tau);
       atomicAdd(ir.part_count, 1);
     }
   }
@@ -1122,6 +1127,7 @@ struct Multi {
   size_t f32cap = 0;
   float* f32 = nullptr;      // 5 x n*k floats: B32 D32 R32 P32 V32
   int* irs = nullptr;        // part, done, status, outer, inner_total (kMaxRhs each), part_count
+  double* irtau = nullptr;   // inner tolerance per column
   double* dstate2 = nullptr; // inner-solve scalars
   int* istate2 = nullptr;
 };
@@ -1140,6 +1146,7 @@ void multi_free(Multi* m) {
   cudaFree(m->istate);
   cudaFree(m->f32);
   cudaFree(m->irs);
+  cudaFree(m->irtau);
   cudaFree(m->dstate2);
   cudaFree(m->istate2);
   delete m;
@@ -1373,7 +1380,8 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
   float* P32 = R32 + nk;
   float* V32 = P32 + nk;
   const float* J32 = m->jacobi32;
-  const MOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps, ai, ir.part, ir.part_count};
+  const MOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps, ai, ir.part, ir.part_count,
+                          ir.tau_col};
   int st = launch_mtile(h, n, k, pre);
   if (!st)
     st = launch_spmm_f32(h, m->csr, k, D32, MEpiInit<float>{B32, R32, P32, J32, k, ai});
@@ -1419,6 +1427,7 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
   }
   if (!mu->irs) {
     CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
+    CELG_CUDA(cudaMalloc(&mu->irtau, sizeof(double) * kMaxRhs));
     CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 7 * kMaxRhs));
     CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 2)));
   }
@@ -1435,6 +1444,8 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
   ir.inner_total = ir.outer + kMaxRhs;
   ir.part_count = ir.inner_total + kMaxRhs;
   ir.outer_max = p->outer_max > 0 ? p->outer_max : 20;
+  ir.tau_col = mu->irtau;
+  ir.tau = inner_eps;
   const MultiArgs a = multi_args(mu->dstate, mu->istate, k, p->iter_max, 0, h->err_d);
   const MultiArgs ai_host = multi_args(mu->dstate2, mu->istate2, k, inner_max, 0, h->err_d);
   if (mu->tuned_mat != (const void*)m || mu->tuned_n != (int)n || mu->tuned_k != k) {

@@ -140,6 +140,7 @@ struct EpiRuResidual {
 // sweep, which read p anyway, so this sweep reads neither d nor p.
 struct OpRuStep {
   static constexpr int NRED = 2;
+  static constexpr int kTilesPerPass = 2;
   struct Regs { float r, v, J; };
   float* r;
   const float* v;
@@ -230,6 +231,7 @@ struct OpRuFlush {
 // while the solve goes on.  The last CTA clears the mark.
 struct OpRuDirection {
   static constexpr int NRED = 0;
+  static constexpr int kTilesPerPass = 2;
   static constexpr bool kFinishAlways = true;
   struct Regs { float p, r, J, d; };
   float* p;

@@ -26,11 +26,23 @@ struct all_lanes : std::false_type {};
 template <class T>
 struct all_lanes<T, std::void_t<decltype(T::kAllLanes)>> : std::integral_constant<bool, T::kAllLanes> {};
 
+// An op with `static constexpr int kTilesPerPass = 2` has each CTA take two
+// of its tiles (k and k + grid) per pass: the loads of both are issued before
+// any arithmetic, and their reductions share the barriers of one fold.  Every
+// tile is still reduced on its own, in the same order.
+template <class T, class = void>
+struct tiles_per_pass : std::integral_constant<int, 1> {};
+template <class T>
+struct tiles_per_pass<T, std::void_t<decltype(T::kTilesPerPass)>>
+    : std::integral_constant<int, T::kTilesPerPass> {};
+
 template <class Op>
 __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx red) {
   constexpr int NR = Op::NRED;
   constexpr bool kB = is_batched<Op>::value;
-  __shared__ double scratch[8];
+  constexpr int TP = kB ? 1 : tiles_per_pass<Op>::value;
+  constexpr int NF = (NR > 0 ? NR : 1) * TP;
+  __shared__ double scratch[8 * NF];
   __shared__ int s_flag;
   Op op = op_in;
   if (!op.prepare()) return;
@@ -41,39 +53,71 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   if constexpr (kB) {
     if (blockIdx.x < ntiles) nxt = op.tile_info(tile_at(blockIdx.x, ntiles, sweep));
   }
-  for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
-    const long t = tile_at(k, ntiles, sweep);
+  for (long k = blockIdx.x; k < ntiles; k += (long)TP * gridDim.x) {
+    long t[TP];
+    bool on[TP];
+#pragma unroll
+    for (int p = 0; p < TP; ++p) {
+      const long kp = k + (long)p * gridDim.x;
+      on[p] = kp < ntiles;
+      t[p] = on[p] ? tile_at(kp, ntiles, sweep) : 0;
+    }
     if constexpr (kB) {
       const TileInfo cur = nxt;
       if (k + gridDim.x < ntiles) nxt = op.tile_info(tile_at(k + gridDim.x, ntiles, sweep));
       if (!cur.act) continue;
       op.begin_tile(cur);
     }
-    Acc<NR> acc;
+    double acc[TP][NR > 0 ? NR : 1];
 #pragma unroll
-    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
-    typename Op::Regs regs[4];
-    const long base = t * kTile + j;
+    for (int p = 0; p < TP; ++p)
+#pragma unroll
+      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[p][r] = 0.0;
+    typename Op::Regs regs[TP][4];
     if constexpr (all_lanes<Op>::value) {
       // every lane takes part (rows past n included: the op guards them), so
       // ops may exchange values between lanes with warp shuffles
 #pragma unroll
-      for (int k = 0; k < 4; ++k) op.load(base + (long)k * kLanes, regs[k]);
+      for (int p = 0; p < TP; ++p)
+        if (on[p])
 #pragma unroll
-      for (int k = 0; k < 4; ++k) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+          for (int q = 0; q < 4; ++q) op.load(t[p] * kTile + j + (long)q * kLanes, regs[p][q]);
+#pragma unroll
+      for (int p = 0; p < TP; ++p)
+        if (on[p])
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            op.compute(t[p] * kTile + j + (long)q * kLanes, regs[p][q], acc[p]);
     } else {
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (base + (long)k * kLanes < n) op.load(base + (long)k * kLanes, regs[k]);
+      for (int p = 0; p < TP; ++p)
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (base + (long)k * kLanes < n) op.compute(base + (long)k * kLanes, regs[k], acc.a);
+        for (int q = 0; q < 4; ++q) {
+          const long i = t[p] * kTile + j + (long)q * kLanes;
+          if (on[p] && i < n) op.load(i, regs[p][q]);
+        }
+#pragma unroll
+      for (int p = 0; p < TP; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const long i = t[p] * kTile + j + (long)q * kLanes;
+          if (on[p] && i < n) op.compute(i, regs[p][q], acc[p]);
+        }
     }
     if (NR > 0) {
+      double f[NF];
 #pragma unroll
-      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
-        const double tot = group_fold256(acc.a[r], scratch, j, 1);
-        if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
+      for (int p = 0; p < TP; ++p)
+#pragma unroll
+        for (int r = 0; r < (NR > 0 ? NR : 1); ++r) f[p * (NR > 0 ? NR : 1) + r] = acc[p][r];
+      group_fold256_n<NF>(f, scratch, j, 1);
+      if (j == 0) {
+#pragma unroll
+        for (int p = 0; p < TP; ++p)
+          if (on[p])
+#pragma unroll
+            for (int r = 0; r < (NR > 0 ? NR : 1); ++r)
+              red.partials[(long)r * red.ntiles + t[p]] = f[p * (NR > 0 ? NR : 1) + r];
       }
       // batched: the systems are completed by batch_finish_kernel
     }

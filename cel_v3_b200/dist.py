@@ -277,9 +277,48 @@ class GpuRank:
     def x(self):
         return self.x_ext[:self.block.n]
 
+    def exchange_plan(self):
+        """The block's exchange lists as celg_dist_set_exchange takes them:
+        neighbours in ascending order, the local rows each one reads and the
+        halo range it provides."""
+        blk = self.block
+        peers = blk.neighbours()
+        return (peers, [blk.send.get(q, np.zeros(0, np.int64)) for q in peers],
+                [blk.recv.get(q, (0, 0)) for q in peers])
+
+    def solve(self, allreduce_sum, halo, poll_every=8):
+        """The whole solve in one library call (celg_dist_pcg_solve), the
+        exchanges done by the callables allreduce_sum(buf_d, count, stream)
+        and halo(vec_ext_d, stream)."""
+        return self.d.solve(allreduce_sum, halo, self.b.data_ptr(), self.x_ext.data_ptr(),
+                            poll_every, history=self.hist is not None)
+
+    def solve_nccl(self, nccl_comm, poll_every=8, overlap=False):
+        """The whole solve in one library call over NCCL
+        (celg_dist_pcg_solve_nccl) with this block's exchange plan."""
+        self.d.set_exchange(*self.exchange_plan())
+        return self.d.solve_nccl(nccl_comm, self.b.data_ptr(), self.x_ext.data_ptr(), poll_every,
+                                 overlap, history=self.hist is not None)
+
     def close(self):
         self.d.destroy()
         self.mat.destroy()
+
+
+def nccl_communicator(rank, world, device):
+    """The library's own NCCL communicator over the ranks of the default
+    torch.distributed group: rank 0 makes the unique id, a broadcast on the
+    group carries it to the others (celg_nccl_unique_id,
+    celg_nccl_comm_create).  Release it with celgpu.nccl_comm_destroy."""
+    import torch
+    import torch.distributed as td
+    from . import celgpu
+    uid = celgpu.nccl_unique_id() if rank == 0 else bytes(celgpu.NCCL_ID_BYTES)
+    if world > 1:
+        t = torch.tensor(list(uid), dtype=torch.uint8, device=torch.device("cuda", device))
+        td.broadcast(t, 0)
+        uid = bytes(t.cpu().tolist())
+    return celgpu.nccl_comm_create(uid, world, rank, device)
 
 
 def iterate(ranks, comm, count, overlap=False):

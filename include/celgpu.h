@@ -30,6 +30,7 @@ extern "C" {
 #define CELG_ERR_NOCONV 4     /* iteration limit reached before tolerance  */
 #define CELG_ERR_TIMEOUT 5    /* a device-side bounded wait gave up        */
 #define CELG_ERR_STATE 6      /* call out of order (e.g. DoIt before MatrixCompleted) */
+#define CELG_ERR_COMM 7       /* an exchange between ranks (callback or NCCL) failed */
 
 /* ---- formats and modes (mv_algorithm, src/fbase/cel_types_module.f90:58-81) */
 #define CELG_FMT_CSR 0
@@ -68,7 +69,10 @@ typedef struct {
   int precision;        /* CELG_PREC_*                                           */
   int literal_ref_bugs; /* CG: alpha-as-beta (:151); GMRES: unrotated Givens (:722-727) */
   int restart;          /* GMRES(m): m (gmres_max_restart)                      */
-  double inner_eps_rel; /* FP32-IR: inner PCG relative tolerance (default 1e-4);
+  double inner_eps_rel; /* FP32-IR: tightest inner PCG relative tolerance
+                         (default 1e-4; a single-system refinement step asks
+                         for the looser tolerance that spreads the remaining
+                         reduction evenly over the steps it needs);
                          FP32-RU: residual drop that triggers an FP64 update */
   int inner_iter_max;   /* FP32-IR: inner iteration cap                         */
   int outer_max;        /* FP32-IR: refinement steps cap                        */
@@ -333,6 +337,52 @@ int celg_dist_pcg_poll(celg_dist* d, int* active, int* iter);
 int celg_dist_pcg_verify(celg_dist* d, const double* b_d, const double* x_ext_d);      /* [R] */
 /* synchronises; returns the solve status, fills res (history from hist_d) */
 int celg_dist_pcg_result(celg_dist* d, celg_result* res);
+
+/* ---- distributed Jacobi-PCG in one call ------------------------------------------- */
+/* The whole solve of one rank, with the exchanges inside the call as in the
+ * reference: the halo of p before every SpMV (cel_fop_mv_axy_distr,
+ * src/fop/cel_fop_mv_module.f90:48-81) and a sum all-reduce per reduction
+ * phase (the MPI_ALLREDUCE in every cel_fop_vec_distr_* dot,
+ * src/fop/cel_fop_vec_distr_module.f90:419-832; the communicator the ELM API
+ * takes, src/felmsolver/cel_elmsolver_module.f90:103).  It runs the phase
+ * sequence above on work vectors the celg_dist object keeps; the caller's
+ * part is the start vector x_ext_d (ncols entries, local part used with
+ * CELG_X0_USER) and b_d.  The host polls the stopping flag every poll_every
+ * iterations (queued iterations after convergence do no work).  res as
+ * celg_dist_pcg_result.  Every rank must make the same calls.
+ *
+ * Exchanges through the caller's communication layer: each callback
+ * enqueues its work on `stream` (the handle's stream) or finishes it before
+ * returning, and returns 0 on success (anything else ends the solve with
+ * CELG_ERR_COMM).  allreduce_sum sums `count` doubles at buf_d (device)
+ * over all ranks, in place; halo sends this rank's rows that other ranks
+ * read and receives their values into entries n..ncols-1 of vec_ext_d. */
+typedef struct {
+  void* ctx;
+  int (*allreduce_sum)(void* ctx, double* buf_d, int count, void* stream);
+  int (*halo)(void* ctx, double* vec_ext_d, void* stream);
+} celg_dist_comm;
+int celg_dist_pcg_solve(celg_dist* d, const celg_dist_comm* comm, const double* b_d,
+                        double* x_ext_d, int poll_every, celg_result* res);
+/* The same with the library running the exchanges over NCCL (libnccl.so.2,
+ * loaded on first use; CELG_ERR_STATE when it cannot be loaded).  The
+ * exchange plan lists, per neighbour (nneigh of them): its rank, the
+ * send_counts[q] local rows (0-based, concatenated over the neighbours in
+ * send_rows) whose values it reads, and the recv_counts[q] halo entries it
+ * provides, which land at vec_ext_d[n + recv_starts[q] ...].  A communicator
+ * comes from celg_nccl_comm_create on every rank with the unique id that
+ * one rank made with celg_nccl_unique_id (the caller broadcasts it).
+ * overlap != 0 sends the halo of p on a side stream while the interior
+ * rows' SpMV runs (celg_dist_pcg_ap_interior / _boundary). */
+#define CELG_NCCL_ID_BYTES 128
+int celg_dist_set_exchange(celg_dist* d, int nneigh, const int* peers, const int* send_counts,
+                           const int* send_rows, const int* recv_starts, const int* recv_counts);
+int celg_nccl_unique_id(unsigned char id[CELG_NCCL_ID_BYTES]);
+int celg_nccl_comm_create(const unsigned char id[CELG_NCCL_ID_BYTES], int nranks, int rank,
+                          int device, void** nccl_comm);
+int celg_nccl_comm_destroy(void* nccl_comm);
+int celg_dist_pcg_solve_nccl(celg_dist* d, void* nccl_comm, const double* b_d, double* x_ext_d,
+                             int poll_every, int overlap, celg_result* res);
 
 /* ---- allocation-free entry point ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot allocate device

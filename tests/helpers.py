@@ -30,3 +30,18 @@ def spd_from_pattern(rp, ci, v):
     A = (A * -0.5 + sp.diags(d)).tocsr()
     A.sort_indices()
     return A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data.astype(np.float64)
+
+
+def ir_step_tolerance(rn, tol, tau):
+    """Inner tolerance of an FP32-refinement step (ir_step_tolerance in
+    cel_v3_b200/csrc/celg_device.cuh): the goal g = tol / (2 rn) if one
+    inner solve at tau reaches it, sqrt(g) if two do, else tau."""
+    import math
+    if not (tol > 0 and rn > tol and 0 < tau < 1 and rn < 1e308):
+        return tau
+    g = tol / (2.0 * rn)
+    if tau <= g:
+        return g
+    if tau * tau <= g:
+        return max(math.sqrt(g), tau)
+    return tau

@@ -6,6 +6,7 @@ import pytest
 
 from cel_v3_b200 import synth
 from oracle import celref as R
+from tests.helpers import ir_step_tolerance
 
 pytestmark = pytest.mark.gpu
 
@@ -155,10 +156,10 @@ def mirror_ir(rp, ci, v, B, eps_rel, inner_eps, inner_max, outer_max):
     spmm32 = lambda X: np.stack([R.spmv_csr_f32(rp, ci, v32, X[:, c]) for c in range(k)], 1)
     D = lambda a: a.astype(f64)
 
-    def inner(B32, part):
+    def inner(B32, part, taus):
         X = np.zeros((n, k), f32)
         bn = np.sqrt(dot_cols(D(B32), D(B32)))
-        eps = inner_eps * bn
+        eps = taus * bn
         Rr = (D(B32) - D(f32(0) + spmm32(X))).astype(f32)
         Z = D(Rr) * D(J32)[:, None]
         P = Z.astype(f32)
@@ -206,9 +207,11 @@ def mirror_ir(rp, ci, v, B, eps_rel, inner_eps, inner_max, outer_max):
         if not part.any():
             break
         B32 = np.zeros((n, k), f32)
+        taus = np.full(k, inner_eps)
         for c in np.flatnonzero(part):
             B32[:, c] = (Rr[:, c] * (1.0 / rn[c])).astype(f32)
-        Dd, its = inner(B32, part)
+            taus[c] = ir_step_tolerance(rn[c], tol[c], inner_eps)
+        Dd, its = inner(B32, part, taus)
         for c in np.flatnonzero(part):
             inner_total[c] += its[c]
             outer[c] += 1

@@ -85,6 +85,39 @@ def test_spmv_f32_bitexact(gpu, name):
     m.destroy()
 
 
+def banded_dictionary_csr(n=5017, seed=7):
+    """Rows of 14..18 entries (one empty row) whose column offsets come from a
+    fixed set of 40, so the FP32 copy has a 1-byte offset dictionary: the
+    FP32 dictionary sweep with rows longer than one 8-entry chunk."""
+    rng = np.random.default_rng(seed)
+    offs = np.sort(rng.choice(np.arange(-60, 61), size=40, replace=False))
+    cols = []
+    for i in range(n):
+        ok = offs[(i + offs >= 0) & (i + offs < n)]
+        k = 0 if i == 100 else min(ok.size, int(rng.integers(14, 19)))
+        cols.append(np.sort(i + rng.choice(ok, size=k, replace=False)))
+    rp = np.concatenate([[0], np.cumsum([c.size for c in cols])]).astype(np.int32)
+    ci = np.concatenate(cols).astype(np.int32)
+    return rp, ci, rng.standard_normal(ci.size)
+
+
+def test_spmv_f32_dictionary_long_rows_bitexact(gpu):
+    celgpu, h, torch = gpu
+    rp, ci, v = banded_dictionary_csr()
+    n = rp.size - 1
+    x = np.random.default_rng(5).standard_normal(n).astype(np.float32)
+    m = h.matrix_from_csr(rp, ci, v).jacobi().make_fp32()
+    yd = dev(torch, np.full(n, 7.0, np.float32))
+    h.spmv_f32(m, dev(torch, x).data_ptr(), yd.data_ptr())
+    y = R.spmv_csr_f32(rp, ci, v.astype(np.float32), x)
+    assert np.array_equal(yd.cpu().numpy(), y)
+    assert yd[100].item() == 0.0                       # the empty row
+    h.spmv_f32(m, dev(torch, x).data_ptr(), yd.data_ptr(), accumulate=True)
+    assert np.array_equal(yd.cpu().numpy(), R.spmv_csr_f32(rp, ci, v.astype(np.float32), x, y=y,
+                                                           accumulate=True))
+    m.destroy()
+
+
 @pytest.mark.parametrize("name", sorted(MATS))
 def test_jad_conversion_and_spmv_bitexact(gpu, name):
     celgpu, h, torch = gpu
