@@ -346,6 +346,9 @@ def batch_form(h, celgpu, torch, stream):
                                                     out["one_by_one"]["solves_per_s"])
     out["systems"] = len(mats)
     out["rows"] = int(sum(s ** 3 for s, *_ in probs))
+    csr_ctas, sweep_ctas = h.tuned_config(celgpu.TUNE_BATCH)
+    out["tuned_launch"] = {"spmv_ctas_per_sm": csr_ctas or "max resident",
+                           "vector_sweep_ctas_per_sm": sweep_ctas}
     for m in mats:
         m.destroy()
     return out
@@ -388,6 +391,7 @@ def multirhs_form(h, celgpu, torch, stream):
             X64 = Xd.clone()
         elif name == "multirhs_fp32_ir":
             out[name]["worst_err_vs_fp64"] = max(rel_err(Xd[:, c], X64[:, c]) for c in range(k))
+    out["tuned_spmm_variant"] = h.tuned_config(celgpu.TUNE_SPMM)[0]
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_multirhs_fp32_ir_vs_one_by_one"] = (out["multirhs_fp32_ir"]["solves_per_s"] /
                                                      out["one_by_one"]["solves_per_s"])

@@ -40,6 +40,8 @@ ERR_COMM = 7
 
 FMT_CSR = 0
 FMT_JAD = 1
+TUNE_BATCH = 0
+TUNE_SPMM = 1
 PRECOND_JACOBI = 0
 PRECOND_BLOCK_JACOBI = 1
 
@@ -171,6 +173,7 @@ def _load():
         "celg_nccl_comm_create": (i, [vp, i, i, i, ctypes.POINTER(vp)]),
         "celg_nccl_comm_destroy": (i, [vp]),
         "celg_dist_pcg_solve_nccl": (i, [vp, vp, vp, vp, i, i, ctypes.POINTER(Result)]),
+        "celg_tuned_config": (i, [vp, i, ip]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -681,6 +684,14 @@ class Handle:
                                   ctypes.byref(p), ctypes.byref(res))
         _check(st, "celg_pcg_adjoint", allow=(ERR_NOCONV,))
         return _info(res, None, st)
+
+    def tuned_config(self, what):
+        """celg_tuned_config: the autotuner's pick for the last batched
+        (TUNE_BATCH: (SpMV CTAs per SM, vector-sweep CTAs per SM)) or
+        multi-RHS (TUNE_SPMM: (variant, -1)) solve."""
+        out = (ctypes.c_int * 2)()
+        _check(lib.celg_tuned_config(self.ptr, int(what), out), "celg_tuned_config")
+        return out[0], out[1]
 
     def diffusion7_face_grad(self, nx, ny, nz, lambda_d, x_d, gkx_d, gky_d, gkz_d):
         _check(lib.celg_diffusion7_face_grad(self.ptr, int(nx), int(ny), int(nz),

@@ -144,8 +144,7 @@ __global__ void offset_index_kernel(int n, const int* __restrict__ rp, const int
 
 // Build ci8/dict (1-byte column offsets col - row); leaves them unset when the matrix has
 // more than kDictMax distinct offsets.
-static int build_offset_dict(celg_handle* h, celg_mat* m) {
-  CsrDev& A = m->csr;
+int build_offset_dict_csr(celg_handle* h, CsrDev& A) {
   cudaFree(A.ci8);
   cudaFree(A.dict);
   A.ci8 = nullptr;
@@ -184,7 +183,7 @@ static int build_offset_dict(celg_handle* h, celg_mat* m) {
 int ensure_offset_dict(celg_handle* h, celg_mat* m) {
   if (m->csr.ci8 || m->dict_tried) return CELG_OK;
   m->dict_tried = true;
-  return build_offset_dict(h, m);
+  return build_offset_dict_csr(h, m->csr);
 }
 
 void free_mat_arrays(celg_mat* m) {
@@ -260,7 +259,9 @@ static int build_jad(celg_mat* m) {
     if ((e = cudaMalloc(&key, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
     if ((e = cudaMalloc(&key2, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
     if ((e = cudaMalloc(&idx, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
-    if ((e = cudaMalloc(&J.perm, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
+    // perm carries 8 spare entries: the staged JAD sweep copies a sub-tile's
+    // perm entries rounded up to 4
+    if ((e = cudaMalloc(&J.perm, sizeof(int) * ((size_t)n + 8))) != cudaSuccess) { fail(e, "jad"); break; }
     cudaMemsetAsync(maxlen_d, 0, sizeof(int), h->stream);
     if (n > 0) row_len_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, m->csr.rp, key, idx, maxlen_d);
     cudaMemcpyAsync(&mmax, maxlen_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream);

@@ -476,6 +476,8 @@ struct Batch {
   double* dstate = nullptr;    // 7 x nsys doubles
   int* istate = nullptr;       // 3 x nsys ints + n_active + nsys pending marks
   int nlive = 0;               // systems with at least one row
+  // launch shape picked by batch_tune (index into kBatchShapes, -1: not tuned)
+  int shape = -1;
   std::vector<long> row_off;
   std::vector<int> n;
   // FP32 refinement (allocated on first use): A.v32 holds the FP32 values
@@ -494,6 +496,8 @@ void batch_free(Batch* b) {
   cudaFree(b->A.rp);
   cudaFree(b->A.ci);
   cudaFree(b->A.v);
+  cudaFree(b->A.ci8);
+  cudaFree(b->A.dict);
   cudaFree(b->J);
   cudaFree(b->B);
   cudaFree(b->tile_arrays);
@@ -597,12 +601,45 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
     return cuda_status(e, "batch assembly");
   }
   int st = csr_compute_cap(h, A);
+  // 1-byte column offsets when the systems together use at most 256
+  // distinct offsets col - row (7-point systems: -1, 0, 1 and +-side,
+  // +-side^2 per distinct side): 9 instead of 12 bytes per non-zero
+  if (!st) st = build_offset_dict_csr(h, A);
   if (st) {
     batch_free(bt);
     return st;
   }
   *out = bt;
   return CELG_OK;
+}
+
+// Launch shapes the batch tuner chooses from: resident CTAs per SM of the
+// CSR sweep (0: as many as fit) and of the vector sweeps.  None changes a
+// result: every tile is reduced on its own, whichever CTA takes it.
+struct BatchShape {
+  int csr_per_sm, tile_per_sm;
+};
+constexpr BatchShape kBatchShapes[] = {{0, 8}, {0, 6}, {0, 4}, {2, 8}, {2, 4}, {1, 8}};
+constexpr int kNumBatchShapes = (int)(sizeof(kBatchShapes) / sizeof(kBatchShapes[0]));
+
+static BatchShape batch_shape(const Batch* bt) {
+  return kBatchShapes[bt->shape >= 0 && bt->shape < kNumBatchShapes ? bt->shape : 0];
+}
+
+// A CSR sweep over the concatenated systems, with the 1-byte column offsets
+// when the batch has them (same values in the same order, same sums).
+template <typename VT, class Epi>
+static int batch_csr(celg_handle* h, const Batch* bt, const VT* vals, const VT* x, const Epi& epi) {
+  const int cap = batch_shape(bt).csr_per_sm;
+  if (bt->A.ci8)
+    return launch_csr_ct<VT, uint8_t>(h, bt->A, vals, bt->A.ci8, bt->A.cap_dict, x, epi, nullptr, cap);
+  return launch_csr_ct<VT, int>(h, bt->A, vals, bt->A.ci, bt->A.cap, x, epi, nullptr, cap);
+}
+
+// A vector sweep over the concatenated systems.
+template <class Op>
+static int batch_tile(celg_handle* h, const Batch* bt, const Op& op) {
+  return launch_tile(h, bt->N, op, batch_shape(bt).tile_per_sm);
 }
 
 static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle cond, const int* errw,
@@ -650,9 +687,79 @@ static int clear_marks(celg_handle* h, const BatchArgs& a) {
   return CELG_OK;
 }
 
+// x0, ||b||, eps, then r = b - A x, p = J r and the first scalars per system
+static int batch_setup(celg_handle* h, Batch* bt, int x0_mode, double eps_abs, double eps_rel,
+                       const BatchArgs& a) {
+  const BOpPre<double> pre{bt->B, bt->X, x0_mode, eps_abs, eps_rel, a};
+  int st = launch_tile(h, bt->N, pre);
+  if (!st) st = batch_finish(h, bt, pre);
+  if (!st) st = batch_csr<double>(h, bt, bt->A.v, bt->X, BEpiInit<double>{bt->B, bt->R, bt->P, bt->J, a});
+  if (!st) st = batch_finish(h, bt, BEpiInit<double>{bt->B, bt->R, bt->P, bt->J, a});
+  return st;
+}
+
+// One iteration of every running system: K1, sigma, K2, beta and the test,
+// K3 (with the deferred x update), then the pending marks cleared.
+static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a) {
+  const BEpiAp<double> ap{bt->V, bt->P, a};
+  const BOpUpdate<double> upd{bt->R, bt->V, bt->J, a, 0.0};
+  int s2 = batch_csr<double>(h, bt, bt->A.v, bt->P, ap);
+  if (!s2) s2 = batch_finish(h, bt, ap);
+  if (!s2) s2 = batch_tile(h, bt, upd);
+  if (!s2) s2 = batch_finish(h, bt, upd);
+  if (!s2) s2 = batch_tile(h, bt, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
+  if (!s2) s2 = clear_marks(h, a);
+  return s2;
+}
+
+// The batch tuner: times a few iterations of the batch's own systems with
+// each launch shape of kBatchShapes and keeps the fastest for the batch
+// (CELG_BATCH_SHAPE=0..5 forces one).  It starts from x0 = 0 in the batch's
+// work vectors, so the caller's vectors are neither read beyond b nor
+// written; the solve that follows sets everything up again.
+static int batch_tune(celg_handle* h, Batch* bt, const double* const* b_d) {
+  if (bt->shape >= 0) return CELG_OK;
+  if (const char* e = std::getenv("CELG_BATCH_SHAPE")) {
+    const int v = std::atoi(e);
+    bt->shape = (v >= 0 && v < kNumBatchShapes) ? v : 0;
+    return CELG_OK;
+  }
+  for (int s = 0; s < bt->nsys; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(bt->B + bt->row_off[s], b_d[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+  }
+  // no iteration cap, so that every system keeps running through the timing
+  const BatchArgs a = batch_args(bt, 1 << 30, 0, h->err_d);
+  cudaEvent_t e0, e1;
+  CELG_CUDA(cudaEventCreate(&e0));
+  CELG_CUDA(cudaEventCreate(&e1));
+  float best = 0.f;
+  int best_shape = 0, st = CELG_OK;
+  for (int c = 0; c < kNumBatchShapes && !st; ++c) {
+    bt->shape = c;
+    st = batch_setup(h, bt, CELG_X0_ZERO, 0.0, 0.0, a);
+    if (!st) st = batch_iteration(h, bt, a);  // warm-up
+    if (st) break;
+    cudaEventRecord(e0, h->stream);
+    for (int k = 0; k < 4 && !st; ++k) st = batch_iteration(h, bt, a);
+    cudaEventRecord(e1, h->stream);
+    if (cudaEventSynchronize(e1) != cudaSuccess) st = CELG_ERR_CUDA;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (!st && (c == 0 || ms < best)) {
+      best = ms;
+      best_shape = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  bt->shape = best_shape;
+  return st;
+}
+
 static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
                           const celg_params* p, BatchArgs a) {
-  const long N = bt->N;
   for (int s = 0; s < bt->nsys; ++s) {
     if (bt->n[s] == 0) continue;
     CELG_CUDA(cudaMemcpyAsync(bt->B + bt->row_off[s], b_d[s], sizeof(double) * (size_t)bt->n[s],
@@ -661,23 +768,8 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
       CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
                                 cudaMemcpyDeviceToDevice, h->stream));
   }
-  const BOpPre<double> pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
-  const BEpiInit<double> init{bt->B, bt->R, bt->P, bt->J, a};
-  const BEpiAp<double> ap{bt->V, bt->P, a};
-  const BOpUpdate<double> upd{bt->R, bt->V, bt->J, a, 0.0};
-  int st = launch_tile(h, N, pre);
-  if (!st) st = batch_finish(h, bt, pre);
-  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, init);
-  if (!st) st = batch_finish(h, bt, init);
-  auto body = [&]() -> int {
-    int s2 = launch_csr<double>(h, bt->A, bt->A.v, bt->P, ap);
-    if (!s2) s2 = batch_finish(h, bt, ap);
-    if (!s2) s2 = launch_tile(h, N, upd);
-    if (!s2) s2 = batch_finish(h, bt, upd);
-    if (!s2) s2 = launch_tile(h, N, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
-    if (!s2) s2 = clear_marks(h, a);
-    return s2;
-  };
+  int st = batch_setup(h, bt, p->x0_mode, p->eps_abs, p->eps_rel, a);
+  auto body = [&]() -> int { return batch_iteration(h, bt, a); };
   if (!st && a.cond) st = capture_while2(h, a.cond, body);
   for (int it = 0; !st && !a.cond && it < p->iter_max; it += 8) {
     for (int q = 0; q < 8 && !st; ++q) st = body();
@@ -689,7 +781,7 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
     if (!live) break;
   }
   const BEpiVerify ver{bt->B, a};
-  if (!st) st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, ver);
+  if (!st) st = batch_csr<double>(h, bt, bt->A.v, bt->X, ver);
   if (!st) st = batch_finish(h, bt, ver);
   if (st) return st;
   for (int s = 0; s < bt->nsys; ++s) {
@@ -738,6 +830,7 @@ int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* 
   char buf[64];
   const std::string& mkey = bt->key;
   st = ensure_partials(h, bt->NT, 2);
+  if (!st) st = batch_tune(h, bt, b_d);
   if (st) return st;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
   std::string gkey = mkey;
@@ -860,15 +953,15 @@ static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, Ba
   const BOpUpdate<float> upd{R32, V32, bt->J32, ai, 0.0};
   int st = launch_tile(h, N, pre);
   if (!st) st = batch_finish(h, bt, pre);
-  if (!st) st = launch_csr<float>(h, bt->A, bt->A.v32, D32, init);
+  if (!st) st = batch_csr<float>(h, bt, bt->A.v32, D32, init);
   if (!st) st = batch_finish(h, bt, init);
   if (!st)
     st = run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
-      int s2 = launch_csr<float>(h, bt->A, bt->A.v32, P32, ap);
+      int s2 = batch_csr<float>(h, bt, bt->A.v32, P32, ap);
       if (!s2) s2 = batch_finish(h, bt, ap);
-      if (!s2) s2 = launch_tile(h, N, upd);
+      if (!s2) s2 = batch_tile(h, bt, upd);
       if (!s2) s2 = batch_finish(h, bt, upd);
-      if (!s2) s2 = launch_tile(h, N, BOpDirection<float>{P32, R32, bt->J32, D32, ai});
+      if (!s2) s2 = batch_tile(h, bt, BOpDirection<float>{P32, R32, bt->J32, D32, ai});
       if (!s2) s2 = clear_marks(h, ai);
       return s2;
     });
@@ -880,6 +973,7 @@ static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, cons
   Batch* bt = nullptr;
   int st = batch_for(h, count, mats, b_d, x_d, &bt);
   if (!st) st = ensure_partials(h, bt->NT, 2);
+  if (!st) st = batch_tune(h, bt, b_d);
   if (!st) st = batch_ensure_f32(h, bt);
   if (st) return st;
   const long N = bt->N;
@@ -925,7 +1019,7 @@ static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, cons
     CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * (size_t)c, h->stream));
     CELG_CUDA(cudaMemsetAsync(ir.part_count, 0, sizeof(int), h->stream));
     const BEpiIrResidual res_op{bt->B, bt->R, a, ir};
-    st = launch_csr<double>(h, bt->A, bt->A.v, bt->X, res_op);
+    st = batch_csr<double>(h, bt, bt->A.v, bt->X, res_op);
     if (!st) st = batch_finish(h, bt, res_op);
     if (st) break;
     int parts = 0;
@@ -1005,4 +1099,23 @@ extern "C" int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats
     if (mats[s] && mats[s]->csr.ncols != mats[s]->csr.n) return CELG_ERR_ARG;  // square systems only
   CELG_CUDA(cudaSetDevice(h->device));
   return celg::pcg_batched(h, count, mats, b_d, x_d, p, res);
+}
+
+extern "C" int celg_tuned_config(celg_handle* h, int what, int out[2]) {
+  if (!h || !out) return CELG_ERR_ARG;
+  out[0] = out[1] = -1;
+  if (what == CELG_TUNE_BATCH) {
+    if (!h->batch || h->batch->shape < 0) return CELG_ERR_STATE;
+    const celg::BatchShape sh = celg::kBatchShapes[h->batch->shape];
+    out[0] = sh.csr_per_sm;
+    out[1] = sh.tile_per_sm;
+    return CELG_OK;
+  }
+  if (what == CELG_TUNE_SPMM) {
+    const int cfg = celg::multi_tuned_cfg(h->multi);
+    if (cfg < 0) return CELG_ERR_STATE;
+    out[0] = cfg;
+    return CELG_OK;
+  }
+  return CELG_ERR_ARG;
 }

@@ -174,6 +174,8 @@ int ensure_f32(celg_handle* h, size_t n);
 // Build the 1-byte column offsets of the matrix once (no-op when built,
 // attempted before, or the matrix has more than 256 column offsets).
 int ensure_offset_dict(celg_handle* h, celg_mat* m);
+// the same for any CSR array set (left unset beyond 256 distinct offsets)
+int build_offset_dict_csr(celg_handle* h, CsrDev& A);
 int alloc_csr(celg_mat* m, int n, int nnz, int ncols);
 int finish_csr(celg_handle* h, celg_mat* m, int base);
 void free_mat_arrays(celg_mat* m);
@@ -187,5 +189,6 @@ void dist_solve_free(void* solve);
 void batch_free(::Batch* b);
 void multi_free(::Multi* m);
 void multi_forget_matrix(::Multi* m, const void* mat);
+int multi_tuned_cfg(::Multi* m);  // the SpMM variant the tuner picked, -1 if none
 
 }  // namespace celg

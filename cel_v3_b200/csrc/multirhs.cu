@@ -1135,6 +1135,8 @@ struct Multi {
 namespace celg {
 
 // a destroyed matrix's address may be reused: drop its tuning record
+int multi_tuned_cfg(Multi* m) { return (m && m->tuned_mat) ? m->cfg : -1; }
+
 void multi_forget_matrix(Multi* m, const void* mat) {
   if (m && m->tuned_mat == mat) m->tuned_mat = nullptr;
 }

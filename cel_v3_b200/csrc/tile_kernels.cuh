@@ -192,9 +192,10 @@ struct TileWindow {
   long partials_cap = 0;
 };
 
+// max_per_sm > 0 caps the resident CTAs per SM (the batched solves' tuner).
 template <typename VT, typename CT, class Epi>
 int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* cols, int cap,
-                  const VT* x, const Epi& epi, const TileWindow* win = nullptr) {
+                  const VT* x, const Epi& epi, const TileWindow* win = nullptr, int max_per_sm = 0) {
   const long nt = ntiles_of(A.n);
   RedCtx red{nullptr, h->ticket, nt};
   long nvis = nt;
@@ -229,6 +230,7 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
   per_sm = std::max(1, per_sm);
+  if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
   const int grid = (int)std::max(1L, std::min(nvis, (long)h->sms * per_sm));
   kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, cols, vals, A.n, cap, x, epi, red, h->err_d,
                                                sizeof(CT) == 1 ? A.dict : nullptr,
@@ -257,6 +259,20 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
+  if (J.mmax <= kJadStageMax) {
+    // the diagonals of each 256-row sub-tile staged by bulk copies
+    red.sweep = next_sweep(h, true);
+    const int smem = kCsrHeader + 64 + kStages * jad_stage_bytes(J.mmax);
+    auto kern = jad_tma_kernel<Epi>;
+    CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    int per_sm = 0;
+    CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
+    const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * std::max(1, per_sm)));
+    kern<<<grid, kCsrThreads, smem, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
+                                                 red, h->err_d);
+    CELG_CUDA(cudaGetLastError());
+    return CELG_OK;
+  }
   red.sweep = next_sweep(h, false);
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi>>(kLanes, 0)));
   jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,

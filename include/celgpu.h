@@ -262,6 +262,16 @@ int celg_check_bounded_wait(celg_handle* h, int limit_ms, int* status);
 int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
                       const celg_params* p, celg_result* res);
 
+/* The launch configuration the autotuners picked on this handle, for the
+ * last batched solve (what = CELG_TUNE_BATCH: out[0] = resident CTAs per SM
+ * of the SpMV sweep, 0 meaning as many as fit; out[1] = CTAs per SM of the
+ * vector sweeps) or multi-right-hand-side solve (what = CELG_TUNE_SPMM:
+ * out[0] = the SpMM variant, 0..14).  No counterpart in the reference, which
+ * has no autotuner.  CELG_ERR_STATE before the first such solve. */
+#define CELG_TUNE_BATCH 0
+#define CELG_TUNE_SPMM 1
+int celg_tuned_config(celg_handle* h, int what, int out[2]);
+
 /* ---- differentiation --------------------------------------------------------- */
 /* Adjoint of a Jacobi-PCG solve x = A^{-1} b (A symmetric): given x_d and
  * g_d = dL/dx, solves A lambda = g with Jacobi-PCG under p (the precision

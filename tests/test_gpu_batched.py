@@ -105,3 +105,34 @@ def test_batched_fp32_refinement_matches_single_refinement(gpu, mode, monkeypatc
         assert np.array_equal(xs[s].cpu().numpy(), xo.cpu().numpy()), s
     for m in mats:
         m.destroy()
+
+
+def test_batched_launch_shapes_give_the_same_bits(gpu, monkeypatch):
+    """Every launch shape the batch tuner chooses from (CTAs per SM of the
+    SpMV and vector sweeps, forced with CELG_BATCH_SHAPE on a fresh handle)
+    gives the same bits, and celg_tuned_config reports the shape in use."""
+    celgpu, h, torch = gpu
+    sy = systems()[:5]
+    kw = dict(eps_rel=1e-9, iter_max=3000, x0_mode=celgpu.X0_ZERO)
+    shapes = [(0, 8), (0, 6), (0, 4), (2, 8), (2, 4), (1, 8)]
+    ref = None
+    for c, shape in enumerate(shapes + [None]):
+        if shape is None:
+            monkeypatch.delenv("CELG_BATCH_SHAPE", raising=False)   # the tuner's own pick
+        else:
+            monkeypatch.setenv("CELG_BATCH_SHAPE", str(c))
+        hq = celgpu.Handle(0, torch.cuda.current_stream().cuda_stream)
+        mats = [hq.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+        bs = [dev(torch, b) for *_, b in sy]
+        xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+        infos = hq.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], **kw)
+        got = hq.tuned_config(celgpu.TUNE_BATCH)
+        assert got in shapes and (shape is None or got == shape)
+        out = [x.cpu().numpy() for x in xs] + [i.iter_done for i in infos]
+        if ref is None:
+            ref = out
+        for a, b in zip(out, ref):
+            assert np.array_equal(a, b)
+        for m in mats:
+            m.destroy()
+        hq.close()
