@@ -140,18 +140,10 @@ struct BEpiAp {
   __device__ void begin_tile(const TileInfo&) {}
   __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
   __device__ const BatchRed& bred() const { return a.br; }
-  static constexpr bool kDiagX = true;
   __device__ void row(long i, VT s, double* acc) const {
     const VT vi = vadd(VT(0), s);
     v[i] = vi;
     acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
-  }
-  // p(i) from the diagonal entry's gather (the sweep runs on x = p)
-  __device__ void row_x(long i, VT s, bool have, VT xi, const VT* x, double* acc) const {
-    const VT vi = vadd(VT(0), s);
-    v[i] = vi;
-    const VT pi = (have && x == p) ? xi : __ldg(p + i);
-    acc[0] = dadd(acc[0], dmul(D(vi), D(pi)));
   }
   __device__ void finish_sys(int s, double* tot) const {
     const double sg = a.alpha[s] / tot[0];

@@ -141,18 +141,10 @@ struct DEpiAp {
   const double* p;
   DistArgs a;
   __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
-  static constexpr bool kDiagX = true;
   __device__ void row(long i, double s, double* acc) const {
     const double vi = dadd(0.0, s);
     v[i] = vi;
     acc[0] = dadd(acc[0], dmul(vi, __ldg(p + i)));
-  }
-  // p(i) from the diagonal entry's gather (the sweep runs on x = p)
-  __device__ void row_x(long i, double s, bool have, double xi, const double* x,
-                        double* acc) const {
-    const double vi = dadd(0.0, s);
-    v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(vi, (have && x == p) ? xi : __ldg(p + i)));
   }
   __device__ void finish(double* tot) const { xch_store(a.st, a, 0.0, 0.0, 0.0, tot[0]); }
 };

@@ -1027,7 +1027,7 @@ static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::
   auto kern = spmm_vec_kernel<Epi, MINB, U, RP>;
   const int rs = 4 * RP;
   const int smem = 8 * (rs * 32 * (int)sizeof(VT) + (sizeof(VT) == 8 ? rs * 64 * 8 : 0));
-  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (const int st = allow_dynamic_smem<spmm_vec_kernel<Epi, MINB, U, RP>>(smem)) return st;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
@@ -1052,7 +1052,7 @@ static int launch_spmm_async(celg_handle* h, const CsrDev& A, int k, const doubl
   if (A.n == 0) return CELG_OK;
   auto kern = spmm_async_kernel<Epi, S, MINB>;
   const int smem = 8 * S * kAsyncSlot * (int)sizeof(double);
-  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (const int st = allow_dynamic_smem<spmm_async_kernel<Epi, S, MINB>>(smem)) return st;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
@@ -1068,7 +1068,7 @@ static int launch_spmm_pair(celg_handle* h, const CsrDev& A, int k, const double
   if (A.n == 0) return CELG_OK;
   auto kern = spmm_pair_kernel<Epi, S, MINB>;
   const int smem = 8 * S * kPairSlot * (int)sizeof(double);
-  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (const int st = allow_dynamic_smem<spmm_pair_kernel<Epi, S, MINB>>(smem)) return st;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));

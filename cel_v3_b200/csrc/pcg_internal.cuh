@@ -168,7 +168,6 @@ struct EpiAp {
   VT* v;
   const VT* p;
   PcgArgs a;
-  static constexpr bool kDiagX = true;
   __device__ bool active() const { return *(volatile int*)&a.st->active != 0; }
   // p(i) is loaded after the row's gathers: issued before them it cost 23 us
   // per 256^3 sweep (290 -> 267 us)
@@ -176,14 +175,6 @@ struct EpiAp {
     const VT vi = vadd(VT(0), s);
     v[i] = vi;
     acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
-  }
-  // p(i) is the x the sweep gathered for the row's diagonal entry (the sweep
-  // runs on x = p); loaded only for a row without a stored diagonal
-  __device__ void row_x(long i, VT s, bool have, VT xi, const VT* x, double* acc) const {
-    const VT vi = vadd(VT(0), s);
-    v[i] = vi;
-    const VT pi = (have && x == p) ? xi : __ldg(p + i);
-    acc[0] = dadd(acc[0], dmul(D(vi), D(pi)));
   }
   __device__ void finish(double* tot) const {
     PcgState* st = a.st;

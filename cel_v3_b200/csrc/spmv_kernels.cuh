@@ -53,16 +53,6 @@ struct Acc {
   double a[N > 0 ? N : 1];
 };
 
-// An epilogue with `static constexpr bool kDiagX = true` takes x(i) of its
-// row through row_x(i, sum, have, xi, x, acc): the sweep hands over the x
-// value it gathered for the row's diagonal entry (have = the row stores its
-// diagonal), so that an epilogue that needs x(i) -- p(i) of p.v, x being p --
-// does not load it a second time after the gathers.
-template <class T, class = void>
-struct takes_diag_x : std::false_type {};
-template <class T>
-struct takes_diag_x<T, std::void_t<decltype(T::kDiagX)>> : std::integral_constant<bool, T::kDiagX> {};
-
 template <typename VT, class Epi, typename CT = int>
 __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT) == 1 ? 3 : 2))
     csr_tma_kernel(const int* __restrict__ rp, const CT* __restrict__ ci,
@@ -98,17 +88,6 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
     for (int q = threadIdx.x; q < ndict; q += blockDim.x) s_dict[q] = dict[q];
   }
   __syncthreads();
-  // the dictionary index of the diagonal (offset 0; the dictionary is
-  // ascending), -1 when no row stores its diagonal
-  [[maybe_unused]] int zc = -1;
-  if constexpr (kDict && takes_diag_x<Epi>::value) {
-    int lo = 0, hi = ndict - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (s_dict[mid] < 0) lo = mid + 1; else hi = mid;
-    }
-    if (ndict > 0 && s_dict[lo] == 0) zc = lo;
-  }
 
   const int sweep = red.sweep;
   if (warp == kConsumerWarps) {
@@ -217,8 +196,6 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       if (row < n) {
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
-        [[maybe_unused]] VT xd = VT(0);  // x(row) from the diagonal entry's gather
-        [[maybe_unused]] bool hd = false;
         if (kDict && sizeof(VT) == 4 && !fb) {
           // FP32 with 1-byte column offsets: the gathers address x from the
           // row's base (one dictionary lookup and one add per entry), and the
@@ -228,25 +205,12 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
           const VT* xr = x + row;
           for (int k = b - a0, ke = e - a0; k < ke; k += 8) {
             VT xv[8];
-            [[maybe_unused]] int cc[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-              if (k + u < ke) {
-                const int c = cis[k + u];
-                if constexpr (takes_diag_x<Epi>::value) cc[u] = c;
-                xv[u] = __ldg(xr + s_dict[c]);
-              }
+              if (k + u < ke) xv[u] = __ldg(xr + s_dict[cis[k + u]]);
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-              if (k + u < ke) {
-                sum = vadd(sum, vmul(vs[k + u], xv[u]));
-                if constexpr (takes_diag_x<Epi>::value) {
-                  if (cc[u] == zc) {
-                    xd = xv[u];
-                    hd = true;
-                  }
-                }
-              }
+              if (k + u < ke) sum = vadd(sum, vmul(vs[k + u], xv[u]));
           }
         } else if (!fb) {
           // chunks of 8 entries: all gathers of a chunk are issued before the
@@ -254,34 +218,22 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
           // the adds stay in stored order
           for (int k = b - a0, ke = e - a0; k < ke; k += 8) {
             VT xv[8], vv[8];
-            [[maybe_unused]] bool dg[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
               if (k + u < ke) {
                 vv[u] = vs[k + u];
-                const int col = entry_col(cis[k + u], row, s_dict);
-                if constexpr (takes_diag_x<Epi>::value) dg[u] = col == (int)row;
-                xv[u] = __ldg(x + col);
+                xv[u] = __ldg(x + entry_col(cis[k + u], row, s_dict));
               }
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-              if (k + u < ke) {
-                sum = vadd(sum, vmul(vv[u], xv[u]));
-                if constexpr (takes_diag_x<Epi>::value) {
-                  if (dg[u]) {
-                    xd = xv[u];
-                    hd = true;
-                  }
-                }
-              }
+              if (k + u < ke) sum = vadd(sum, vmul(vv[u], xv[u]));
           }
         } else {
           for (int k = b; k < e; ++k)
             sum = vadd(sum, vmul(__ldg(v + k), __ldg(x + entry_col(__ldg(ci + k), row, s_dict))));
         }
-        if constexpr (takes_diag_x<Epi>::value) ep.row_x(row, sum, hd, xd, x, acc.a);
-        else ep.row(row, sum, acc.a);
+        ep.row(row, sum, acc.a);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[st]);

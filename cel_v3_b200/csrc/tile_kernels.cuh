@@ -13,6 +13,7 @@
 // in flight per thread, and the reduction order is the oracle's.
 #pragma once
 #include <algorithm>
+#include <mutex>
 
 #include "celg_internal.h"
 #include "spmv_kernels.cuh"
@@ -132,6 +133,25 @@ __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx r
   }
 }
 
+// Allow `bytes` of dynamic shared memory for a kernel on the current device.
+// The attribute belongs to the function, shared by every handle and thread
+// of the process, so it is only ever raised (under a lock): a launch of
+// another handle that needs less is never left above the attribute.
+template <auto Kern>
+int allow_dynamic_smem(int bytes) {
+  static std::mutex mu;
+  static int allowed[64] = {};
+  int dev = 0;
+  CELG_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  const int slot = dev >= 0 && dev < 64 ? dev : 0;
+  if (bytes > allowed[slot] || dev >= 64) {
+    CELG_CUDA(cudaFuncSetAttribute(Kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    allowed[slot] = bytes;
+  }
+  return CELG_OK;
+}
+
 // Resident CTAs per SM of a kernel at a fixed block size and dynamic shared
 // memory (queried once per kernel).
 template <auto Kern>
@@ -226,7 +246,7 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   red.sweep = next_sweep(h, true);
   const int smem = csr_smem_bytes(cap, (int)sizeof(VT), (int)sizeof(CT));
   auto kern = csr_tma_kernel<VT, Epi, CT>;
-  CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  if (const int st = allow_dynamic_smem<csr_tma_kernel<VT, Epi, CT>>(smem)) return st;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
   per_sm = std::max(1, per_sm);
@@ -264,7 +284,7 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
     red.sweep = next_sweep(h, true);
     const int smem = kCsrHeader + 64 + kStages * jad_stage_bytes(J.mmax);
     auto kern = jad_tma_kernel<Epi>;
-    CELG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    if (const int st = allow_dynamic_smem<jad_tma_kernel<Epi>>(smem)) return st;
     int per_sm = 0;
     CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
     const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * std::max(1, per_sm)));
