@@ -259,9 +259,7 @@ static int build_jad(celg_mat* m) {
     if ((e = cudaMalloc(&key, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
     if ((e = cudaMalloc(&key2, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
     if ((e = cudaMalloc(&idx, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
-    // perm carries 8 spare entries: the staged JAD sweep copies a sub-tile's
-    // perm entries rounded up to 4
-    if ((e = cudaMalloc(&J.perm, sizeof(int) * ((size_t)n + 8))) != cudaSuccess) { fail(e, "jad"); break; }
+    if ((e = cudaMalloc(&J.perm, sizeof(int) * std::max(1, n))) != cudaSuccess) { fail(e, "jad"); break; }
     cudaMemsetAsync(maxlen_d, 0, sizeof(int), h->stream);
     if (n > 0) row_len_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, m->csr.rp, key, idx, maxlen_d);
     cudaMemcpyAsync(&mmax, maxlen_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream);

@@ -332,163 +332,6 @@ __global__ void __launch_bounds__(kLanes, 3)
   }
 }
 
-// ---- JAD with the jagged diagonals staged by bulk copies --------------------
-//
-// The same work split as jad_kernel (thread j of a CTA computes the permuted
-// rows i = t*1024 + q*256 + j, q = 0..3, of tile t, in that order), with the
-// data of each 256-row sub-tile staged like csr_tma_kernel's: a producer
-// warp copies, per jagged diagonal d that reaches the sub-tile, its column
-// and value entries for those rows (one contiguous run each, the start
-// rounded down to 4 entries) and the sub-tile's perm entries into a
-// kStages-deep shared-memory ring (cp.async.bulk + mbarrier).  A consumer
-// thread issues the x gathers of all of its row's diagonals before the first
-// add; the adds run in diagonal order from 0.0, so the sums are jad_kernel's
-// bit for bit.  Matrices with more than kJadStageMax diagonals use
-// jad_kernel.
-constexpr int kJadStageMax = 8;
-constexpr int kJadSlot = kSub + 8;  // entries per diagonal slot
-
-__host__ __device__ inline int jad_stage_bytes(int mmax) {
-  const int b = kSub * 4 + mmax * kJadSlot * 12;  // perm, then columns, then values
-  return (b + 127) & ~127;
-}
-
-template <class Epi>
-__global__ void __launch_bounds__(kCsrThreads, 2)
-    jad_tma_kernel(const int* __restrict__ jb, const int* __restrict__ jci,
-                   const double* __restrict__ jv, const int* __restrict__ perm, int n, int mmax,
-                   const double* __restrict__ x, Epi epi, RedCtx red, int* err) {
-  constexpr int NR = Epi::NRED;
-  extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* empty = full + kStages;
-  double* scratch = reinterpret_cast<double*>(smem + 128);
-  int* s_flag = reinterpret_cast<int*>(smem + 192);
-  int* s_jb = reinterpret_cast<int*>(smem + kCsrHeader);  // mmax + 1 <= 9 entries
-  unsigned char* stages = smem + kCsrHeader + 64;
-  const int sbytes = jad_stage_bytes(mmax);
-  const int ci_off = kSub * 4, v_off = kSub * 4 + mmax * kJadSlot * 4;
-
-  if (!epi.active()) return;
-  const long ntiles = ((long)n + kTile - 1) / kTile;
-  const long nsub = ((long)n + kSub - 1) / kSub;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], kConsumerWarps);
-    }
-    fence_mbar_init();
-  }
-  for (int d = threadIdx.x; d <= mmax; d += blockDim.x) s_jb[d] = jb[d];
-  __syncthreads();
-  const int sweep = red.sweep;
-
-  if (warp == kConsumerWarps) {
-    // ---------------- producer warp ----------------
-    const uint64_t pol = l2_evict_first_policy();
-    int it = 0;
-    for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
-      const long t = tile_at(k, ntiles, sweep);
-      for (int q = 0; q < kSubPerTile; ++q) {
-        const long s = t * kSubPerTile + q;
-        if (s >= nsub) break;
-        int abort_ = 0;
-        if (lane == 0) {
-          const int st = it % kStages;
-          if (it >= kStages &&
-              !mbar_wait_bounded(&empty[st], (uint32_t)(((it / kStages) - 1) & 1), err)) {
-            abort_ = 1;
-          } else {
-            const int row0 = (int)(s * kSub);
-            const int rows = min(kSub, n - row0);
-            const uint32_t pb = (uint32_t)(((rows + 3) & ~3) * 4);
-            uint32_t bytes = pb;
-            for (int d = 0; d < mmax; ++d) {
-              const int len = s_jb[d + 1] - s_jb[d];
-              if (row0 >= len) break;  // diagonals shorten with d
-              const int start = s_jb[d] + row0;
-              const int a0 = start & ~3, a1 = (start + min(kSub, len - row0) + 3) & ~3;
-              bytes += (uint32_t)(a1 - a0) * 12u;
-            }
-            unsigned char* sb = stages + (size_t)st * sbytes;
-            mbar_arrive_expect_tx(&full[st], bytes);
-            bulk_g2s_hint(sb, perm + row0, pb, &full[st], pol);
-            for (int d = 0; d < mmax; ++d) {
-              const int len = s_jb[d + 1] - s_jb[d];
-              if (row0 >= len) break;
-              const int start = s_jb[d] + row0;
-              const int a0 = start & ~3, a1 = (start + min(kSub, len - row0) + 3) & ~3;
-              bulk_g2s_hint(sb + ci_off + d * kJadSlot * 4, jci + a0, (uint32_t)(a1 - a0) * 4u,
-                            &full[st], pol);
-              bulk_g2s_hint(sb + v_off + d * kJadSlot * 8, jv + a0, (uint32_t)(a1 - a0) * 8u,
-                            &full[st], pol);
-            }
-          }
-        }
-        abort_ = __shfl_sync(0xffffffffu, abort_, 0);
-        if (abort_) return;
-        ++it;
-      }
-    }
-    return;
-  }
-
-  // ---------------- consumer warps ----------------
-  const int j = threadIdx.x;
-  int it = 0;
-  for (long k = blockIdx.x; k < ntiles; k += gridDim.x) {
-    const long t = tile_at(k, ntiles, sweep);
-    Acc<NR> acc;
-#pragma unroll
-    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
-    for (int q = 0; q < kSubPerTile; ++q) {
-      const long s = t * kSubPerTile + q;
-      if (s >= nsub) break;
-      const int st = it % kStages;
-      if (!mbar_wait_bounded(&full[st], (uint32_t)((it / kStages) & 1), err)) return;
-      const unsigned char* sb = stages + (size_t)st * sbytes;
-      const int row0 = (int)(s * kSub);
-      const int i = row0 + j;
-      if (i < n) {
-        double xv[kJadStageMax], vv[kJadStageMax];
-        bool on[kJadStageMax];
-#pragma unroll
-        for (int d = 0; d < kJadStageMax; ++d) {
-          on[d] = d < mmax && i < s_jb[d + 1] - s_jb[d];
-          if (on[d]) {
-            const int start = s_jb[d] + row0;
-            const int e = start - (start & ~3) + j;
-            const int col = reinterpret_cast<const int*>(sb + ci_off + d * kJadSlot * 4)[e];
-            vv[d] = reinterpret_cast<const double*>(sb + v_off + d * kJadSlot * 8)[e];
-            xv[d] = __ldg(x + col);
-          }
-        }
-        double sum = 0.0;
-#pragma unroll
-        for (int d = 0; d < kJadStageMax; ++d)
-          if (on[d]) sum = dadd(sum, dmul(vv[d], xv[d]));
-        const long row = (long)reinterpret_cast<const int*>(sb)[j];
-        epi.row(row, sum, acc.a);
-      }
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&empty[st]);
-      ++it;
-    }
-    if (NR > 0) {
-#pragma unroll
-      for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
-        const double tot = group_fold256(acc.a[r], scratch, j, 1);
-        if (j == 0) red.partials[(long)r * red.ntiles + t] = tot;
-      }
-    }
-  }
-  if constexpr (NR > 0) {
-    double tot[NR > 0 ? NR : 1];
-    if (grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) epi.finish(tot);
-  }
-}
-
 // ---- plain epilogues -------------------------------------------------------
 
 // y = (accumulate ? y : 0) + row sum

@@ -279,20 +279,6 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
     red.partials = h->partials;
   }
   if (A.n == 0) return CELG_OK;
-  if (J.mmax <= kJadStageMax) {
-    // the diagonals of each 256-row sub-tile staged by bulk copies
-    red.sweep = next_sweep(h, true);
-    const int smem = kCsrHeader + 64 + kStages * jad_stage_bytes(J.mmax);
-    auto kern = jad_tma_kernel<Epi>;
-    if (const int st = allow_dynamic_smem<jad_tma_kernel<Epi>>(smem)) return st;
-    int per_sm = 0;
-    CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCsrThreads, smem));
-    const int grid = (int)std::max(1L, std::min(nt, (long)h->sms * std::max(1, per_sm)));
-    kern<<<grid, kCsrThreads, smem, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
-                                                 red, h->err_d);
-    CELG_CUDA(cudaGetLastError());
-    return CELG_OK;
-  }
   red.sweep = next_sweep(h, false);
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi>>(kLanes, 0)));
   jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,

@@ -130,18 +130,29 @@ def test_thread_ranks_one_call_solve_match_cpu_mirror(gpu, world):
     assert res[0].verified_relres == rc[0]["verified_relres"] <= 1.5e-8
 
 
-def test_thread_ranks_unstructured_blocks_iteration_cap(gpu):
+@pytest.mark.parametrize("iter_max", [9, 13])
+def test_thread_ranks_unstructured_blocks_iteration_cap(gpu, iter_max):
     """Unaligned blocks of an unstructured matrix (scattered send lists) and
-    the iteration cap: CELG_ERR_NOCONV on every rank, same bits as the mirror."""
+    an iteration cap: every rank stops at the same step with the status of
+    the phase-by-phase driver (CELG_ERR_NOCONV at the cap; CELG_OK when the
+    reference's absolute guard |r.z| <= 1.1 eps_mach ends the loop there),
+    and the solution has the mirror's bits."""
     celgpu, h, torch = gpu
     from tests.helpers import random_csr, spd_from_pattern
     rp, ci, v = spd_from_pattern(*random_csr(5000, np.random.default_rng(8), max_len=7,
                                              empty_frac=0.0))
     b = np.random.default_rng(9).uniform(-1, 1, 5000)
     blocks = [D.RowBlock(rp, ci, v, D.partition(5000, 3), q) for q in range(3)]
-    x, res = solve_in_threads(celgpu, torch, blocks, b, eps_rel=1e-30, iter_max=13)
-    xc, rc = run_cpu(blocks, b, eps_rel=1e-30, iter_max=13)
-    assert all(r.status == celgpu.ERR_NOCONV and r.iter_done == 13 for r in res)
+    x, res = solve_in_threads(celgpu, torch, blocks, b, eps_rel=1e-30, iter_max=iter_max)
+    xc, rc = run_cpu(blocks, b, eps_rel=1e-30, iter_max=iter_max)
+    ranks = [D.GpuRank(h, blk, b[blk.r0:blk.r1], eps_rel=1e-30, iter_max=iter_max)
+             for blk in blocks]
+    res_p = D.run_pcg(ranks, D.LocalComm(), check_every=4)
+    for r in ranks:
+        r.close()
+    assert [r.status for r in res] == [r.status for r in res_p]
+    assert all(r.iter_done == iter_max == rc[0]["iter_done"] for r in res)
+    assert res[0].status == (celgpu.ERR_NOCONV if iter_max == 9 else celgpu.OK)
     assert np.array_equal(x, xc)
 
 
