@@ -137,7 +137,11 @@ struct EpiRuResidual {
 
 // r -= sigma v ; rz' = r.J r ; ||r||^2 ; update decision.  The iteration's
 // d += sigma p is left pending (s.xpend) for the flush or the direction
-// sweep, which read p anyway, so this sweep reads neither d nor p.
+// sweep, which read p anyway, so this sweep reads neither d nor p.  The
+// FP32 residual is updated in FP32 arithmetic (r + (float)(-sigma) v, each
+// operation rounded once); its dot products stay FP64 on exact products.
+// Done in FP64 and rounded back, the update took three more conversions per
+// element, and the sweep was bound by the conversion rate, not by memory.
 struct OpRuStep {
   static constexpr int NRED = 2;
   static constexpr int kTilesPerPass = 2;
@@ -146,13 +150,13 @@ struct OpRuStep {
   const float* v;
   const float* J;
   RuArgs a;
-  double sg;
+  float nsg;
   __device__ bool prepare() {
     if (*(volatile int*)&a.st->s.active == 0) {
       if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(a.cond, 0);
       return false;
     }
-    sg = a.st->s.sigma;
+    nsg = (float)(-a.st->s.sigma);
     return true;
   }
   __device__ void load(long i, Regs& g) const {
@@ -161,7 +165,7 @@ struct OpRuStep {
     g.J = __ldg(J + i);
   }
   __device__ void compute(long i, Regs& g, double* acc) const {
-    const float ri = (float)dadd((double)g.r, dmul(-sg, (double)g.v));
+    const float ri = fadd(g.r, fmul(nsg, g.v));
     r[i] = ri;
     const double z = dmul((double)ri, (double)g.J);
     acc[0] = dadd(acc[0], dmul((double)ri, z));
@@ -313,7 +317,7 @@ static int ru_body(celg_handle* h, celg_mat* m, const double* b, double* x, RuAr
   }
   PcgArgs pa = a.pcg();
   int st = launch_csr<float>(h, m->csr, m->csr.v32, pv, EpiAp<float>{v, pv, pa});
-  if (!st) st = launch_tile(h, n, OpRuStep{r, v, m->jacobi32, a, 0.0});
+  if (!st) st = launch_tile(h, n, OpRuStep{r, v, m->jacobi32, a, 0.0f});
   auto update = [&]() -> int {
     int s2 = launch_tile(h, n, OpRuFlush{x, d, pv, a, 0});
     if (!s2)

@@ -341,7 +341,7 @@ def ru_oracle(rp, ci, v, b, eps_rel=1e-10, delta=1e-2, iter_max=5000):
         w = R.spmv_csr_f32(rp, ci, v32, p)
         sigma = rz / R.dot(w.astype(f64), p.astype(f64), T)
         d = (d.astype(f64) + sigma * p.astype(f64)).astype(f32)
-        r = (r.astype(f64) + (-sigma) * w.astype(f64)).astype(f32)
+        r = r + f32(-sigma) * w                       # FP32 arithmetic, one rounding each
         z = r.astype(f64) * J32
         rz_new = R.dot(r.astype(f64), z, T)
         norm = np.sqrt(R.dot(r.astype(f64), r.astype(f64), T))
