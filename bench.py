@@ -812,6 +812,8 @@ def run_profile(argv):
     (ncu), with no timing of its own.
 
       spmv SIDE [REPS]          REPS CSR SpMVs, SIDE^3 Poisson
+      jad SIDE [REPS]           REPS JAD SpMVs of the same system
+      gmres SIDE [M]            one GMRES(M)-Jacobi solve to 1e-8
       spmv32 SIDE [REPS]        the same on the FP32 copy (1-byte columns)
       pcg SIDE ITERS [fp64|ru|ir]
                                 one solve capped at ITERS iterations
@@ -855,6 +857,20 @@ def run_profile(argv):
             h.spmv(m, x.data_ptr(), y.data_ptr())
         torch.cuda.synchronize()
         print("spmv", side, float(y.sum()))
+    elif what == "jad":
+        m.to_jad()
+        for _ in range(int(argv[2]) if len(argv) > 2 else 4):
+            h.spmv(m, x.data_ptr(), y.data_ptr(), fmt=celgpu.FMT_JAD)
+        torch.cuda.synchronize()
+        print("jad", side, float(y.sum()))
+    elif what == "gmres":
+        restart = int(argv[2]) if len(argv) > 2 else 30
+        h.spmv(m, x.data_ptr(), y.data_ptr())  # b = A x_true
+        xs = torch.zeros_like(y)
+        info = h.gmres_jacobi(m, y.data_ptr(), xs.data_ptr(), restart=restart, eps_rel=1e-8,
+                              iter_max=2000, x0_mode=celgpu.X0_ZERO)
+        torch.cuda.synchronize()
+        print("gmres", side, restart, info.arnoldi_steps, info.status)
     elif what == "pcg":
         iters = int(argv[2])
         mode = argv[3] if len(argv) > 3 else "fp64"
