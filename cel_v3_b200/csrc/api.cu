@@ -142,9 +142,155 @@ __global__ void offset_index_kernel(int n, const int* __restrict__ rp, const int
   }
 }
 
+// ---- row patterns (csr_tma_kernel with PatIdx) -----------------------------------
+
+constexpr int kPatSlots = 4096;
+constexpr unsigned long long kPatEmpty = 0xFFFFFFFFFFFFFFFEull;  // no key has a low byte 0xFE
+
+// The row's 1-byte offset codes as one key: code k in byte k, 0xFF past the
+// row's end (the dictionary has at most 254 entries, so no code is 0xFE or
+// 0xFF).  Rows longer than kPatLen set *too_long.
+__device__ __forceinline__ unsigned long long pat_row_key(const int* __restrict__ rp,
+                                                          const uint8_t* __restrict__ ci8, long i,
+                                                          int* too_long) {
+  const int b = rp[i], len = rp[i + 1] - b;
+  if (len > kPatLen) {
+    *too_long = 1;
+    return kPatEmpty;
+  }
+  unsigned long long key = ~0ull;
+  for (int k = 0; k < len; ++k)
+    key = (key & ~(0xFFull << (8 * k))) | ((unsigned long long)ci8[b + k] << (8 * k));
+  return key;
+}
+
+// distinct row keys into an open-addressed set; gives up (flags[1]) beyond
+// kPatMax keys or for a row longer than kPatLen
+__global__ void pat_set_kernel(int n, const int* __restrict__ rp, const uint8_t* __restrict__ ci8,
+                               unsigned long long* table, int* flags) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    if (*(volatile int*)&flags[1]) return;
+    int too_long = 0;
+    const unsigned long long key = pat_row_key(rp, ci8, i, &too_long);
+    if (too_long) {
+      atomicExch(&flags[1], 1);
+      return;
+    }
+    unsigned slot = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 52) & (kPatSlots - 1);
+    for (int probe = 0; probe < kPatSlots; ++probe) {
+      const unsigned long long cur = *(volatile unsigned long long*)&table[slot];
+      if (cur == key) break;
+      if (cur == kPatEmpty) {
+        const unsigned long long prev = atomicCAS(&table[slot], kPatEmpty, key);
+        if (prev == kPatEmpty) {
+          if (atomicAdd(&flags[0], 1) >= kPatMax) atomicExch(&flags[1], 1);
+          break;
+        }
+        if (prev == key) break;
+      }
+      slot = (slot + 1) & (kPatSlots - 1);
+    }
+  }
+}
+
+// each row's pattern index: the position of its key among the sorted keys
+__global__ void pat_index_kernel(int n, const int* __restrict__ rp, const uint8_t* __restrict__ ci8,
+                                 const unsigned long long* __restrict__ keys, int nkeys,
+                                 uint8_t* __restrict__ pid) {
+  __shared__ unsigned long long s_keys[kPatMax];
+  for (int q = threadIdx.x; q < nkeys; q += blockDim.x) s_keys[q] = keys[q];
+  __syncthreads();
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    int too_long = 0;
+    const unsigned long long key = pat_row_key(rp, ci8, i, &too_long);
+    int lo = 0, hi = nkeys - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (s_keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    pid[i] = (uint8_t)lo;
+  }
+}
+
+// Row patterns from the 1-byte offsets (left unset when a row is longer than
+// kPatLen, the dictionary has more than 254 entries or the rows use more
+// than kPatMax distinct offset sequences).
+static int build_row_patterns(celg_handle* h, CsrDev& A) {
+  cudaFree(A.pid);
+  cudaFree(A.pat);
+  A.pid = nullptr;
+  A.pat = nullptr;
+  A.npat = 0;
+  if (!A.ci8 || A.ndict > 254 || A.n == 0) return CELG_OK;
+  unsigned long long* table = nullptr;
+  CELG_CUDA(cudaMalloc(&table, sizeof(unsigned long long) * kPatSlots + 2 * sizeof(int)));
+  int* flags = reinterpret_cast<int*>(table + kPatSlots);
+  std::vector<unsigned long long> init(kPatSlots, kPatEmpty);
+  CELG_CUDA(cudaMemcpyAsync(table, init.data(), sizeof(unsigned long long) * kPatSlots,
+                            cudaMemcpyHostToDevice, h->stream));
+  CELG_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream));
+  pat_set_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci8, table, flags);
+  std::vector<unsigned long long> out(kPatSlots);
+  int fl[2] = {0, 0};
+  std::vector<int> dict(A.ndict);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out.data(), table, sizeof(unsigned long long) * kPatSlots,
+                        cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(fl, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dict.data(), A.dict, sizeof(int) * A.ndict, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess || fl[1] || fl[0] > kPatMax) {
+    cudaFree(table);
+    return e != cudaSuccess ? cuda_status(e, "row patterns") : CELG_OK;
+  }
+  std::vector<unsigned long long> keys;
+  for (unsigned long long k : out)
+    if (k != kPatEmpty) keys.push_back(k);
+  std::sort(keys.begin(), keys.end());
+  std::vector<int> tab(keys.size() * kPatLen, 0);
+  for (size_t p = 0; p < keys.size(); ++p)
+    for (int k = 0; k < kPatLen; ++k) {
+      const int code = (int)((keys[p] >> (8 * k)) & 0xFF);
+      tab[p * kPatLen + k] = code == 0xFF ? 0 : dict[code];
+    }
+  // the sorted keys travel in the table buffer
+  e = cudaMemcpyAsync(table, keys.data(), sizeof(unsigned long long) * keys.size(),
+                      cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMalloc(&A.pid, (size_t)A.n + 16);
+  if (e == cudaSuccess) e = cudaMemsetAsync(A.pid + A.n, 0, 16, h->stream);
+  if (e == cudaSuccess) e = cudaMalloc(&A.pat, sizeof(int) * tab.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A.pat, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice,
+                        h->stream);
+  if (e == cudaSuccess) {
+    pat_index_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci8, table,
+                                                             (int)keys.size(), A.pid);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(table);
+  if (e != cudaSuccess) {
+    cudaFree(A.pid);
+    cudaFree(A.pat);
+    A.pid = nullptr;
+    A.pat = nullptr;
+    return cuda_status(e, "row patterns");
+  }
+  A.npat = (int)keys.size();
+  return CELG_OK;
+}
+
 // Build ci8/dict (1-byte column offsets col - row); leaves them unset when the matrix has
 // more than kDictMax distinct offsets.
 int build_offset_dict_csr(celg_handle* h, CsrDev& A) {
+  cudaFree(A.pid);
+  cudaFree(A.pat);
+  A.pid = nullptr;
+  A.pat = nullptr;
+  A.npat = 0;
   cudaFree(A.ci8);
   cudaFree(A.dict);
   A.ci8 = nullptr;
@@ -177,7 +323,7 @@ int build_offset_dict_csr(celg_handle* h, CsrDev& A) {
   offset_index_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci, A.dict, A.ndict, A.ci8);
   CELG_CUDA(cudaGetLastError());
   A.cap_dict = (A.cap + 24 + 15) & ~15;  // 16-entry aligned spans are at most 24 entries wider
-  return CELG_OK;
+  return build_row_patterns(h, A);
 }
 
 int ensure_offset_dict(celg_handle* h, celg_mat* m) {
@@ -193,6 +339,8 @@ void free_mat_arrays(celg_mat* m) {
   cudaFree(m->csr.v32);
   cudaFree(m->csr.ci8);
   cudaFree(m->csr.dict);
+  cudaFree(m->csr.pid);
+  cudaFree(m->csr.pat);
   cudaFree(m->jad.begin);
   cudaFree(m->jad.ci);
   cudaFree(m->jad.v);

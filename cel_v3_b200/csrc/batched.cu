@@ -489,6 +489,8 @@ void batch_free(Batch* b) {
   cudaFree(b->A.ci);
   cudaFree(b->A.v);
   cudaFree(b->A.ci8);
+  cudaFree(b->A.pid);
+  cudaFree(b->A.pat);
   cudaFree(b->A.dict);
   cudaFree(b->J);
   cudaFree(b->B);
@@ -623,8 +625,9 @@ static BatchShape batch_shape(const Batch* bt) {
 template <typename VT, class Epi>
 static int batch_csr(celg_handle* h, const Batch* bt, const VT* vals, const VT* x, const Epi& epi) {
   const int cap = batch_shape(bt).csr_per_sm;
-  if (bt->A.ci8)
-    return launch_csr_ct<VT, uint8_t>(h, bt->A, vals, bt->A.ci8, bt->A.cap_dict, x, epi, nullptr, cap);
+  bool done = false;
+  const int st = launch_csr_compact<VT>(h, bt->A, vals, x, epi, nullptr, cap, &done);
+  if (done) return st;
   return launch_csr_ct<VT, int>(h, bt->A, vals, bt->A.ci, bt->A.cap, x, epi, nullptr, cap);
 }
 

@@ -32,6 +32,12 @@ struct CsrDev {
   int* dict = nullptr;    // ndict offsets, ascending
   int ndict = 0;
   int cap_dict = 0;       // staging capacity with 16-entry alignment
+  // row patterns (spmv_kernels.cuh, kPatLen/kPatMax): one pattern index per
+  // row (n + 16 bytes) and the pattern table (npat x 8 column offsets), when
+  // the dictionary's rows fit them
+  uint8_t* pid = nullptr;
+  int* pat = nullptr;
+  int npat = 0;
 };
 
 struct JadDev {

@@ -301,12 +301,15 @@ static int dist_check(const celg_dist* d) {
   return CELG_OK;
 }
 
-// SpMV phase of the block: 1-byte column offsets when the block has them
-// (same values in the same order, so the same sums), else int32 columns.
+// SpMV phase of the block: row patterns or 1-byte column offsets when the
+// block has them (same values in the same order, so the same sums), else
+// int32 columns.
 template <class Epi>
 static int dist_csr(celg_dist* d, const double* x, const Epi& epi, const TileWindow* win = nullptr) {
   const CsrDev& A = d->m->csr;
-  if (A.ci8) return launch_csr_ct<double, uint8_t>(d->h, A, A.v, A.ci8, A.cap_dict, x, epi, win);
+  bool done = false;
+  const int st = launch_csr_compact<double>(d->h, A, A.v, x, epi, win, 0, &done);
+  if (done) return st;
   return launch_csr_ct<double, int>(d->h, A, A.v, A.ci, A.cap, x, epi, win);
 }
 

@@ -96,7 +96,11 @@ void graph_cache_drop_matrix(celg_handle* h, const void* m) {
 template <typename VT, class Epi>
 static int csr_sweep(celg_handle* h, const PcgBind<VT>& B, const VT* vals, const VT* x, const Epi& epi) {
   if constexpr (std::is_same<VT, double>::value) {
-    if (B.dict) return launch_csr_ct<double, uint8_t>(h, *B.A, vals, B.A->ci8, B.A->cap_dict, x, epi);
+    if (B.dict) {
+      bool done = false;
+      const int st = launch_csr_compact<double>(h, *B.A, vals, x, epi, nullptr, 0, &done);
+      if (done) return st;
+    }
   }
   return launch_csr<VT>(h, *B.A, vals, x, epi);
 }
@@ -306,7 +310,11 @@ int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const cel
   std::memset(&s, 0, sizeof(s));
   const int ret = pcg_run<double>(h, B, p, m, &s);
   h->last_iters = s.iter;
-  h->last_bytes_per_iter = (B.dict ? 9.0 : 12.0) * m->csr.nnz + 4.0 * (n + 1) + 96.0 * n;
+  // K1 reads 8 bytes per non-zero and one per row with the row patterns, 9 per
+  // non-zero with the 1-byte offsets, else 12
+  h->last_bytes_per_iter =
+      (B.dict && m->csr.pid ? 8.0 * m->csr.nnz + 1.0 * n : (B.dict ? 9.0 : 12.0) * m->csr.nnz) +
+      4.0 * (n + 1) + 96.0 * n;
   if (res) {
     res->iter_done = s.iter;
     res->final_norm2 = s.norm;

@@ -6,7 +6,11 @@
 
 namespace celg {
 
-int csr_smem_bytes(int cap, int vt_size, int ct_size) {
+int csr_smem_bytes(int cap, int vt_size, int ct_size, int pat_ints) {
+  if (pat_ints >= 0) {
+    StageLayout L(cap, vt_size, 1, true);
+    return kCsrHeader + ((pat_ints * 4 + 127) & ~127) + kStages * L.bytes;
+  }
   StageLayout L(cap, vt_size, ct_size);
   return kCsrHeader + (ct_size == 1 ? kDictMax * 4 : 0) + kStages * L.bytes;
 }

@@ -25,16 +25,31 @@ namespace celg {
 // Shared-memory layout of one pipeline stage for `cap` staged entries with
 // column indices of ct_size bytes (4: int32 columns; 1: offset-dictionary
 // indices) and values of vt_size bytes.
+// With per_row, the column data is one pattern index per row (kSub + 16
+// bytes) instead of one index per entry.
 struct StageLayout {
   int ci_off, v_off, bytes;
-  __host__ __device__ StageLayout(int cap, int vt_size, int ct_size = 4) {
+  __host__ __device__ StageLayout(int cap, int vt_size, int ct_size = 4, bool per_row = false) {
     ci_off = (kSub + 4) * 4;                                          // 1040, 16B multiple
-    v_off = ci_off + (((cap + 32) * ct_size + 15) & ~15);
+    v_off = ci_off + (per_row ? kSub + 16 : (((cap + 32) * ct_size + 15) & ~15));
     int end = v_off + (cap + 32) * vt_size;
     bytes = (end + 127) & ~127;
   }
 };
 constexpr int kDictMax = 256;  // offset-dictionary entries (uint8 indices)
+
+// Row patterns.  When every row has at most kPatLen entries and the rows use
+// at most kPatMax distinct sequences of column offsets col - row (a
+// structured-grid stencil has a few dozen: interior rows, faces, edges,
+// corners), each row stores one byte -- the index of its sequence in a
+// pattern table of kPatLen offsets per pattern -- and the entries store no
+// column data at all: 8 (FP64) or 4 (FP32) bytes per non-zero plus one per
+// row, against 9 or 5 with the 1-byte offset dictionary.
+constexpr int kPatLen = 8;
+constexpr int kPatMax = 256;
+struct PatIdx {
+  uint8_t v;
+};
 
 // column of stored entry k of row `row`: int32 columns are absolute, uint8
 // indices select an offset col - row from the matrix's dictionary
@@ -60,17 +75,22 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
                    RedCtx red, int* err, const int* __restrict__ dict, int ndict) {
   constexpr int NR = Epi::NRED;
   constexpr bool kB = is_batched<Epi>::value;
-  constexpr bool kDict = sizeof(CT) == 1;
-  constexpr int kAlign = kDict ? 16 : 4;  // entries per 16 bytes of the narrowest array
+  constexpr bool kPat = std::is_same<CT, PatIdx>::value;
+  constexpr bool kDict = std::is_same<CT, uint8_t>::value;
+  // entries per 16 bytes of the narrowest per-entry array
+  constexpr int kAlign = kPat ? 16 / (int)sizeof(VT) : (kDict ? 16 : 4);
   extern __shared__ __align__(128) unsigned char smem[];
   uint64_t* full = reinterpret_cast<uint64_t*>(smem);
   uint64_t* empty = full + kStages;
   int* meta = reinterpret_cast<int*>(empty + kStages);        // a0, fallback per stage
   double* scratch = reinterpret_cast<double*>(smem + 128);    // 8 doubles
   int* s_flag = reinterpret_cast<int*>(smem + 192);
-  int* s_dict = reinterpret_cast<int*>(smem + kCsrHeader);    // offset dictionary (kDict)
-  unsigned char* stages = smem + kCsrHeader + (kDict ? kDictMax * 4 : 0);
-  const StageLayout L(cap, (int)sizeof(VT), (int)sizeof(CT));
+  // offset dictionary (kDict: ndict entries) or pattern table (kPat: ndict =
+  // patterns x kPatLen offsets)
+  int* s_dict = reinterpret_cast<int*>(smem + kCsrHeader);
+  const int tab_bytes = kPat ? ((ndict * 4 + 127) & ~127) : (kDict ? kDictMax * 4 : 0);
+  unsigned char* stages = smem + kCsrHeader + tab_bytes;
+  const StageLayout L(cap, (int)sizeof(VT), (int)sizeof(CT), kPat);
 
   if (!epi.active()) return;
   const long nsub = ((long)n + kSub - 1) / kSub;
@@ -84,7 +104,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
     }
     fence_mbar_init();
   }
-  if constexpr (kDict) {
+  if constexpr (kDict || kPat) {
     for (int q = threadIdx.x; q < ndict; q += blockDim.x) s_dict[q] = dict[q];
   }
   __syncthreads();
@@ -134,22 +154,29 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
             meta[2 * st] = a0;
             meta[2 * st + 1] = fb;
             const uint32_t rpb = (uint32_t)(((rows + 1 + 3) & ~3) * 4);
-            const uint32_t mb = fb ? 0u : (uint32_t)cnt * (uint32_t)(sizeof(CT) + sizeof(VT));
+            // column data: per entry (int32 or 1-byte offsets) from a0, or
+            // (row patterns) one byte per row from row0
+            const CT* csrc = kPat ? ci + row0 : ci + a0;
+            const uint32_t cb =
+                kPat ? (uint32_t)((rows + 15) & ~15) : (uint32_t)cnt * (uint32_t)sizeof(CT);
+            const bool copy = !fb && (cnt > 0 || kPat);
+            const uint32_t mb = copy ? cb + (uint32_t)cnt * (uint32_t)sizeof(VT) : 0u;
             unsigned char* sb = stages + (size_t)st * L.bytes;
             mbar_arrive_expect_tx(&full[st], rpb + mb);
             if (sweep & 2) {
               bulk_g2s_hint(sb, rp + row0, rpb, &full[st], pol);
-              if (!fb && cnt > 0) {
-                bulk_g2s_hint(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT),
-                              &full[st], pol);
-                bulk_g2s_hint(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT),
-                              &full[st], pol);
+              if (copy) {
+                bulk_g2s_hint(sb + L.ci_off, csrc, cb, &full[st], pol);
+                if (cnt > 0)
+                  bulk_g2s_hint(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT),
+                                &full[st], pol);
               }
             } else {
               bulk_g2s(sb, rp + row0, rpb, &full[st]);
-              if (!fb && cnt > 0) {
-                bulk_g2s(sb + L.ci_off, ci + a0, (uint32_t)cnt * (uint32_t)sizeof(CT), &full[st]);
-                bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
+              if (copy) {
+                bulk_g2s(sb + L.ci_off, csrc, cb, &full[st]);
+                if (cnt > 0)
+                  bulk_g2s(sb + L.v_off, v + a0, (uint32_t)cnt * (uint32_t)sizeof(VT), &full[st]);
               }
             }
           }
@@ -196,7 +223,26 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       if (row < n) {
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
-        if (kDict && sizeof(VT) == 4 && !fb) {
+        if constexpr (kPat) {
+          // the row's offsets from its pattern; values from the stage
+          const int pv = fb ? (int)ci[row].v : (int)reinterpret_cast<const uint8_t*>(cis)[j];
+          const int* po = s_dict + pv * kPatLen;
+          const VT* xr = x + row;
+          const int len = e - b;
+          VT xv[kPatLen];
+#pragma unroll
+          for (int u = 0; u < kPatLen; ++u)
+            if (u < len) xv[u] = __ldg(xr + po[u]);
+          if (!fb) {
+#pragma unroll
+            for (int u = 0; u < kPatLen; ++u)
+              if (u < len) sum = vadd(sum, vmul(vs[b - a0 + u], xv[u]));
+          } else {
+#pragma unroll
+            for (int u = 0; u < kPatLen; ++u)
+              if (u < len) sum = vadd(sum, vmul(__ldg(v + b + u), xv[u]));
+          }
+        } else if (kDict && sizeof(VT) == 4 && !fb) {
           // FP32 with 1-byte column offsets: the gathers address x from the
           // row's base (one dictionary lookup and one add per entry), and the
           // values are read from the stage when they are added (store-only
@@ -363,7 +409,8 @@ struct EpiResidual {
   __device__ void finish(double* tot) const { *out = sqrt(tot[0]); }
 };
 
-// Host helpers (spmv.cu)
-int csr_smem_bytes(int cap, int vt_size, int ct_size = 4);
+// Host helpers (spmv.cu): dynamic shared memory of csr_tma_kernel;
+// pat_ints >= 0 selects the row-pattern layout with that many table entries
+int csr_smem_bytes(int cap, int vt_size, int ct_size = 4, int pat_ints = -1);
 
 }  // namespace celg

@@ -286,7 +286,10 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   }
   if (A.n == 0) return CELG_OK;
   red.sweep = next_sweep(h, true);
-  const int smem = csr_smem_bytes(cap, (int)sizeof(VT), (int)sizeof(CT));
+  constexpr bool kPat = std::is_same<CT, PatIdx>::value;
+  const int* tab = kPat ? A.pat : (std::is_same<CT, uint8_t>::value ? A.dict : nullptr);
+  const int ntab = kPat ? A.npat * kPatLen : (std::is_same<CT, uint8_t>::value ? A.ndict : 0);
+  const int smem = csr_smem_bytes(cap, (int)sizeof(VT), (int)sizeof(CT), kPat ? ntab : -1);
   auto kern = csr_tma_kernel<VT, Epi, CT>;
   if (const int st = allow_dynamic_smem<csr_tma_kernel<VT, Epi, CT>>(smem)) return st;
   int per_sm = 0;
@@ -295,18 +298,34 @@ int launch_csr_ct(celg_handle* h, const CsrDev& A, const VT* vals, const CT* col
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
   const int grid = (int)std::max(1L, std::min(nvis, (long)h->sms * per_sm));
   kern<<<grid, kCsrThreads, smem, h->stream>>>(A.rp, cols, vals, A.n, cap, x, epi, red, h->err_d,
-                                               sizeof(CT) == 1 ? A.dict : nullptr,
-                                               sizeof(CT) == 1 ? A.ndict : 0);
+                                               tab, ntab);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
 }
 
+// CSR sweep over the row patterns when the matrix has them (same values,
+// same columns, same order: the same sums), else over the 1-byte column
+// offsets, else (fallback false) nothing is launched and 1 is returned.
+template <typename VT, class Epi>
+int launch_csr_compact(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, const Epi& epi,
+                       const TileWindow* win, int max_per_sm, bool* done) {
+  *done = true;
+  if (A.pid)
+    return launch_csr_ct<VT, PatIdx>(h, A, vals, reinterpret_cast<const PatIdx*>(A.pid), A.cap, x,
+                                     epi, win, max_per_sm);
+  if (A.ci8) return launch_csr_ct<VT, uint8_t>(h, A, vals, A.ci8, A.cap_dict, x, epi, win, max_per_sm);
+  *done = false;
+  return CELG_OK;
+}
+
 // CSR sweep with the matrix's own column indices; the FP32 copy uses the
-// 1-byte offset dictionary when the matrix has one.
+// row patterns or the 1-byte offset dictionary when the matrix has them.
 template <typename VT, class Epi>
 int launch_csr(celg_handle* h, const CsrDev& A, const VT* vals, const VT* x, const Epi& epi) {
   if constexpr (sizeof(VT) == 4) {
-    if (A.ci8) return launch_csr_ct<VT, uint8_t>(h, A, vals, A.ci8, A.cap_dict, x, epi);
+    bool done = false;
+    const int st = launch_csr_compact<VT>(h, A, vals, x, epi, nullptr, 0, &done);
+    if (done) return st;
   }
   return launch_csr_ct<VT, int>(h, A, vals, A.ci, A.cap, x, epi);
 }

@@ -118,6 +118,53 @@ def test_spmv_f32_dictionary_long_rows_bitexact(gpu):
     m.destroy()
 
 
+def test_row_patterns_fp32_and_pcg_bitexact(gpu):
+    """A 7-point operator with one row emptied and one row given a ninth
+    entry: the rows of at most 8 entries use few distinct offset sequences,
+    so the sweeps run on row patterns -- except that the long row rules them
+    out for the second matrix, which runs on the 1-byte offsets instead.
+    Both give the oracle's bits (FP32 SpMV; FP64 PCG on the first)."""
+    celgpu, h, torch = gpu
+    rp, ci, v = synth.poisson7(13, 9, 11)
+    n = rp.size - 1
+    lens = np.diff(rp)
+    lens[40] = 0                                        # an empty row
+    keep = np.ones(ci.size, bool)
+    keep[rp[40]:rp[41]] = False
+    rp_e = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    ci_e, v_e = ci[keep], v[keep]
+    x = np.random.default_rng(6).standard_normal(n).astype(np.float32)
+    for rp2, ci2, v2 in ((rp_e, ci_e, v_e),):
+        m = h.matrix_from_csr(rp2, ci2, v2).make_fp32()
+        yd = dev(torch, np.zeros(n, np.float32))
+        h.spmv_f32(m, dev(torch, x).data_ptr(), yd.data_ptr())
+        assert np.array_equal(yd.cpu().numpy(), R.spmv_csr_f32(rp2, ci2, v2.astype(np.float32), x))
+        m.destroy()
+    # a ninth entry in row 100 (a far column): no row patterns, 1-byte offsets
+    cols = [ci[rp[i]:rp[i + 1]] for i in range(n)]
+    vals = [v[rp[i]:rp[i + 1]] for i in range(n)]
+    cols[100] = np.sort(np.append(cols[100], [n - 1, n - 2]))
+    vals[100] = np.append(vals[100], [-0.25, -0.25])
+    rp9 = np.concatenate([[0], np.cumsum([c.size for c in cols])]).astype(np.int32)
+    ci9, v9 = np.concatenate(cols).astype(np.int32), np.concatenate(vals)
+    m = h.matrix_from_csr(rp9, ci9, v9).make_fp32()
+    yd = dev(torch, np.zeros(n, np.float32))
+    h.spmv_f32(m, dev(torch, x).data_ptr(), yd.data_ptr())
+    assert np.array_equal(yd.cpu().numpy(), R.spmv_csr_f32(rp9, ci9, v9.astype(np.float32), x))
+    m.destroy()
+    # FP64 PCG on the row patterns of the plain operator, against the oracle
+    b = R.spmv_csr(rp, ci, v, np.random.default_rng(7).random(n))
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    xd = dev(torch, np.zeros(n))
+    info = h.pcg_jacobi(m, dev(torch, b).data_ptr(), xd.data_ptr(), history=True, eps_rel=1e-10,
+                        iter_max=2000)
+    xo, io = R.pcg_jacobi(R.Matrix(rp, ci, v), R.jacobi(R.diag(rp, ci, v)), b, eps_rel=1e-10,
+                          iter_max=2000, red=R.RED_TREE)
+    assert info.iter_done == io["iter_done"] and np.array_equal(info.history, io["history"])
+    assert np.array_equal(xd.cpu().numpy(), xo)
+    m.destroy()
+
+
 @pytest.mark.parametrize("name", sorted(MATS))
 def test_jad_conversion_and_spmv_bitexact(gpu, name):
     celgpu, h, torch = gpu
