@@ -489,13 +489,18 @@ __device__ __forceinline__ void vacc(float4& s, float v, const float4& x) {
 // and the epilogue's loads and stores stay coalesced.  RP > 1 gives a warp
 // more gathers in flight at fewer resident CTAs, which keeps the rows of X in
 // use by all CTAs together within L2.
-template <class Epi, int MINB, int U, int RP>
+// PAT: the matrix's row patterns (pid, pat; spmv_kernels.cuh) give each
+// entry's column as row + offset, so the X gathers need no column load.
+template <class Epi, int MINB, int U, int RP, bool PAT>
 __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __restrict__ rp,
                                                                const int* __restrict__ ci,
                                                                const typename Epi::VT* __restrict__ v,
                                                                int n, int k,
                                                                const typename Epi::VT* __restrict__ X,
-                                                               Epi epi, RedCtx red) {
+                                                               Epi epi, RedCtx red,
+                                                               const uint8_t* __restrict__ pid,
+                                                               const int* __restrict__ pat,
+                                                               int pat_ints) {
   using VT = typename Epi::VT;
   using V16 = typename Vec16<VT>::T;
   constexpr int NR = Epi::NRED;
@@ -528,6 +533,11 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __res
   constexpr int kWarpDoubles = RS * 32 * (int)sizeof(VT) / 8 + (kStaged ? RS * 64 : 0);
   VT* sw = reinterpret_cast<VT*>(s_dyn + (long)warp * kWarpDoubles);
   double* sp = s_dyn + (long)warp * kWarpDoubles + RS * 32 * (int)sizeof(VT) / 8;
+  [[maybe_unused]] int* s_pat = reinterpret_cast<int*>(s_dyn + 8L * kWarpDoubles);
+  if constexpr (PAT) {
+    for (int q = threadIdx.x; q < pat_ints; q += blockDim.x) s_pat[q] = pat[q];
+    __syncthreads();
+  }
   const long ntiles = ((long)n + kTile - 1) / kTile;
   for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
     const long t = tile_at(kt, ntiles, red.sweep);
@@ -551,12 +561,14 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __res
             if (on && s0 + rr < nrows) pre[rr] = epi.pre(row0 + s0 + rr, lane);
         }
         int b[RP], e[RP];
+        [[maybe_unused]] const int* po[RP];
         int lmax = 0;
 #pragma unroll
         for (int j = 0; j < RP; ++j) {
           const int r = s0 + g + 4 * j;
           b[j] = r < nrows ? __ldg(rp + row0 + r) : 0;
           e[j] = r < nrows ? __ldg(rp + row0 + r + 1) : 0;
+          if constexpr (PAT) po[j] = s_pat + (r < nrows ? (int)__ldg(pid + row0 + r) : 0) * kPatLen;
           lmax = max(lmax, e[j] - b[j]);
         }
         V16 sum[RP][NV];
@@ -572,7 +584,10 @@ __global__ void __launch_bounds__(kLanes, MINB) spmm_vec_kernel(const int* __res
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               const int kk = b[j] + c0 + u;
-              cc[j][u] = kk < e[j] ? __ldg(ci + kk) : 0;
+              if constexpr (PAT)
+                cc[j][u] = kk < e[j] ? (int)(row0 + s0 + g + 4 * j) + po[j][c0 + u] : 0;
+              else
+                cc[j][u] = kk < e[j] ? __ldg(ci + kk) : 0;
               vv[j][u] = kk < e[j] ? __ldg(v + kk) : VT(0);
             }
           V16 xg[RP][U][NV];
@@ -1016,24 +1031,36 @@ static int launch_spmm_cfg(celg_handle* h, const CsrDev& A, const typename Epi::
   return CELG_OK;
 }
 
-template <class Epi, int MINB, int U, int RP>
-static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
-                           const typename Epi::VT* X, const Epi& epi) {
+template <class Epi, int MINB, int U, int RP, bool PAT>
+static int launch_spmm_vec_p(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
+                             const typename Epi::VT* X, const Epi& epi) {
   using VT = typename Epi::VT;
   const long nt = ntiles_of(A.n);
   RedCtx red{h->partials, h->ticket, nt};
   if (A.n == 0) return CELG_OK;
   red.sweep = next_sweep(h, false);
-  auto kern = spmm_vec_kernel<Epi, MINB, U, RP>;
+  auto kern = spmm_vec_kernel<Epi, MINB, U, RP, PAT>;
   const int rs = 4 * RP;
-  const int smem = 8 * (rs * 32 * (int)sizeof(VT) + (sizeof(VT) == 8 ? rs * 64 * 8 : 0));
-  if (const int st = allow_dynamic_smem<spmm_vec_kernel<Epi, MINB, U, RP>>(smem)) return st;
+  const int pat_ints = PAT ? A.npat * kPatLen : 0;
+  const int smem =
+      8 * (rs * 32 * (int)sizeof(VT) + (sizeof(VT) == 8 ? rs * 64 * 8 : 0)) + pat_ints * 4;
+  if (const int st = allow_dynamic_smem<spmm_vec_kernel<Epi, MINB, U, RP, PAT>>(smem)) return st;
   int per_sm = 0;
   CELG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kLanes, smem));
   const int grid = grid_for_tiles(h, nt, std::max(1, per_sm));
-  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, vals, A.n, k, X, epi, red);
+  kern<<<grid, kLanes, smem, h->stream>>>(A.rp, A.ci, vals, A.n, k, X, epi, red, A.pid, A.pat,
+                                          pat_ints);
   CELG_CUDA(cudaGetLastError());
   return CELG_OK;
+}
+
+// The 16-byte-gather SpMM, on the row patterns when the matrix has them
+// (same columns in the same order: the same sums).
+template <class Epi, int MINB, int U, int RP>
+static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::VT* vals, int k,
+                           const typename Epi::VT* X, const Epi& epi) {
+  if (A.pid) return launch_spmm_vec_p<Epi, MINB, U, RP, true>(h, A, vals, k, X, epi);
+  return launch_spmm_vec_p<Epi, MINB, U, RP, false>(h, A, vals, k, X, epi);
 }
 
 // SpMM of the FP32 inner solve: the 16-byte-gather kernel when k is a
@@ -1218,6 +1245,9 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
 
 int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
                  const celg_params* p, celg_result* res) {
+  // row patterns (or 1-byte offsets) of the matrix, before the SpMM variants
+  // are timed: the 16-byte-gather SpMM reads them instead of the columns
+  if (const int st = ensure_offset_dict(h, m)) return st;
   if (p->precision == CELG_PREC_FP32_IR) return multirhs_ir(h, m, k, B, X, p, res);
   if (p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
   const long n = m->csr.n;
