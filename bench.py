@@ -175,8 +175,13 @@ def plain_large_form(h, celgpu, torch, stream, m, b, x, iters_csr):
         xs = torch.from_numpy(np.random.default_rng(1).random(n)).cuda()
         ys = torch.zeros(n, dtype=torch.float64, device="cuda")
         row = {}
+        # JAD reads no column data when the matrix has row patterns: 8 bytes
+        # per non-zero and one pattern byte per row instead of 12
+        pat = mm.column_form() == celgpu.COLS_PATTERN
+        jad_bytes = (8 * nnz + n if pat else 12 * nnz) + 4 * 8 + 20 * n
+        row["jad_columns"] = "row patterns" if pat else "int32"
         for name, fmt, nbytes in (("csr", celgpu.FMT_CSR, 12 * nnz + 4 * (n + 1) + 16 * n),
-                                  ("jad", celgpu.FMT_JAD, 12 * nnz + 4 * 8 + 20 * n)):
+                                  ("jad", celgpu.FMT_JAD, jad_bytes)):
             ms, _ = time_it(lambda: h.spmv(mm, xs.data_ptr(), ys.data_ptr(), fmt=fmt), 50)
             gbs = nbytes / (ms / 1e3) / 1e9
             row[name] = {"ms": ms, "gbs": gbs, "frac_of_measured": gbs / peak, "bytes": nbytes}

@@ -40,6 +40,7 @@ ERR_COMM = 7
 
 FMT_CSR = 0
 FMT_JAD = 1
+COLS_INT32, COLS_OFFSET8, COLS_PATTERN = 0, 1, 2
 TUNE_BATCH = 0
 TUNE_SPMM = 1
 PRECOND_JACOBI = 0
@@ -174,6 +175,7 @@ def _load():
         "celg_nccl_comm_destroy": (i, [vp]),
         "celg_dist_pcg_solve_nccl": (i, [vp, vp, vp, vp, i, i, ctypes.POINTER(Result)]),
         "celg_tuned_config": (i, [vp, i, ip]),
+        "celg_mat_column_form": (i, [vp, ip]),
     }
     for name, (res, args) in sigs.items():
         if hasattr(lib, name):
@@ -429,6 +431,12 @@ class Matrix:
     @property
     def n(self):
         return self.info()[0]
+
+    def column_form(self):
+        """celg_mat_column_form: COLS_INT32, COLS_OFFSET8 or COLS_PATTERN."""
+        f = ctypes.c_int()
+        _check(lib.celg_mat_column_form(self.ptr, ctypes.byref(f)), "celg_mat_column_form")
+        return f.value
 
     def to_jad(self):
         n = self.n

@@ -74,6 +74,13 @@ __global__ void jad_key_kernel(int n, int mmax, int* key, int* hist) {
   }
 }
 
+// pattern index of each permuted row
+__global__ void jad_pid_kernel(int n, const int* __restrict__ perm, const uint8_t* __restrict__ pid,
+                               uint8_t* __restrict__ ppid) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    ppid[i] = pid[perm[i]];
+}
+
 __global__ void jad_fill_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
                                 const double* __restrict__ v, const int* __restrict__ perm,
                                 const int* __restrict__ jb, int* __restrict__ jci,
@@ -345,6 +352,7 @@ void free_mat_arrays(celg_mat* m) {
   cudaFree(m->jad.ci);
   cudaFree(m->jad.v);
   cudaFree(m->jad.perm);
+  cudaFree(m->jad.pid);
   cudaFree(m->diag);
   cudaFree(m->jacobi);
   cudaFree(m->jacobi32);
@@ -393,6 +401,7 @@ static int build_jad(celg_mat* m) {
   cudaFree(J.ci);
   cudaFree(J.v);
   cudaFree(J.perm);
+  cudaFree(J.pid);
   J = JadDev();
   int *key = nullptr, *key2 = nullptr, *idx = nullptr, *hist = nullptr;
   void* tmp = nullptr;
@@ -445,6 +454,11 @@ static int build_jad(celg_mat* m) {
     if (n > 0)
       jad_fill_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, m->csr.rp, m->csr.ci, m->csr.v, J.perm,
                                                           J.begin, J.ci, J.v);
+    // the pattern index of each permuted row, when the matrix has row patterns
+    if (m->csr.pid && n > 0) {
+      if ((e = cudaMalloc(&J.pid, (size_t)n + 16)) != cudaSuccess) { fail(e, "jad"); break; }
+      jad_pid_kernel<<<ew_grid(h, n), 256, 0, h->stream>>>(n, J.perm, m->csr.pid, J.pid);
+    }
     if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) { fail(e, "jad fill"); break; }
     J.mmax = mmax;
   } while (0);
@@ -695,10 +709,18 @@ extern "C" int celg_mat_info(const celg_mat* m, int* n, int* nnz, int* jad_mmax)
   return CELG_OK;
 }
 
+extern "C" int celg_mat_column_form(const celg_mat* m, int* form) {
+  if (!m || !form) return CELG_ERR_ARG;
+  *form = m->csr.pid ? CELG_COLS_PATTERN : (m->csr.ci8 ? CELG_COLS_OFFSET8 : CELG_COLS_INT32);
+  return CELG_OK;
+}
+
 extern "C" int celg_mat_to_jad(celg_mat* m, int* perm_out) {
   if (!m || m->csr.ncols != m->csr.n) return CELG_ERR_ARG;
   CELG_CUDA(cudaSetDevice(m->h->device));
-  int st = build_jad(m);
+  // the row patterns first, so that the JAD sweep can take its columns from them
+  int st = ensure_offset_dict(m->h, m);
+  if (!st) st = build_jad(m);
   if (st) return st;
   if (perm_out && m->csr.n > 0)
     CELG_CUDA(cudaMemcpy(perm_out, m->jad.perm, sizeof(int) * (size_t)m->csr.n, cudaMemcpyDeviceToHost));

@@ -46,6 +46,7 @@ struct JadDev {
   int* ci = nullptr;      // nnz
   double* v = nullptr;    // nnz
   int* perm = nullptr;    // n
+  uint8_t* pid = nullptr; // pattern index of each permuted row (n + 16), with row patterns
 };
 
 struct PcgState;  // device scalar state of one solve (pcg_internal.cuh)

@@ -300,15 +300,26 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   }
 }
 
-template <class Epi>
+// PAT: the matrix has row patterns and ppid holds the pattern index of each
+// permuted row (ppid[i] = pid[perm[i]]): the column of diagonal d of permuted
+// row i is perm[i] + pat[ppid[i] * kPatLen + d], so the x gathers of a group
+// wait for no column load (one memory round trip per group instead of two).
+template <class Epi, bool PAT = false>
 __global__ void __launch_bounds__(kLanes, 3)
     jad_kernel(const int* __restrict__ jb, const int* __restrict__ jci,
                const double* __restrict__ jv, const int* __restrict__ perm, int n, int mmax,
-               const double* __restrict__ x, Epi epi, RedCtx red) {
+               const double* __restrict__ x, Epi epi, RedCtx red,
+               const uint8_t* __restrict__ ppid = nullptr, const int* __restrict__ pat = nullptr,
+               int pat_ints = 0) {
   constexpr int NR = Epi::NRED;
   __shared__ double scratch[8];
   __shared__ int s_flag;
+  __shared__ int s_pat[PAT ? kPatMax * kPatLen : 1];
   if (!epi.active()) return;
+  if constexpr (PAT) {
+    for (int q = threadIdx.x; q < pat_ints; q += blockDim.x) s_pat[q] = pat[q];
+    __syncthreads();
+  }
   const int j = threadIdx.x;
   const long ntiles = ((long)n + kTile - 1) / kTile;
   for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
@@ -318,10 +329,17 @@ __global__ void __launch_bounds__(kLanes, 3)
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
     long i[4];
     double sum[4];
+    [[maybe_unused]] int prow[4];
+    [[maybe_unused]] const int* po[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       i[k] = t * kTile + (long)k * kLanes + j;
       sum[k] = 0.0;
+      if constexpr (PAT) {
+        const bool ok = i[k] < n;
+        prow[k] = ok ? __ldg(perm + i[k]) : 0;
+        po[k] = s_pat + (ok ? (int)__ldg(ppid + i[k]) : 0) * kPatLen;
+      }
     }
     // diagonals in groups of kJadDiag: every load of the group (values,
     // columns, then the x gathers) is issued before the group's adds, which
@@ -343,7 +361,10 @@ __global__ void __launch_bounds__(kLanes, 3)
 #pragma unroll
         for (int k = 0; k < 4; ++k)
           if (i[k] < len[g]) {
-            col[g][k] = __ldg(jci + beg[g] + i[k]);
+            if constexpr (PAT)
+              col[g][k] = prow[k] + po[k][d + g];
+            else
+              col[g][k] = __ldg(jci + beg[g] + i[k]);
             vv[g][k] = __ldg(jv + beg[g] + i[k]);
           }
 #pragma unroll

@@ -341,6 +341,16 @@ int launch_jad(celg_handle* h, const CsrDev& A, const JadDev& J, const double* x
   }
   if (A.n == 0) return CELG_OK;
   red.sweep = next_sweep(h, false);
+  if (J.pid && A.pat && J.mmax <= kPatLen) {
+    // the columns from the row patterns (same columns in the same order)
+    const int grid =
+        grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi, true>>(kLanes, 0)));
+    jad_kernel<Epi, true><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax,
+                                                          x, epi, red, J.pid, A.pat,
+                                                          A.npat * kPatLen);
+    CELG_CUDA(cudaGetLastError());
+    return CELG_OK;
+  }
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<jad_kernel<Epi>>(kLanes, 0)));
   jad_kernel<Epi><<<grid, kLanes, 0, h->stream>>>(J.begin, J.ci, J.v, J.perm, A.n, J.mmax, x, epi,
                                                     red);

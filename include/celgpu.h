@@ -149,6 +149,18 @@ int celg_mat_from_csr_device(celg_handle* h, int n, int nnz, const int* row_ptr_
                              const int* cols_d, const double* vals_d, celg_mat** out);
 int celg_mat_destroy(celg_mat* m);
 int celg_mat_info(const celg_mat* m, int* n, int* nnz, int* jad_mmax);
+/* The column data the solver sweeps (and the JAD SpMV) read for this matrix,
+ * which sets their bytes per non-zero: CELG_COLS_INT32 (the int32 columns),
+ * CELG_COLS_OFFSET8 (1-byte indices into a dictionary of at most 256 column
+ * offsets col - row) or CELG_COLS_PATTERN (one byte per row indexing at most
+ * 256 sequences of at most 8 offsets; no column data per entry).  The last
+ * two are built on the first solve, FP32 copy or JAD conversion of a matrix
+ * whose rows fit them; results are the same bits in every form.  celg_spmv
+ * in CSR reads the int32 columns.  No counterpart in the reference. */
+#define CELG_COLS_INT32 0
+#define CELG_COLS_OFFSET8 1
+#define CELG_COLS_PATTERN 2
+int celg_mat_column_form(const celg_mat* m, int* form);
 /* CSR -> JAD, cel_sp_mat_jad_from_sp_mat_local
  * (src/fspmtconverter/cel_sp_mat_jad_converter_module.f90:93-175): the reference's
  * permutation (stable sort by descending row length) and Saad's jagged
