@@ -450,9 +450,14 @@ struct GmPlan {
   double* Hp(int i, int j) const { return a.H + (size_t)j * (a.M + 1) + i; }
 };
 
+// w = A z on the row patterns or 1-byte offsets when the matrix has them
+// (same columns in the same order: the same sums)
 static int gm_spmv(celg_handle* h, const GmPlan& g, const double* x, double* y) {
   const EpiStoreIf epi{y, &g.a.st->act};
   if (g.fmt == CELG_FMT_JAD) return launch_jad(h, g.m->csr, g.m->jad, x, epi);
+  bool done = false;
+  const int st = launch_csr_compact<double>(h, g.m->csr, g.m->csr.v, x, epi, nullptr, 0, &done);
+  if (done) return st;
   return launch_csr<double>(h, g.m->csr, g.m->csr.v, x, epi);
 }
 
@@ -525,6 +530,7 @@ int gmres_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const c
   if (fmt == CELG_FMT_JAD && m->jad.mmax < 0) return CELG_ERR_STATE;
   const size_t nn = (size_t)std::max(1L, n);
   int st = ensure_work(h, (size_t)n);
+  if (!st) st = ensure_offset_dict(h, m);
   if (!st) st = ensure_gmres_work(h, nn, M);
   if (!st) st = ensure_partials(h, ntiles_of(n), 2);
   const int hist_cap = (res && res->history && res->history_cap > 0) ? res->history_cap : 0;
