@@ -822,7 +822,9 @@ def run_profile(argv):
       spmv32 SIDE [REPS]        the same on the FP32 copy (1-byte columns)
       pcg SIDE ITERS [fp64|ru|ir]
                                 one solve capped at ITERS iterations
-      mrhs SIDE ITERS K         K right-hand sides, capped at ITERS
+      mrhs SIDE ITERS K [fp64|ir]
+                                K right-hand sides, capped at ITERS (ir: one
+                                outer step of FP32 refinement, ITERS inner)
       batch 0 ITERS             the 64 uneven systems, capped at ITERS
 
     Set CELG_GRAPH=0 to launch the solver kernels from a host loop instead of
@@ -890,9 +892,13 @@ def run_profile(argv):
         print("pcg", side, mode, info.iter_done, info.status)
     elif what == "mrhs":
         iters, k = int(argv[2]), int(argv[3])
+        mode = argv[4] if len(argv) > 4 else "fp64"
+        kw = (dict(precision=celgpu.PREC_FP32_IR, inner_iter_max=iters, outer_max=1)
+              if mode == "ir" else {})
         B = torch.rand((n, k), dtype=torch.float64, device="cuda")
         X = torch.zeros_like(B)
-        infos = h.pcg_multirhs(m, k, B.data_ptr(), X.data_ptr(), eps_rel=1e-12, iter_max=iters)
+        infos = h.pcg_multirhs(m, k, B.data_ptr(), X.data_ptr(), eps_rel=1e-12, iter_max=iters,
+                               **kw)
         torch.cuda.synchronize()
         print("mrhs", side, k, max(i.iter_done for i in infos))
     else:

@@ -25,6 +25,7 @@ constexpr int kSub = 256;       // rows per pipeline sub-tile of the CSR kernel
 constexpr int kSubPerTile = kTile / kSub;
 constexpr int kStages = 4;      // bulk-copy pipeline depth of the CSR kernel
 constexpr int kConsumerWarps = 8;
+constexpr int kHeldTiles = 16;  // tiles whose warp sums wait in shared memory before their fold
 constexpr int kCsrThreads = (kConsumerWarps + 1) * 32;  // + one producer warp
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // bounded wait on an mbarrier: 2 s
 

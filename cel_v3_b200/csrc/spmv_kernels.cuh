@@ -63,6 +63,52 @@ constexpr int kCsrHeader = 256;  // mbarriers, stage meta, fold scratch
 // Issued before the gathers (tried for the p of p.v), they cost 23 us per
 // 256^3 sweep.
 
+// Sum of a row of L entries, 0 + v0 x0 + v1 x1 + ... in stored order, with
+// separate multiply and add roundings; G: values read from global memory.
+template <int L, bool G, typename VT>
+__device__ __forceinline__ VT pat_dot(const VT* vs, const VT (&xv)[kPatLen]) {
+  VT s = VT(0);
+#pragma unroll
+  for (int u = 0; u < L; ++u) s = vadd(s, vmul(G ? __ldg(vs + u) : vs[u], xv[u]));
+  return s;
+}
+
+// The same for a row of len entries: one branch on the length instead of a
+// predicate per entry.
+template <bool G, typename VT>
+__device__ __forceinline__ VT pat_dot_len(int len, const VT* vs, const VT (&xv)[kPatLen]) {
+  static_assert(kPatLen == 8, "lengths 1..8");
+  switch (len) {
+    case 7: return pat_dot<7, G>(vs, xv);
+    case 6: return pat_dot<6, G>(vs, xv);
+    case 5: return pat_dot<5, G>(vs, xv);
+    case 4: return pat_dot<4, G>(vs, xv);
+    case 8: return pat_dot<8, G>(vs, xv);
+    case 3: return pat_dot<3, G>(vs, xv);
+    case 2: return pat_dot<2, G>(vs, xv);
+    case 1: return pat_dot<1, G>(vs, xv);
+    default: return VT(0);
+  }
+}
+
+// x[base + off] through the read-only path, the address formed by one
+// 32 x 32 -> 64-bit multiply-add (at 256^3 this took the FP32 pattern sweep
+// from 109 to 101 M warp instructions, 141 -> 139 us)
+template <typename VT>
+__device__ __forceinline__ VT ldg_at(const VT* base, int off) {
+  if constexpr (sizeof(VT) == 8) {
+    double v;
+    asm("{\n\t.reg .u64 a;\n\tmad.wide.s32 a, %1, 8, %2;\n\tld.global.nc.f64 %0, [a];\n\t}"
+        : "=d"(v) : "r"(off), "l"(base));
+    return v;
+  } else {
+    float v;
+    asm("{\n\t.reg .u64 a;\n\tmad.wide.s32 a, %1, 4, %2;\n\tld.global.nc.f32 %0, [a];\n\t}"
+        : "=f"(v) : "r"(off), "l"(base));
+    return v;
+  }
+}
+
 template <int N>
 struct Acc {
   double a[N > 0 ? N : 1];
@@ -77,6 +123,9 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   constexpr bool kB = is_batched<Epi>::value;
   constexpr bool kPat = std::is_same<CT, PatIdx>::value;
   constexpr bool kDict = std::is_same<CT, uint8_t>::value;
+  // sub-tiles per consumer pass on row patterns (at 256^3: FP32 sweep 155 ->
+  // 148 us, FP64 205 -> 197 us against one per pass)
+  constexpr int kPR = kPat ? 2 : 1;
   // entries per 16 bytes of the narrowest per-entry array
   constexpr int kAlign = kPat ? 16 / (int)sizeof(VT) : (kDict ? 16 : 4);
   extern __shared__ __align__(128) unsigned char smem[];
@@ -192,6 +241,28 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   // ---------------- consumer warps (256 threads, lane j = row in sub-tile) ----
   const int j = threadIdx.x;
   int it = 0;
+  // Tile partials without a barrier per tile (as in tile_kernel): each warp
+  // folds its lanes of a tile with the butterfly and parks the warp sum; every
+  // kHeldTiles tiles (and at the end) the consumer warps meet once and add
+  // each tile's warp sums in warp order -- group_fold256's order and bits.
+  constexpr bool kHold = !kB && NR > 0;
+  constexpr int NR1 = NR > 0 ? NR : 1;
+  __shared__ double held[kHold ? kHeldTiles : 1][NR1][8];
+  __shared__ long held_tile[kHold ? kHeldTiles : 1];
+  [[maybe_unused]] int nheld = 0;
+  [[maybe_unused]] auto flush = [&]() {
+    named_bar_sync(1, kLanes);
+    for (int q = j; q < nheld * NR1; q += kLanes) {
+      const int sl = q / NR1, r = q % NR1;
+      double tot = held[sl][r][0];
+#pragma unroll
+      for (int w = 1; w < 8; ++w) tot = dadd(tot, held[sl][r][w]);
+      red.partials[(long)r * red.ntiles + held_tile[sl]] = tot;
+    }
+    __threadfence();  // every writer's partials visible before the grid's ticket
+    named_bar_sync(1, kLanes);
+    nheld = 0;
+  };
   Epi ep = epi;
   TileInfo nxt{0, 0.0};
   if constexpr (kB) {
@@ -208,7 +279,76 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
     Acc<NR> acc;
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc.a[r] = 0.0;
-    for (int q = 0; q < kSubPerTile; ++q) {
+    if constexpr (kPat) {
+      // Row patterns: kPR sub-tiles per pass, one row of each per thread.
+      // All gathers of the pass are issued before the first sum, and the
+      // per-stage bookkeeping (waits, stage pointers, release) is shared by
+      // kPR rows.  Rows j, j + 256, ... still reach the epilogue in order,
+      // so the tile sums keep their order.
+      static_assert(kSubPerTile % kPR == 0, "passes tile the tile");
+      static_assert(kPatLen == 8, "two int4 per pattern");
+      for (int q = 0; q < kSubPerTile; q += kPR) {
+        const long s0 = t * kSubPerTile + q;
+        if (s0 >= nsub) break;
+        const int nr = (int)min((long)kPR, nsub - s0);
+        int stg[kPR];
+#pragma unroll
+        for (int r = 0; r < kPR; ++r) {
+          stg[r] = (it + r) % kStages;
+          if (r < nr && !mbar_wait_bounded(&full[stg[r]], (uint32_t)(((it + r) / kStages) & 1), err))
+            return;
+        }
+        VT xv[kPR][kPatLen];
+        int len[kPR], vb[kPR], fbr[kPR];
+        // row indices as unsigned: s0 * kSub + j < n + kPR * kSub < 2^32
+        const unsigned row0 = (unsigned)s0 * (unsigned)kSub + (unsigned)j;
+#pragma unroll
+        for (int r = 0; r < kPR; ++r) {
+          len[r] = 0;
+          const unsigned row = row0 + (unsigned)(r * kSub);
+          if (r < nr && row < (unsigned)n) {
+            const unsigned char* sb = stages + (size_t)stg[r] * L.bytes;
+            const int* rps = reinterpret_cast<const int*>(sb);
+            const int b = rps[j];
+            len[r] = rps[j + 1] - b;
+            fbr[r] = meta[2 * stg[r] + 1];
+            vb[r] = fbr[r] ? b : b - meta[2 * stg[r]];
+            // the row's offsets from its pattern (two 16-byte shared loads;
+            // the table is 16-byte aligned, kPatLen ints per pattern, and a
+            // shorter pattern is padded with offset 0, so all kPatLen gathers
+            // are issued unpredicated: the padding reads x(row))
+            const int pv = fbr[r] ? (int)ci[row].v : (int)(sb + L.ci_off)[j];
+            const int4* pq = reinterpret_cast<const int4*>(s_dict + pv * kPatLen);
+            const int4 q0 = pq[0], q1 = pq[1];
+            const int po[kPatLen] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            const VT* xr = x + row;
+#pragma unroll
+            for (int u = 0; u < kPatLen; ++u) xv[r][u] = ldg_at(xr, po[u]);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kPR; ++r) {
+          const unsigned row = row0 + (unsigned)(r * kSub);
+          if (r < nr && row < (unsigned)n) {
+            const VT sum =
+                fbr[r] ? pat_dot_len<true>(len[r], v + vb[r], xv[r])
+                       : pat_dot_len<false>(
+                             len[r],
+                             reinterpret_cast<const VT*>(stages + (size_t)stg[r] * L.bytes + L.v_off) + vb[r],
+                             xv[r]);
+            ep.row((long)row, sum, acc.a);
+          }
+        }
+        __syncwarp();
+        if (lane == 0) {
+#pragma unroll
+          for (int r = 0; r < kPR; ++r)
+            if (r < nr) mbar_arrive(&empty[stg[r]]);
+        }
+        it += nr;
+      }
+    }
+    for (int q = 0; q < (kPat ? 0 : kSubPerTile); ++q) {
       const long s = t * kSubPerTile + q;
       if (s >= nsub) break;
       const int st = it % kStages;
@@ -224,24 +364,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
         const int b = rps[j], e = rps[j + 1];
         VT sum = VT(0);
         if constexpr (kPat) {
-          // the row's offsets from its pattern; values from the stage
-          const int pv = fb ? (int)ci[row].v : (int)reinterpret_cast<const uint8_t*>(cis)[j];
-          const int* po = s_dict + pv * kPatLen;
-          const VT* xr = x + row;
-          const int len = e - b;
-          VT xv[kPatLen];
-#pragma unroll
-          for (int u = 0; u < kPatLen; ++u)
-            if (u < len) xv[u] = __ldg(xr + po[u]);
-          if (!fb) {
-#pragma unroll
-            for (int u = 0; u < kPatLen; ++u)
-              if (u < len) sum = vadd(sum, vmul(vs[b - a0 + u], xv[u]));
-          } else {
-#pragma unroll
-            for (int u = 0; u < kPatLen; ++u)
-              if (u < len) sum = vadd(sum, vmul(__ldg(v + b + u), xv[u]));
-          }
+          // handled by the pass loop above
         } else if (kDict && sizeof(VT) == 4 && !fb) {
           // FP32 with 1-byte column offsets: the gathers address x from the
           // row's base (one dictionary lookup and one add per entry), and the
@@ -285,7 +408,16 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       if (lane == 0) mbar_arrive(&empty[st]);
       ++it;
     }
-    if (NR > 0) {
+    if constexpr (kHold) {
+      if (nheld == kHeldTiles) flush();
+#pragma unroll
+      for (int r = 0; r < NR1; ++r) {
+        const double w = warp_fold(acc.a[r]);
+        if (lane == 0) held[nheld][r][warp] = w;
+      }
+      if (j == 0) held_tile[nheld] = t;
+      ++nheld;
+    } else if (NR > 0) {
 #pragma unroll
       for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
@@ -294,6 +426,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       // batched: the systems are completed by batch_finish_kernel
     }
   }
+  if constexpr (kHold) flush();
   if constexpr (!kB && NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (red.finish && grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);

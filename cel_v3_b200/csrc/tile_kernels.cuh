@@ -44,7 +44,6 @@ struct tiles_per_pass<T, std::void_t<decltype(T::kTilesPerPass)>>
 // the tile partials are the same bits, but the warps no longer wait for one
 // another after every tile.  (Measured on the 256^3 FP32 update sweep: the
 // per-tile barrier pair was about a quarter of its time.)
-constexpr int kHeldTiles = 16;
 
 template <class Op>
 __global__ void __launch_bounds__(kLanes) tile_kernel(long n, Op op_in, RedCtx red) {
