@@ -375,9 +375,12 @@ def multirhs_form(h, celgpu, torch, stream):
     out = {}
     p32 = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO,
                         precision=celgpu.PREC_FP32_IR, inner_eps_rel=1e-4, inner_iter_max=5000)
+    p32ru = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO,
+                          precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
     runs = (("one_by_one", lambda: [h.pcg_jacobi(m, c.data_ptr(), x.data_ptr(), p) for c, x in zip(cols, xs)]),
             ("multirhs", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p)),
-            ("multirhs_fp32_ir", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p32)))
+            ("multirhs_fp32_ir", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p32)),
+            ("multirhs_fp32_ru", lambda: h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), p32ru)))
     for name, fn in runs:
         fn()
         torch.cuda.synchronize()
@@ -394,11 +397,15 @@ def multirhs_form(h, celgpu, torch, stream):
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
         if name == "multirhs":
             X64 = Xd.clone()
-        elif name == "multirhs_fp32_ir":
+        elif name in ("multirhs_fp32_ir", "multirhs_fp32_ru"):
             out[name]["worst_err_vs_fp64"] = max(rel_err(Xd[:, c], X64[:, c]) for c in range(k))
+        if name == "multirhs_fp32_ru":
+            out[name]["max_reliable_updates"] = max(i.arnoldi_steps for i in infos)
     out["tuned_spmm_variant"] = h.tuned_config(celgpu.TUNE_SPMM)[0]
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_multirhs_fp32_ir_vs_one_by_one"] = (out["multirhs_fp32_ir"]["solves_per_s"] /
+                                                     out["one_by_one"]["solves_per_s"])
+    out["speedup_multirhs_fp32_ru_vs_one_by_one"] = (out["multirhs_fp32_ru"]["solves_per_s"] /
                                                      out["one_by_one"]["solves_per_s"])
     m.destroy()
     return out
@@ -516,6 +523,7 @@ def forms_summary(forms, value):
         "batched_fp32_ir_x": g("batched_64", "speedup_batched_fp32_ir_vs_one_by_one"),
         "multirhs_x": g("multirhs_128_k32", "speedup_multirhs_vs_one_by_one"),
         "multirhs_fp32_ir_x": g("multirhs_128_k32", "speedup_multirhs_fp32_ir_vs_one_by_one"),
+        "multirhs_fp32_ru_x": g("multirhs_128_k32", "speedup_multirhs_fp32_ru_vs_one_by_one"),
         "grad_per_s": g("differentiation_128_b8", "gradients_per_s"),
         "grad_fd_err": g("differentiation_128_b8", "fd_check", "max_rel_err_dLdg"),
         "jad_pcg_solves_s": g("plain_large_256", "pcg_jad_256", "solves_per_s"),
@@ -822,9 +830,10 @@ def run_profile(argv):
       spmv32 SIDE [REPS]        the same on the FP32 copy (1-byte columns)
       pcg SIDE ITERS [fp64|ru|ir]
                                 one solve capped at ITERS iterations
-      mrhs SIDE ITERS K [fp64|ir]
+      mrhs SIDE ITERS K [fp64|ir|ru]
                                 K right-hand sides, capped at ITERS (ir: one
-                                outer step of FP32 refinement, ITERS inner)
+                                outer step of FP32 refinement, ITERS inner;
+                                ru: FP32 with reliable updates)
       batch 0 ITERS             the 64 uneven systems, capped at ITERS
 
     Set CELG_GRAPH=0 to launch the solver kernels from a host loop instead of
@@ -893,8 +902,8 @@ def run_profile(argv):
     elif what == "mrhs":
         iters, k = int(argv[2]), int(argv[3])
         mode = argv[4] if len(argv) > 4 else "fp64"
-        kw = (dict(precision=celgpu.PREC_FP32_IR, inner_iter_max=iters, outer_max=1)
-              if mode == "ir" else {})
+        kw = {"ir": dict(precision=celgpu.PREC_FP32_IR, inner_iter_max=iters, outer_max=1),
+              "ru": dict(precision=celgpu.PREC_FP32_RU)}.get(mode, {})
         B = torch.rand((n, k), dtype=torch.float64, device="cuda")
         X = torch.zeros_like(B)
         infos = h.pcg_multirhs(m, k, B.data_ptr(), X.data_ptr(), eps_rel=1e-12, iter_max=iters,

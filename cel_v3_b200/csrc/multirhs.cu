@@ -122,6 +122,9 @@ __device__ __forceinline__ void multi_grid_finish(const RedCtx& red, const Op& o
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -897,6 +900,232 @@ struct MEpiVerify {
   __device__ void finish_global() const {}
 };
 
+// ---- FP32 PCG with FP64 reliable updates for every column (CELG_PREC_FP32_RU) ----
+// The recurrence of ru_solve (ru.cu) for all columns at once: FP32 matrix and
+// vectors, one FP32 SpMM per iteration, and per column the FP64 correction
+// (x64 += d, r = b - A x64 with the FP64 matrix) whenever the column's FP32
+// residual has fallen by delta since its last one.  A column's arithmetic is
+// the single solve's; its reductions follow the multi-column order.
+
+struct MultiRu {
+  double* maxr;      // ||r64|| at the column's last reliable update
+  double* rz_prev;   // rz before the column's current step
+  double* norm64;    // the column's last FP64 residual norm
+  int* updates;      // reliable updates so far (the set-up residual included)
+  unsigned* umask;   // columns whose reliable update is due (bit c)
+  double delta;
+  cudaGraphConditionalHandle cond_update;  // IF node of the update (0: none)
+};
+
+__device__ __forceinline__ int mru_go(const MultiArgs& a, const MultiRu& u, int c) {
+  return (a.err[c] == 0 && *(volatile const int*)a.errw == 0 && a.iter[c] < a.iter_max &&
+          u.norm64[c] > a.eps[c])
+             ? 1
+             : 0;
+}
+
+// set-up: every column starts with a reliable update (the initial residual)
+__global__ void mru_init_kernel(int k, MultiRu u) {
+  const int c = threadIdx.x;
+  if (c < k) u.updates[c] = 0;
+  if (c == 0) *u.umask = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+}
+
+// FP64 residual of the columns due for an update, and its FP32 copy:
+//   r64 = b - (0 + A x);  r = (float) r64;  z = (double) r * J;  rz = r.z;  ||r64||^2
+// init: also p = (float) z.
+struct MEpiRuResidual {
+  using VT = double;
+  static constexpr int NRED = 2;
+  const double* B;
+  float* R32;
+  float* P32;  // set-up only
+  const float* J32;
+  int k;
+  MultiArgs a;
+  MultiRu u;
+  int init;
+  struct Pre { double b; float J; };
+  __device__ bool active() const { return *(volatile unsigned*)u.umask != 0u; }
+  __device__ bool col_active(int c) const { return ((*(volatile unsigned*)u.umask >> c) & 1u) != 0; }
+  __device__ Pre pre(long i, int c) const { return Pre{__ldg(B + i * k + c), __ldg(J32 + i)}; }
+  __device__ void stage_pre(long i, int c, double* st) const {
+    cp_async8(st + c, B + i * k + c);
+    cp_async4(reinterpret_cast<float*>(st + 32) + c, J32 + i);
+  }
+  __device__ Pre staged(const double* st, int c) const {
+    return Pre{st[c], reinterpret_cast<const float*>(st + 32)[c]};
+  }
+  __device__ void row(long i, int c, double s, const Pre& g, double* acc) const {
+    const long e = i * k + c;
+    const double r64 = __dsub_rn(g.b, dadd(0.0, s));
+    const float rf = (float)r64;
+    R32[e] = rf;
+    const double z = dmul((double)rf, (double)g.J);
+    if (init) P32[e] = (float)z;
+    acc[0] = dadd(acc[0], dmul((double)rf, z));
+    acc[1] = dadd(acc[1], dmul(r64, r64));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    if (!((*u.umask >> c) & 1u)) return;
+    u.norm64[c] = sqrt(tot[1]);
+    u.maxr[c] = u.norm64[c];
+    u.updates[c] += 1;
+    if (init) {
+      a.alpha[c] = tot[0];
+      a.norm[c] = u.norm64[c];
+    } else {
+      a.beta[c] = tot[0] / u.rz_prev[c];
+      a.alpha[c] = tot[0];
+    }
+    if (!mru_go(a, u, c) && a.active[c]) {
+      a.active[c] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {
+    *u.umask = 0u;
+    set_cond(a.cond, *(volatile int*)a.n_active > 0);
+  }
+};
+
+// r -= sigma v in FP32 arithmetic (r + (float)(-sigma) v); rz' = r.J r and
+// ||r||^2 on exact products; the column's update decision.  d += sigma p is
+// left pending (bit c of xmask) for the flush or the direction sweep.
+struct MOpRuStep {
+  static constexpr int NRED = 2;
+  struct Regs { float r, v, J; };
+  float* R32;
+  const float* V32;
+  const float* J32;
+  MultiArgs a;
+  MultiRu u;
+  float nsg = 0.0f;
+  __device__ bool prepare() {
+    if (*(volatile int*)a.n_active > 0) return true;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      set_cond(u.cond_update, 0);
+      set_cond(a.cond, 0);
+    }
+    return false;
+  }
+  __device__ bool col_active(int c) const { return *(volatile int*)&a.active[c] != 0; }
+  __device__ void begin_col(int c) { nsg = (float)(-a.sigma[c]); }
+  __device__ void load(long e, long i, Regs& g) const {
+    g.r = R32[e];
+    g.v = __ldcs(V32 + e);
+    g.J = __ldg(J32 + i);
+  }
+  __device__ void compute(long e, long, Regs& g, double* acc) const {
+    const float ri = fadd(g.r, fmul(nsg, g.v));
+    R32[e] = ri;
+    const double z = dmul((double)ri, (double)g.J);
+    acc[0] = dadd(acc[0], dmul((double)ri, z));
+    acc[1] = dadd(acc[1], dmul((double)ri, (double)ri));
+  }
+  __device__ void finish_col(int c, double* tot) const {
+    if (!a.active[c]) return;
+    u.rz_prev[c] = a.alpha[c];
+    a.beta[c] = tot[0] / a.alpha[c];
+    a.alpha[c] = tot[0];
+    a.norm[c] = sqrt(tot[1]);
+    a.iter[c] += 1;
+    atomicOr(a.xmask, 1u << c);
+    const int upd = (a.norm[c] < u.delta * u.maxr[c]) || (a.norm[c] <= a.eps[c]) ||
+                    (a.iter[c] >= a.iter_max);
+    if (upd) {
+      atomicOr(u.umask, 1u << c);
+    } else if (!(a.err[c] == 0 && *(volatile const int*)a.errw == 0 && a.iter[c] < a.iter_max &&
+                 fabs(a.alpha[c]) > 0.0)) {
+      a.active[c] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {
+    set_cond(u.cond_update, *(volatile unsigned*)u.umask != 0u);
+    set_cond(a.cond, *(volatile int*)a.n_active > 0);
+  }
+};
+
+// x64 += (double) d ; d = 0 for the columns due for an update (all columns
+// with `always`).  A d += sigma p still pending from the step is applied
+// first, with the step's rounding, and the column's mark is cleared.
+struct MOpRuFlush {
+  static constexpr int NRED = 0;
+  struct Regs { double x; float d, p; };
+  double* X;
+  float* D32;
+  const float* P32;  // null: nothing pending (the final flush)
+  MultiArgs a;
+  MultiRu u;
+  int always;
+  bool dp = false;
+  double sg = 0.0;
+  __device__ bool prepare() { return always || *(volatile unsigned*)u.umask != 0u; }
+  __device__ bool col_active(int c) const {
+    return always || ((*(volatile unsigned*)u.umask >> c) & 1u) != 0;
+  }
+  __device__ void begin_col(int c) {
+    dp = P32 != nullptr && ((*(volatile unsigned*)a.xmask >> c) & 1u) != 0;
+    sg = a.sigma[c];
+  }
+  __device__ void load(long e, long, Regs& g) const {
+    g.x = X[e];
+    g.d = D32[e];
+    if (dp) g.p = __ldg(P32 + e);
+  }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    const float di = dp ? (float)dadd((double)g.d, dmul(sg, (double)g.p)) : g.d;
+    X[e] = dadd(g.x, (double)di);
+    D32[e] = 0.0f;
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {
+    if (!always) *a.xmask &= ~*u.umask;
+  }
+};
+
+// d += sigma p where the step left it pending, then p = beta p + J r while
+// the column goes on.  The last CTA clears the pending marks.
+struct MOpRuDirection {
+  static constexpr int NRED = 0;
+  struct Regs { float p, r, J, d; };
+  float* P32;
+  const float* R32;
+  const float* J32;
+  float* D32;
+  MultiArgs a;
+  double bt = 0.0, sg = 0.0;
+  bool dp = false, act = false;
+  __device__ bool prepare() {
+    return *(volatile int*)a.n_active > 0 || *(volatile unsigned*)a.xmask != 0u;
+  }
+  __device__ bool col_active(int c) const {
+    return *(volatile int*)&a.active[c] != 0 || ((*(volatile unsigned*)a.xmask >> c) & 1u);
+  }
+  __device__ void begin_col(int c) {
+    bt = a.beta[c];
+    sg = a.sigma[c];
+    act = *(volatile int*)&a.active[c] != 0;
+    dp = ((*(volatile unsigned*)a.xmask >> c) & 1u) != 0;
+  }
+  // r and d are streamed (evict-first), so that L2 keeps the new p
+  __device__ void load(long e, long i, Regs& g) const {
+    g.p = P32[e];
+    if (act) {
+      g.r = __ldcs(R32 + e);
+      g.J = __ldg(J32 + i);
+    }
+    if (dp) g.d = __ldcs(D32 + e);
+  }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    if (dp) __stcs(D32 + e, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
+    if (act) P32[e] = celg::R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const { *a.xmask = 0u; }
+};
+
 // ---- FP32 refinement of every column (celg_pcg_multirhs, CELG_PREC_FP32_IR) -----
 // The outer loop of ir_solve (ir.cu) for all columns at once; each column
 // keeps its own residual norm, outer count and status.
@@ -1157,6 +1386,10 @@ struct Multi {
   double* irtau = nullptr;   // inner tolerance per column
   double* dstate2 = nullptr; // inner-solve scalars
   int* istate2 = nullptr;
+  // FP32 with reliable updates: maxr, rz_prev, norm64 (kMaxRhs each);
+  // updates (kMaxRhs), umask
+  double* rud = nullptr;
+  int* rui = nullptr;
 };
 
 namespace celg {
@@ -1178,6 +1411,8 @@ void multi_free(Multi* m) {
   cudaFree(m->irtau);
   cudaFree(m->dstate2);
   cudaFree(m->istate2);
+  cudaFree(m->rud);
+  cudaFree(m->rui);
   delete m;
 }
 
@@ -1242,6 +1477,8 @@ static MultiArgs multi_args(double* ds, int* is, int k, int iter_max, cudaGraphC
 
 static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
                        const celg_params* p, celg_result* res);
+static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
+                       const celg_params* p, celg_result* res);
 
 int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
                  const celg_params* p, celg_result* res) {
@@ -1249,6 +1486,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   // are timed: the 16-byte-gather SpMM reads them instead of the columns
   if (const int st = ensure_offset_dict(h, m)) return st;
   if (p->precision == CELG_PREC_FP32_IR) return multirhs_ir(h, m, k, B, X, p, res);
+  if (p->precision == CELG_PREC_FP32_RU) return multirhs_ru(h, m, k, B, X, p, res);
   if (p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
   const long n = m->csr.n;
   const size_t nk = (size_t)n * (size_t)k;
@@ -1558,6 +1796,179 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
     }
   }
   h->last_iters = inner_most;
+  return ret;
+}
+
+// FP32 PCG with FP64 reliable updates for every column: one graph launch
+// with a WHILE node over { FP32 SpMM, step, IF(any column due) { flush, FP64
+// residual SpMM }, direction }; self-skipping kernels from a host loop when
+// graphs are off.
+static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
+                       const celg_params* p, celg_result* res) {
+  const long n = m->csr.n;
+  const size_t nk = (size_t)n * (size_t)k;
+  if (!m->csr.v32 || !m->jacobi32) {
+    int st = celg_mat_make_fp32(m);
+    if (st) return st;
+  }
+  if (!h->multi) h->multi = new Multi();
+  Multi* mu = h->multi;
+  if (nk > mu->cap || !mu->work) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->work);
+    mu->work = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
+    mu->cap = nk;
+  }
+  if (!mu->dstate) {
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
+  }
+  if (nk > mu->f32cap || !mu->f32) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->f32);
+    mu->f32 = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->f32, sizeof(float) * std::max<size_t>(nk, 1) * 5));
+    mu->f32cap = nk;
+  }
+  if (!mu->rud) {
+    CELG_CUDA(cudaMalloc(&mu->rud, sizeof(double) * 3 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->rui, sizeof(int) * (kMaxRhs + 1)));
+  }
+  int st = ensure_partials(h, ntiles_of(n), 2 * k);
+  if (st) return st;
+  float* D32 = mu->f32;
+  float* R32 = D32 + nk;
+  float* P32 = R32 + nk;
+  float* V32 = P32 + nk;
+  const float* J32 = m->jacobi32;
+  MultiArgs a = multi_args(mu->dstate, mu->istate, k, p->iter_max, 0, h->err_d);
+  MultiRu u;
+  u.maxr = mu->rud;
+  u.rz_prev = u.maxr + kMaxRhs;
+  u.norm64 = u.rz_prev + kMaxRhs;
+  u.updates = mu->rui;
+  u.umask = reinterpret_cast<unsigned*>(u.updates + kMaxRhs);
+  u.delta = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-2;
+  u.cond_update = 0;
+  if (mu->tuned_mat != (const void*)m || mu->tuned_n != (int)n || mu->tuned_k != k) {
+    st = spmm_tune(h, m->csr, k, B, X, mu->work + 2 * nk, a, &mu->cfg);
+    if (st) return st;
+    mu->tuned_mat = m;
+    mu->tuned_n = (int)n;
+    mu->tuned_k = k;
+  }
+  const int cfg = mu->cfg;
+  auto setup = [&](const MultiArgs& ac) -> int {
+    int s2 = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
+    if (!s2) {
+      mru_init_kernel<<<1, kMaxRhs, 0, h->stream>>>(k, u);
+      CELG_CUDA(cudaGetLastError());
+      CELG_CUDA(cudaMemsetAsync(D32, 0, sizeof(float) * nk, h->stream));
+      s2 = launch_spmm(h, m->csr, k, X, MEpiRuResidual{B, R32, P32, J32, k, ac, u, 1}, cfg);
+    }
+    return s2;
+  };
+  auto body = [&](const MultiArgs& ac, bool in_graph) -> int {
+    MultiRu uc = u;
+    if (in_graph) {
+      int s2 = capture_new_handle(h, 0, &uc.cond_update);
+      if (s2) return s2;
+    }
+    int s3 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ac});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpRuStep{R32, V32, J32, ac, uc});
+    auto update = [&]() -> int {
+      int s4 = launch_mtile(h, n, k, MOpRuFlush{X, D32, P32, ac, uc, 0});
+      if (!s4) s4 = launch_spmm(h, m->csr, k, X, MEpiRuResidual{B, R32, nullptr, J32, k, ac, uc, 0}, cfg);
+      return s4;
+    };
+    if (!s3) s3 = in_graph ? capture_if(h, uc.cond_update, update) : update();
+    if (!s3) s3 = launch_mtile(h, n, k, MOpRuDirection{P32, R32, J32, D32, ac});
+    return s3;
+  };
+  auto tail = [&](const MultiArgs& ac) -> int {
+    int s2 = launch_mtile(h, n, k, MOpRuFlush{X, D32, nullptr, ac, u, 1});
+    if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac}, cfg);
+    return s2;
+  };
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  if (!graphs_enabled()) {
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = setup(a);
+    for (int it = 0; !st && it < p->iter_max; it += 8) {
+      for (int q = 0; q < 8 && !st; ++q) st = body(a, false);
+      int act = 0;
+      if (!st) {
+        CELG_CUDA(cudaMemcpyAsync(&act, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CELG_CUDA(cudaStreamSynchronize(h->stream));
+      }
+      if (!act) break;
+    }
+    if (!st) st = tail(a);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    auto record = [&](cudaGraphConditionalHandle cond) -> int {
+      MultiArgs ac = a;
+      ac.cond = cond;
+      int s2 = setup(ac);
+      if (!s2) s2 = capture_while2(h, cond, [&]() -> int { return body(ac, true); });
+      if (!s2) s2 = tail(ac);
+      return s2;
+    };
+    char kb[256];
+    std::snprintf(kb, sizeof(kb), "mrhs-ru|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%.17g|%d|%d",
+                  (const void*)m, m->csr.n, k, (const void*)B, (const void*)X, (const void*)D32,
+                  p->x0_mode, p->eps_abs, p->eps_rel, u.delta, p->iter_max, cfg);
+    const std::string key(kb);
+    GraphEntry* ge = graph_cache_find(h, key);
+    if (!ge) {
+      st = graph_build(h, key, record, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  }
+  std::vector<double> ds(7 * kMaxRhs), rd(3 * kMaxRhs);
+  std::vector<int> is(3 * kMaxRhs + 1), ri(kMaxRhs + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), mu->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), mu->istate, sizeof(int) * is.size(), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(rd.data(), mu->rud, sizeof(double) * rd.size(), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaMemcpyAsync(ri.data(), mu->rui, sizeof(int) * ri.size(), cudaMemcpyDeviceToHost, h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, iters = 0;
+  for (int c = 0; c < k; ++c) {
+    const double norm64 = rd[2 * kMaxRhs + c], eps = ds[5 * kMaxRhs + c];
+    const int it = is[c], err = is[2 * kMaxRhs + c];
+    int rs = CELG_OK;
+    if (err) rs = err;
+    else if (!(norm64 <= eps)) rs = CELG_ERR_NOCONV;
+    if (rs && !ret) ret = rs;
+    iters = std::max(iters, it);
+    if (res) {
+      res[c].iter_done = it;
+      res[c].final_norm2 = norm64;
+      res[c].bnorm = ds[4 * kMaxRhs + c];
+      res[c].verified_relres = ds[6 * kMaxRhs + c];
+      res[c].err = rs;
+      res[c].arnoldi_steps = ri[c];
+      res[c].history_len = 0;
+    }
+  }
+  h->last_iters = iters;
+  // FP32 SpMM (matrix; P gathered, V stored: 8 n k), step (R, V read, R
+  // stored: 12 n k; J 4 n), direction (P, R, D read, P, D stored: 20 n k;
+  // J 4 n); 4 bytes per non-zero and one per row on row patterns, else 5
+  // per non-zero with the 1-byte offsets, 8 with int32 columns
+  const double mat = m->csr.pid ? 4.0 * m->csr.nnz + n : (m->csr.ci8 ? 5.0 : 8.0) * m->csr.nnz;
+  h->last_bytes_per_iter = mat + 4.0 * (n + 1) + 40.0 * (double)nk + 8.0 * n;
   return ret;
 }
 

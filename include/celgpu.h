@@ -270,7 +270,13 @@ int celg_check_bounded_wait(celg_handle* h, int limit_ms, int* status);
  * recurrence (own scalars, own convergence); each iteration reads the matrix
  * once for all columns (block SpMM).  res (k entries, nullable) receives the
  * per-column reports.  Per-column SpMVs are bit-identical to celg_spmv; the
- * column dot products use a warp-ordered tile reduction (see multirhs.cu). */
+ * column dot products use a warp-ordered tile reduction (see multirhs.cu).
+ * precision CELG_PREC_FP32_IR refines every column around FP32 inner solves
+ * (iter_done = outer steps, arnoldi_steps = inner iterations);
+ * CELG_PREC_FP32_RU runs every column as FP32 PCG with FP64 reliable updates
+ * (threshold inner_eps_rel, default 1e-2; arnoldi_steps = reliable updates,
+ * final_norm2 = the last FP64 residual norm), the column's arithmetic that of
+ * celg_pcg_jacobi with CELG_PREC_FP32_RU. */
 int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, double* X_d,
                       const celg_params* p, celg_result* res);
 

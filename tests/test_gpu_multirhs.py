@@ -245,3 +245,119 @@ def test_multirhs_fp32_refinement_bitexact(gpu, mode, k, monkeypatch):
     assert [i.final_norm2 for i in infos] == list(rn)
     assert all(i.status == celgpu.OK and i.verified_relres <= 1e-10 for i in infos)
     m.destroy()
+
+
+def mirror_ru(rp, ci, v, B, eps_rel, delta, iter_max):
+    """FP32 PCG with FP64 reliable updates of every column: the recurrence of
+    the single solve (ru_oracle in test_gpu_solvers.py) per column, composed
+    from oracle pieces in the multi-column reduction order."""
+    f32, f64 = np.float32, np.float64
+    n, k = B.shape
+    J32 = R.jacobi(R.diag(rp, ci, v)).astype(f32).astype(f64)
+    v32 = v.astype(f32)
+    dc = lambda a, b: dot_cols(a[:, None], b[:, None])[0]
+    X = np.zeros((n, k))
+    its, ups, norms = [], [], []
+    for c in range(k):
+        b = B[:, c]
+
+        def residual(x):
+            r64 = b - (0.0 + R.spmv_csr(rp, ci, v, x))
+            r = r64.astype(f32)
+            z = r.astype(f64) * J32
+            return r, z, dc(r.astype(f64), z), np.sqrt(dc(r64, r64))
+
+        x = np.zeros(n)
+        eps = eps_rel * np.sqrt(dc(b, b))
+        r, z, rz, norm64 = residual(x)
+        p = z.astype(f32)
+        d = np.zeros(n, f32)
+        maxr, it, updates = norm64, 0, 1
+        active = norm64 > eps and it < iter_max
+        while active:
+            w = (f32(0) + R.spmv_csr_f32(rp, ci, v32, p)).astype(f32)
+            sigma = rz / dc(w.astype(f64), p.astype(f64))
+            d = (d.astype(f64) + sigma * p.astype(f64)).astype(f32)
+            r = r + f32(-sigma) * w                 # FP32 arithmetic, one rounding each
+            z = r.astype(f64) * J32
+            rz_new = dc(r.astype(f64), z)
+            norm = np.sqrt(dc(r.astype(f64), r.astype(f64)))
+            rz_prev, beta, rz = rz, rz_new / rz, rz_new
+            it += 1
+            if norm < delta * maxr or norm <= eps or it >= iter_max:
+                x = x + d.astype(f64)
+                d[:] = 0
+                r, z, rzh, norm64 = residual(x)
+                maxr = norm64
+                beta, rz = rzh / rz_prev, rzh
+                updates += 1
+                active = norm64 > eps and it < iter_max
+            else:
+                active = it < iter_max and abs(rz) > 0
+            if active:
+                p = (beta * p.astype(f64) + z).astype(f32)
+        X[:, c] = x + d.astype(f64)
+        its.append(it)
+        ups.append(updates)
+        norms.append(norm64)
+    return X, its, ups, norms
+
+
+def ru_problem(k, seed=15):
+    rng = np.random.default_rng(seed)
+    _, (kx, ky, kz) = synth.lognormal_faces(rng, 9, 8, 10, 0.5)
+    rp, ci, v = synth.diffusion7(9, 8, 10, kx, ky, kz)
+    B = rng.uniform(-1.0, 1.0, (rp.size - 1, k))
+    B[:, 3] *= 1e-3                         # columns of different scale
+    return rp, ci, v, B
+
+
+@pytest.mark.parametrize("mode", ["graph", "host_loop"])
+@pytest.mark.parametrize("k", [6, 8])
+def test_multirhs_fp32_reliable_update_bitexact(gpu, mode, k, monkeypatch):
+    """Every column runs FP32 PCG with FP64 reliable updates: X, iteration and
+    update counts and the last FP64 residual norms equal the mirror's.  k = 8
+    runs the FP32 SpMM with 16-byte gathers, k = 6 the register pipeline."""
+    celgpu, h, torch = gpu
+    if mode == "host_loop":
+        monkeypatch.setenv("CELG_GRAPH", "0")
+    rp, ci, v, B = ru_problem(k)
+    n = rp.size - 1
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-10, iter_max=3000,
+                           precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
+    Xo, its, ups, norms = mirror_ru(rp, ci, v, B, 1e-10, 1e-2, 3000)
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == its
+    assert [i.arnoldi_steps for i in infos] == ups
+    assert [i.final_norm2 for i in infos] == norms
+    assert all(i.status == celgpu.OK and i.verified_relres <= 1e-10 for i in infos)
+    # the same solutions as the FP64 multi-column solve, to the tolerance
+    # (column 3, scaled by 1e-3, is left out: the FP64 loop's absolute guard
+    # |r.z| > 1.1 eps_mach ends it before rel-res 1e-10)
+    X64 = dev(torch, np.zeros((n, k)))
+    h.pcg_multirhs(m, k, Bd.data_ptr(), X64.data_ptr(), eps_rel=1e-10, iter_max=3000)
+    Xr, X6 = Xd.cpu().numpy(), X64.cpu().numpy()
+    for c in range(k):
+        if c != 3:
+            assert np.abs(Xr[:, c] - X6[:, c]).max() <= 1e-6 * np.abs(X6[:, c]).max()
+    m.destroy()
+
+
+@pytest.mark.parametrize("iter_max", [1, 9])
+def test_multirhs_fp32_reliable_update_iteration_cap(gpu, iter_max):
+    """The iteration cap forces a reliable update; the pending d += sigma p is
+    applied before x is flushed, and every column reports CELG_ERR_NOCONV."""
+    celgpu, h, torch = gpu
+    rp, ci, v, B = ru_problem(5, seed=16)
+    n, k = B.shape
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-10, iter_max=iter_max,
+                           precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
+    Xo, its, ups, norms = mirror_ru(rp, ci, v, B, 1e-10, 1e-2, iter_max)
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == its == [iter_max] * k
+    assert all(i.status == celgpu.ERR_NOCONV for i in infos)
+    m.destroy()
