@@ -401,7 +401,7 @@ def multirhs_form(h, celgpu, torch, stream):
             out[name]["worst_err_vs_fp64"] = max(rel_err(Xd[:, c], X64[:, c]) for c in range(k))
         if name == "multirhs_fp32_ru":
             out[name]["max_reliable_updates"] = max(i.arnoldi_steps for i in infos)
-    out["tuned_spmm_variant"] = h.tuned_config(celgpu.TUNE_SPMM)[0]
+    out["tuned_spmm_variant"], out["tuned_spmm32_shape"] = h.tuned_config(celgpu.TUNE_SPMM)
     out["speedup_multirhs_vs_one_by_one"] = out["multirhs"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_multirhs_fp32_ir_vs_one_by_one"] = (out["multirhs_fp32_ir"]["solves_per_s"] /
                                                      out["one_by_one"]["solves_per_s"])

@@ -696,7 +696,7 @@ class Handle:
     def tuned_config(self, what):
         """celg_tuned_config: the autotuner's pick for the last batched
         (TUNE_BATCH: (SpMV CTAs per SM, vector-sweep CTAs per SM)) or
-        multi-RHS (TUNE_SPMM: (variant, -1)) solve."""
+        multi-RHS (TUNE_SPMM: (FP64 variant, FP32 shape or -1)) solve."""
         out = (ctypes.c_int * 2)()
         _check(lib.celg_tuned_config(self.ptr, int(what), out), "celg_tuned_config")
         return out[0], out[1]

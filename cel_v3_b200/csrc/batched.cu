@@ -1110,6 +1110,7 @@ extern "C" int celg_tuned_config(celg_handle* h, int what, int out[2]) {
     const int cfg = celg::multi_tuned_cfg(h->multi);
     if (cfg < 0) return CELG_ERR_STATE;
     out[0] = cfg;
+    out[1] = celg::multi_tuned_cfg32(h->multi);
     return CELG_OK;
   }
   return CELG_ERR_ARG;

@@ -197,5 +197,6 @@ void batch_free(::Batch* b);
 void multi_free(::Multi* m);
 void multi_forget_matrix(::Multi* m, const void* mat);
 int multi_tuned_cfg(::Multi* m);  // the SpMM variant the tuner picked, -1 if none
+int multi_tuned_cfg32(::Multi* m);  // the FP32 SpMM shape the tuner picked, -1 if none
 
 }  // namespace celg

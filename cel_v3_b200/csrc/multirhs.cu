@@ -1292,12 +1292,24 @@ static int launch_spmm_vec(celg_handle* h, const CsrDev& A, const typename Epi::
   return launch_spmm_vec_p<Epi, MINB, U, RP, false>(h, A, vals, k, X, epi);
 }
 
-// SpMM of the FP32 inner solve: the 16-byte-gather kernel when k is a
-// multiple of 4 and X is 16-byte aligned, else the register pipeline.
+// SpMM of the FP32 solves: the 16-byte-gather kernel when k is a multiple
+// of 4 and X is 16-byte aligned, in one of kSpmm32NumCfgs launch shapes
+// (resident CTAs per SM / entries per gather round / rows per lane group:
+// 4/4/1, 3/4/1, 3/2/2, 2/4/2, 2/8/1; picked by spmm_tune32), else the
+// register pipeline.
+constexpr int kSpmm32NumCfgs = 5;
 template <class Epi>
-static int launch_spmm_f32(celg_handle* h, const CsrDev& A, int k, const float* X, const Epi& epi) {
-  if ((k & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0)
-    return launch_spmm_vec<Epi, 4, 4, 1>(h, A, A.v32, k, X, epi);
+static int launch_spmm_f32(celg_handle* h, const CsrDev& A, int k, const float* X, const Epi& epi,
+                           int cfg32 = 0) {
+  if ((k & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {
+    switch (cfg32) {
+      case 1: return launch_spmm_vec<Epi, 3, 4, 1>(h, A, A.v32, k, X, epi);
+      case 2: return launch_spmm_vec<Epi, 3, 2, 2>(h, A, A.v32, k, X, epi);
+      case 3: return launch_spmm_vec<Epi, 2, 4, 2>(h, A, A.v32, k, X, epi);
+      case 4: return launch_spmm_vec<Epi, 2, 8, 1>(h, A, A.v32, k, X, epi);
+      default: return launch_spmm_vec<Epi, 4, 4, 1>(h, A, A.v32, k, X, epi);
+    }
+  }
   return launch_spmm_cfg<Epi, 4, 4>(h, A, A.v32, k, X, epi);
 }
 
@@ -1390,15 +1402,20 @@ struct Multi {
   // updates (kMaxRhs), umask
   double* rud = nullptr;
   int* rui = nullptr;
+  // FP32 SpMM shape picked for the last (matrix, n, k) tuned
+  const void* tuned32_mat = nullptr;
+  int tuned32_n = -1, tuned32_k = -1, cfg32 = 0;
 };
 
 namespace celg {
 
 // a destroyed matrix's address may be reused: drop its tuning record
 int multi_tuned_cfg(Multi* m) { return (m && m->tuned_mat) ? m->cfg : -1; }
+int multi_tuned_cfg32(Multi* m) { return (m && m->tuned32_mat) ? m->cfg32 : -1; }
 
 void multi_forget_matrix(Multi* m, const void* mat) {
   if (m && m->tuned_mat == mat) m->tuned_mat = nullptr;
+  if (m && m->tuned32_mat == mat) m->tuned32_mat = nullptr;
 }
 
 void multi_free(Multi* m) {
@@ -1450,6 +1467,54 @@ static int spmm_tune(celg_handle* h, const CsrDev& A, int k, const double* B, do
       *best = c;
     }
   }
+  return CELG_OK;
+}
+
+// The FP32 SpMM shapes timed the same way on the FP32 copy of the matrix,
+// with the iteration's epilogue applied to P32 (set to a finite constant) and
+// the output in V32; the solve's own set-up overwrites both and the state.
+// CELG_SPMM32_CFG=0..4 forces one (profiling).
+static int spmm_tune32(celg_handle* h, const CsrDev& A, int k, const double* B, double* X,
+                       float* P32, float* V32, size_t nk, const MultiArgs& a, int* best) {
+  if (const char* e = std::getenv("CELG_SPMM32_CFG")) {
+    *best = std::min(std::max(std::atoi(e), 0), kSpmm32NumCfgs - 1);
+    return CELG_OK;
+  }
+  *best = 0;
+  if ((k & 3) != 0 || (reinterpret_cast<uintptr_t>(P32) & 15) != 0) return CELG_OK;
+  int st = launch_mtile(h, A.n, k, MOpPre<double>{B, X, CELG_X0_USER, 0.0, 0.0, a});
+  if (st) return st;
+  CELG_CUDA(cudaMemsetAsync(a.alpha, 0, sizeof(double) * kMaxRhs, h->stream));
+  CELG_CUDA(cudaMemsetAsync(P32, 0x3f, sizeof(float) * nk, h->stream));  // 0.747f everywhere
+  const MEpiAp<float> ep{V32, P32, k, a};
+  float best_ms = 0.f;
+  for (int c = 0; c < kSpmm32NumCfgs; ++c) {
+    st = launch_spmm_f32(h, A, k, P32, ep, c);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    for (int r = 0; r < 3 && !st; ++r) st = launch_spmm_f32(h, A, k, P32, ep, c);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+    CELG_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    CELG_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    if (c == 0 || ms < best_ms) {
+      best_ms = ms;
+      *best = c;
+    }
+  }
+  return CELG_OK;
+}
+
+static int ensure_tuned32(celg_handle* h, Multi* mu, celg_mat* m, int k, const double* B, double* X,
+                          float* P32, float* V32, size_t nk, const MultiArgs& a) {
+  if (mu->tuned32_mat == (const void*)m && mu->tuned32_n == m->csr.n && mu->tuned32_k == k)
+    return CELG_OK;
+  const int st = spmm_tune32(h, m->csr, k, B, X, P32, V32, nk, a, &mu->cfg32);
+  if (st) return st;
+  mu->tuned32_mat = m;
+  mu->tuned32_n = m->csr.n;
+  mu->tuned32_k = k;
   return CELG_OK;
 }
 
@@ -1642,7 +1707,7 @@ static int multi_run_while(celg_handle* h, cudaGraphConditionalHandle cond, cons
 }
 
 static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size_t nk,
-                              const MultiIr& ir, MultiArgs ai, double inner_eps) {
+                              const MultiIr& ir, MultiArgs ai, double inner_eps, int cfg32) {
   const long n = m->csr.n;
   float* B32 = F;
   float* D32 = B32 + nk;
@@ -1654,10 +1719,10 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
                           ir.tau_col};
   int st = launch_mtile(h, n, k, pre);
   if (!st)
-    st = launch_spmm_f32(h, m->csr, k, D32, MEpiInit<float>{B32, R32, P32, J32, k, ai});
+    st = launch_spmm_f32(h, m->csr, k, D32, MEpiInit<float>{B32, R32, P32, J32, k, ai}, cfg32);
   if (!st)
     st = multi_run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
-      int s2 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ai});
+      int s2 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ai}, cfg32);
       if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{R32, V32, J32, ai, 0.0});
       if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, D32, ai});
       return s2;
@@ -1726,13 +1791,16 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
     mu->tuned_k = k;
   }
   const int cfg = mu->cfg;
+  st = ensure_tuned32(h, mu, m, k, B, X, mu->f32 + 3 * nk, mu->f32 + 4 * nk, nk, a);
+  if (st) return st;
+  const int cfg32 = mu->cfg32;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
   CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
   st = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, a});
   CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * (5 * kMaxRhs + 1), h->stream));
   char kb[160];
-  std::snprintf(kb, sizeof(kb), "mrhs-ir|%p|%d|%d|%p|%d|%.17g", (const void*)m, m->csr.n, k,
-                (const void*)mu->f32, inner_max, inner_eps);
+  std::snprintf(kb, sizeof(kb), "mrhs-ir|%p|%d|%d|%p|%d|%.17g|%d", (const void*)m, m->csr.n, k,
+                (const void*)mu->f32, inner_max, inner_eps, cfg32);
   const std::string gkey(kb);
   for (int it = 0; !st && it <= ir.outer_max; ++it) {
     CELG_CUDA(cudaMemsetAsync(ir.part, 0, sizeof(int) * kMaxRhs, h->stream));
@@ -1751,13 +1819,13 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
         st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
           return record_multi_inner(h, m, k, mu->f32, nk, ir,
                                     multi_args(mu->dstate2, mu->istate2, k, inner_max, cond, h->err_d),
-                                    inner_eps);
+                                    inner_eps, cfg32);
         }, &ge);
         if (st) break;
       }
       CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
     } else {
-      st = record_multi_inner(h, m, k, mu->f32, nk, ir, ai_host, inner_eps);
+      st = record_multi_inner(h, m, k, mu->f32, nk, ir, ai_host, inner_eps, cfg32);
       if (st) break;
     }
     mir_count_kernel<<<1, kMaxRhs, 0, h->stream>>>(k, ir, ai_host.iter, ai_host.err);
@@ -1861,6 +1929,9 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
     mu->tuned_k = k;
   }
   const int cfg = mu->cfg;
+  st = ensure_tuned32(h, mu, m, k, B, X, P32, V32, nk, a);
+  if (st) return st;
+  const int cfg32 = mu->cfg32;
   auto setup = [&](const MultiArgs& ac) -> int {
     int s2 = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
     if (!s2) {
@@ -1877,7 +1948,7 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
       int s2 = capture_new_handle(h, 0, &uc.cond_update);
       if (s2) return s2;
     }
-    int s3 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ac});
+    int s3 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ac}, cfg32);
     if (!s3) s3 = launch_mtile(h, n, k, MOpRuStep{R32, V32, J32, ac, uc});
     auto update = [&]() -> int {
       int s4 = launch_mtile(h, n, k, MOpRuFlush{X, D32, P32, ac, uc, 0});
@@ -1919,9 +1990,9 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
       return s2;
     };
     char kb[256];
-    std::snprintf(kb, sizeof(kb), "mrhs-ru|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%.17g|%d|%d",
+    std::snprintf(kb, sizeof(kb), "mrhs-ru|%p|%d|%d|%p|%p|%p|%d|%.17g|%.17g|%.17g|%d|%d|%d",
                   (const void*)m, m->csr.n, k, (const void*)B, (const void*)X, (const void*)D32,
-                  p->x0_mode, p->eps_abs, p->eps_rel, u.delta, p->iter_max, cfg);
+                  p->x0_mode, p->eps_abs, p->eps_rel, u.delta, p->iter_max, cfg, cfg32);
     const std::string key(kb);
     GraphEntry* ge = graph_cache_find(h, key);
     if (!ge) {

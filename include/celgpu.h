@@ -284,8 +284,10 @@ int celg_pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B_d, dou
  * last batched solve (what = CELG_TUNE_BATCH: out[0] = resident CTAs per SM
  * of the SpMV sweep, 0 meaning as many as fit; out[1] = CTAs per SM of the
  * vector sweeps) or multi-right-hand-side solve (what = CELG_TUNE_SPMM:
- * out[0] = the SpMM variant, 0..14).  No counterpart in the reference, which
- * has no autotuner.  CELG_ERR_STATE before the first such solve. */
+ * out[0] = the FP64 SpMM variant, 0..14; out[1] = the FP32 SpMM shape of
+ * the FP32 forms, 0..4, or -1 before the first of them).  No counterpart in
+ * the reference, which has no autotuner.  CELG_ERR_STATE before the first
+ * such solve. */
 #define CELG_TUNE_BATCH 0
 #define CELG_TUNE_SPMM 1
 int celg_tuned_config(celg_handle* h, int what, int out[2]);

@@ -361,3 +361,22 @@ def test_multirhs_fp32_reliable_update_iteration_cap(gpu, iter_max):
     assert [i.iter_done for i in infos] == its == [iter_max] * k
     assert all(i.status == celgpu.ERR_NOCONV for i in infos)
     m.destroy()
+
+
+@pytest.mark.parametrize("cfg32", range(5))
+def test_every_fp32_spmm_shape_is_bitexact(gpu, cfg32, monkeypatch):
+    """Each FP32 SpMM launch shape the tuner chooses from (forced with
+    CELG_SPMM32_CFG) gives the mirror's bits in the reliable-update form."""
+    celgpu, h, torch = gpu
+    monkeypatch.setenv("CELG_SPMM32_CFG", str(cfg32))
+    rp, ci, v, B = ru_problem(8, seed=17)
+    n, k = B.shape
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-10, iter_max=3000,
+                           precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
+    assert h.tuned_config(celgpu.TUNE_SPMM)[1] == cfg32
+    Xo, its, _, _ = mirror_ru(rp, ci, v, B, 1e-10, 1e-2, 3000)
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == its
+    m.destroy()
