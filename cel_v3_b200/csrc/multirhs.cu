@@ -677,6 +677,108 @@ __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, 
   else multi_grid_finish<1>(red, op, 0, scratch, &s_flag, s_tot);
 }
 
+// The same sweeps for FP32 storage with 16-byte accesses (k a multiple of 4,
+// the arrays 16-byte aligned): in a step of 4 rows, lane l works on row
+// l / 8 of the step and columns 4 (l % 8) .. 4 (l % 8) + 3, so every load and
+// store moves 16 bytes per lane instead of 4.  An op with 4-column methods
+// (load4, begin_col4, compute4, store4) returns each element's reduction
+// terms; they are transposed through shared memory to lane = column and
+// added in row order there, so the per-column sums keep the order (and the
+// bits) of mtile_kernel.
+template <class T, class = void>
+struct has_vec4 : std::false_type {};
+template <class T>
+struct has_vec4<T, std::void_t<decltype(&T::store4)>> : std::true_type {};
+
+template <class Op>
+__global__ void __launch_bounds__(kLanes) mtile4_kernel(long n, int k, Op op_in, RedCtx red) {
+  // 4-row steps whose loads are in flight together (128^3 x 32 reliable-
+  // update step: 233 / 204 / 193 / 183 us for 1 / 2 / 4 / 8; direction sweep
+  // 226 / 215 / 216 / 226 us)
+  constexpr int RV = 4;
+  static_assert(32 % (4 * RV) == 0, "steps tile the warp's 32 rows");
+  constexpr int NR = Op::NRED;
+  constexpr int NR1 = NR > 0 ? NR : 1;
+  __shared__ double s_w[NR1 * 8 * 32];
+  __shared__ double scratch[8];
+  __shared__ double s_tot[NR1 * kMaxRhs];
+  __shared__ int s_flag;
+  __shared__ __align__(16) double s_c[NR > 0 ? 8 : 1][NR1][4][32];
+  Op op = op_in;
+  if (!op.prepare()) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gr = lane >> 3, c0 = 4 * (lane & 7);
+  const bool von = c0 < k;
+  op.begin_col4(von ? c0 : 0);
+  const long ntiles = (n + kTile - 1) / kTile;
+  for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
+    const long t = tile_at(kt, ntiles, red.sweep);
+    double acc[NR1];
+#pragma unroll
+    for (int r = 0; r < NR1; ++r) acc[r] = 0.0;
+    for (int q = 0; q < 4; ++q) {
+      const long row0 = t * kTile + q * kSub + warp * 32;
+      if (row0 >= n) break;
+      for (int r16 = 0; r16 < 32; r16 += 4 * RV) {
+        // the loads of RV steps are issued before the first is used
+        typename Op::Regs4 g[RV];
+#pragma unroll
+        for (int v = 0; v < RV; ++v) {
+          const long i = row0 + r16 + 4 * v + gr;
+          if (von && i < n) op.load4(i * k + c0, i, g[v]);
+        }
+#pragma unroll
+        for (int v = 0; v < RV; ++v) {
+        const int r4 = r16 + 4 * v;
+        const long i = row0 + r4 + gr;
+        const bool ok = von && i < n;
+        double ct[NR1][4];
+#pragma unroll
+        for (int r = 0; r < NR1; ++r)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) ct[r][j] = 0.0;
+        if (ok) {
+          op.template compute4<NR1>(g[v], ct);
+          op.store4(i * k + c0, g[v]);
+        }
+        if constexpr (NR > 0) {
+          if (von) {
+#pragma unroll
+            for (int r = 0; r < NR1; ++r) {
+              *reinterpret_cast<double2*>(&s_c[warp][r][gr][c0]) = make_double2(ct[r][0], ct[r][1]);
+              *reinterpret_cast<double2*>(&s_c[warp][r][gr][c0 + 2]) = make_double2(ct[r][2], ct[r][3]);
+            }
+          }
+          __syncwarp();
+          if (lane < k) {
+#pragma unroll
+            for (int gg = 0; gg < 4; ++gg)
+              if (row0 + r4 + gg < n) {
+#pragma unroll
+                for (int r = 0; r < NR1; ++r) acc[r] = dadd(acc[r], s_c[warp][r][gg][lane]);
+              }
+          }
+          __syncwarp();  // the terms are read before the next step overwrites them
+        }
+        }
+      }
+    }
+    if (NR > 0) multi_tile_store<NR1>(acc, s_w, k, t, red.ntiles, red.partials, warp, lane);
+  }
+  if (NR > 0) multi_grid_finish<NR1>(red, op, k, scratch, &s_flag, s_tot);
+  else multi_grid_finish<1>(red, op, 0, scratch, &s_flag, s_tot);
+}
+
+__device__ __forceinline__ float f4c(const float4& v, int j) {
+  return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void f4s(float4& v, int j, float x) {
+  if (j == 0) v.x = x;
+  else if (j == 1) v.y = x;
+  else if (j == 2) v.z = x;
+  else v.w = x;
+}
+
 // ---- the sweeps of the multi-column PCG ------------------------------------------
 
 // x0 and ||b|| per column.  With `part` set (the refinement's inner solves)
@@ -877,6 +979,82 @@ struct MOpDirection {
   __device__ void finish_global() const { *a.xmask = 0u; }
 };
 
+// The FP32 update and direction sweeps of the refinement's inner solves
+// with 4-column methods for mtile4_kernel (same arithmetic per element).
+struct MOpUpdate32 : MOpUpdate<float> {
+  struct Regs4 { float4 r, v; float J; };
+  double sg4[4];
+  bool act4[4];
+  __device__ void begin_col4(int c0) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j < a.k ? c0 + j : 0;
+      sg4[j] = a.sigma[c];
+      act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
+    }
+  }
+  __device__ void load4(long e, long i, Regs4& g) const {
+    g.r = *reinterpret_cast<const float4*>(R + e);
+    g.v = __ldcs(reinterpret_cast<const float4*>(V + e));
+    g.J = __ldg(J + i);
+  }
+  template <int NR1>
+  __device__ void compute4(Regs4& g, double (&ct)[NR1][4]) const {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (act4[j]) {
+        const float ri = celg::R<float>(dadd(D(f4c(g.r, j)), dmul(-sg4[j], D(f4c(g.v, j)))));
+        f4s(g.r, j, ri);
+        const double z = dmul(D(ri), D(g.J));
+        ct[0][j] = dmul(D(ri), z);
+        ct[1][j] = dmul(D(ri), D(ri));
+      }
+  }
+  __device__ void store4(long e, const Regs4& g) const { *reinterpret_cast<float4*>(R + e) = g.r; }
+};
+
+struct MOpDirection32 : MOpDirection<float> {
+  struct Regs4 { float4 p, r, x; float J; };
+  double bt4[4], sg4[4];
+  bool xp4[4], act4[4];
+  bool anyx = false, anya = false;
+  __device__ void begin_col4(int c0) {
+    const unsigned xm = *(volatile unsigned*)a.xmask;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j < a.k ? c0 + j : 0;
+      bt4[j] = a.beta[c];
+      sg4[j] = a.sigma[c];
+      act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
+      xp4[j] = c0 + j < a.k && ((xm >> c) & 1u) != 0;
+    }
+    anyx = xp4[0] || xp4[1] || xp4[2] || xp4[3];
+    anya = act4[0] || act4[1] || act4[2] || act4[3];
+  }
+  __device__ void load4(long e, long i, Regs4& g) const {
+    g.p = *reinterpret_cast<const float4*>(P + e);
+    if (anya) {
+      g.r = __ldcs(reinterpret_cast<const float4*>(R + e));
+      g.J = __ldg(J + i);
+    }
+    if (anyx) g.x = __ldcs(reinterpret_cast<const float4*>(X + e));
+  }
+  template <int NR1>
+  __device__ void compute4(Regs4& g, double (&)[NR1][4]) const {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float pj = f4c(g.p, j);
+      if (xp4[j]) f4s(g.x, j, celg::R<float>(dadd(D(f4c(g.x, j)), dmul(sg4[j], D(pj)))));
+      if (act4[j])
+        f4s(g.p, j, celg::R<float>(dadd(dmul(bt4[j], D(pj)), dmul(D(f4c(g.r, j)), D(g.J)))));
+    }
+  }
+  __device__ void store4(long e, const Regs4& g) const {
+    if (anyx) __stcs(reinterpret_cast<float4*>(X + e), g.x);
+    if (anya) *reinterpret_cast<float4*>(P + e) = g.p;
+  }
+};
+
 // ||b - A x|| / ||b|| per column
 struct MEpiVerify {
   using VT = double;
@@ -1023,6 +1201,38 @@ struct MOpRuStep {
     acc[0] = dadd(acc[0], dmul((double)ri, z));
     acc[1] = dadd(acc[1], dmul((double)ri, (double)ri));
   }
+  // 4 columns c0..c0+3 per lane (mtile4_kernel)
+  struct Regs4 { float4 r, v; float J; };
+  float nsg4[4];
+  bool act4[4];
+  __device__ void begin_col4(int c0) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j < a.k ? c0 + j : 0;
+      nsg4[j] = (float)(-a.sigma[c]);
+      act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
+    }
+  }
+  __device__ void load4(long e, long i, Regs4& g) const {
+    g.r = *reinterpret_cast<const float4*>(R32 + e);
+    g.v = __ldcs(reinterpret_cast<const float4*>(V32 + e));
+    g.J = __ldg(J32 + i);
+  }
+  template <int NR1>
+  __device__ void compute4(Regs4& g, double (&ct)[NR1][4]) const {
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (act4[j]) {
+        const float ri = fadd(f4c(g.r, j), fmul(nsg4[j], f4c(g.v, j)));
+        f4s(g.r, j, ri);
+        const double z = dmul((double)ri, (double)g.J);
+        ct[0][j] = dmul((double)ri, z);
+        ct[1][j] = dmul((double)ri, (double)ri);
+      }
+  }
+  __device__ void store4(long e, const Regs4& g) const {
+    *reinterpret_cast<float4*>(R32 + e) = g.r;
+  }
   __device__ void finish_col(int c, double* tot) const {
     if (!a.active[c]) return;
     u.rz_prev[c] = a.alpha[c];
@@ -1121,6 +1331,46 @@ struct MOpRuDirection {
   __device__ void compute(long e, long, Regs& g, double*) const {
     if (dp) __stcs(D32 + e, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
     if (act) P32[e] = celg::R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  // 4 columns c0..c0+3 per lane (mtile4_kernel)
+  struct Regs4 { float4 p, r, d; float J; };
+  double bt4[4], sg4[4];
+  bool dp4[4], act4[4];
+  bool anyd = false, anya = false;
+  __device__ void begin_col4(int c0) {
+    const unsigned xm = *(volatile unsigned*)a.xmask;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j < a.k ? c0 + j : 0;
+      bt4[j] = a.beta[c];
+      sg4[j] = a.sigma[c];
+      act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
+      dp4[j] = c0 + j < a.k && ((xm >> c) & 1u) != 0;
+    }
+    anyd = dp4[0] || dp4[1] || dp4[2] || dp4[3];
+    anya = act4[0] || act4[1] || act4[2] || act4[3];
+  }
+  __device__ void load4(long e, long i, Regs4& g) const {
+    g.p = *reinterpret_cast<const float4*>(P32 + e);
+    if (anya) {
+      g.r = __ldcs(reinterpret_cast<const float4*>(R32 + e));
+      g.J = __ldg(J32 + i);
+    }
+    if (anyd) g.d = __ldcs(reinterpret_cast<const float4*>(D32 + e));
+  }
+  template <int NR1>
+  __device__ void compute4(Regs4& g, double (&)[NR1][4]) const {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const float pj = f4c(g.p, j);
+      if (dp4[j]) f4s(g.d, j, (float)dadd((double)f4c(g.d, j), dmul(sg4[j], (double)pj)));
+      if (act4[j])
+        f4s(g.p, j, celg::R<float>(dadd(dmul(bt4[j], D(pj)), dmul(D(f4c(g.r, j)), D(g.J)))));
+    }
+  }
+  __device__ void store4(long e, const Regs4& g) const {
+    if (anyd) __stcs(reinterpret_cast<float4*>(D32 + e), g.d);
+    if (anya) *reinterpret_cast<float4*>(P32 + e) = g.p;
   }
   __device__ void finish_col(int, double*) const {}
   __device__ void finish_global() const { *a.xmask = 0u; }
@@ -1370,11 +1620,22 @@ static int launch_spmm(celg_handle* h, const CsrDev& A, int k, const double* X, 
   }
 }
 
+// vec4: the op's FP32 arrays are 16-byte aligned (checked by the caller);
+// the 16-byte sweep then runs when k is a multiple of 4
 template <class Op>
-static int launch_mtile(celg_handle* h, long n, int k, const Op& op) {
+static int launch_mtile(celg_handle* h, long n, int k, const Op& op, bool vec4 = false) {
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
   red.sweep = next_sweep(h, false);
+  if constexpr (has_vec4<Op>::value) {
+    if (vec4 && (k & 3) == 0) {
+      const int grid =
+          grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile4_kernel<Op>>(kLanes, 0)));
+      mtile4_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
+      CELG_CUDA(cudaGetLastError());
+      return CELG_OK;
+    }
+  }
   const int grid = grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile_kernel<Op>>(kLanes, 0)));
   mtile_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
   CELG_CUDA(cudaGetLastError());
@@ -1715,6 +1976,8 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
   float* P32 = R32 + nk;
   float* V32 = P32 + nk;
   const float* J32 = m->jacobi32;
+  // the arrays start at multiples of n k floats from a cudaMalloc base
+  const bool vec4 = (k & 3) == 0 && (reinterpret_cast<uintptr_t>(F) & 15) == 0;
   const MOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, inner_eps, ai, ir.part, ir.part_count,
                           ir.tau_col};
   int st = launch_mtile(h, n, k, pre);
@@ -1723,8 +1986,8 @@ static int record_multi_inner(celg_handle* h, celg_mat* m, int k, float* F, size
   if (!st)
     st = multi_run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
       int s2 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ai}, cfg32);
-      if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate<float>{R32, V32, J32, ai, 0.0});
-      if (!s2) s2 = launch_mtile(h, n, k, MOpDirection<float>{P32, R32, J32, D32, ai});
+      if (!s2) s2 = launch_mtile(h, n, k, MOpUpdate32{{R32, V32, J32, ai, 0.0}}, vec4);
+      if (!s2) s2 = launch_mtile(h, n, k, MOpDirection32{{P32, R32, J32, D32, ai}}, vec4);
       return s2;
     });
   return st;
@@ -1932,6 +2195,9 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
   st = ensure_tuned32(h, mu, m, k, B, X, P32, V32, nk, a);
   if (st) return st;
   const int cfg32 = mu->cfg32;
+  // the FP32 work arrays start at multiples of n k floats from a cudaMalloc
+  // base: 16-byte aligned when k is a multiple of 4
+  const bool vec4 = (k & 3) == 0 && (reinterpret_cast<uintptr_t>(D32) & 15) == 0;
   auto setup = [&](const MultiArgs& ac) -> int {
     int s2 = launch_mtile(h, n, k, MOpPre<double>{B, X, p->x0_mode, p->eps_abs, p->eps_rel, ac});
     if (!s2) {
@@ -1949,14 +2215,14 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
       if (s2) return s2;
     }
     int s3 = launch_spmm_f32(h, m->csr, k, P32, MEpiAp<float>{V32, P32, k, ac}, cfg32);
-    if (!s3) s3 = launch_mtile(h, n, k, MOpRuStep{R32, V32, J32, ac, uc});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpRuStep{R32, V32, J32, ac, uc}, vec4);
     auto update = [&]() -> int {
       int s4 = launch_mtile(h, n, k, MOpRuFlush{X, D32, P32, ac, uc, 0});
       if (!s4) s4 = launch_spmm(h, m->csr, k, X, MEpiRuResidual{B, R32, nullptr, J32, k, ac, uc, 0}, cfg);
       return s4;
     };
     if (!s3) s3 = in_graph ? capture_if(h, uc.cond_update, update) : update();
-    if (!s3) s3 = launch_mtile(h, n, k, MOpRuDirection{P32, R32, J32, D32, ac});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpRuDirection{P32, R32, J32, D32, ac}, vec4);
     return s3;
   };
   auto tail = [&](const MultiArgs& ac) -> int {
