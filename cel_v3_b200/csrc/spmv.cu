@@ -47,8 +47,7 @@ int csr_compute_cap(celg_handle* h, CsrDev& A) {
   CELG_CUDA(cudaMemcpyAsync(&span, d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   CELG_CUDA(cudaStreamSynchronize(h->stream));
   int cap = std::max(16, (span + 3) & ~3);
-  // (dynamic shared memory per CTA; the kernel adds about 2 KB of static)
-  const int two_cta = 110 * 1024, one_cta = 224 * 1024;
+  const int two_cta = 113 * 1024, one_cta = 227 * 1024;
   if (csr_smem_bytes(cap, 8) > two_cta) {
     int lim = cap;
     while (lim > 16 && csr_smem_bytes(lim, 8) > one_cta) lim -= 64;

@@ -241,28 +241,6 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
   // ---------------- consumer warps (256 threads, lane j = row in sub-tile) ----
   const int j = threadIdx.x;
   int it = 0;
-  // Tile partials without a barrier per tile (as in tile_kernel): each warp
-  // folds its lanes of a tile with the butterfly and parks the warp sum; every
-  // kHeldTiles tiles (and at the end) the consumer warps meet once and add
-  // each tile's warp sums in warp order -- group_fold256's order and bits.
-  constexpr bool kHold = !kB && NR > 0;
-  constexpr int NR1 = NR > 0 ? NR : 1;
-  __shared__ double held[kHold ? kHeldTiles : 1][NR1][8];
-  __shared__ long held_tile[kHold ? kHeldTiles : 1];
-  [[maybe_unused]] int nheld = 0;
-  [[maybe_unused]] auto flush = [&]() {
-    named_bar_sync(1, kLanes);
-    for (int q = j; q < nheld * NR1; q += kLanes) {
-      const int sl = q / NR1, r = q % NR1;
-      double tot = held[sl][r][0];
-#pragma unroll
-      for (int w = 1; w < 8; ++w) tot = dadd(tot, held[sl][r][w]);
-      red.partials[(long)r * red.ntiles + held_tile[sl]] = tot;
-    }
-    __threadfence();  // every writer's partials visible before the grid's ticket
-    named_bar_sync(1, kLanes);
-    nheld = 0;
-  };
   Epi ep = epi;
   TileInfo nxt{0, 0.0};
   if constexpr (kB) {
@@ -408,16 +386,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       if (lane == 0) mbar_arrive(&empty[st]);
       ++it;
     }
-    if constexpr (kHold) {
-      if (nheld == kHeldTiles) flush();
-#pragma unroll
-      for (int r = 0; r < NR1; ++r) {
-        const double w = warp_fold(acc.a[r]);
-        if (lane == 0) held[nheld][r][warp] = w;
-      }
-      if (j == 0) held_tile[nheld] = t;
-      ++nheld;
-    } else if (NR > 0) {
+    if (NR > 0) {
 #pragma unroll
       for (int r = 0; r < (NR > 0 ? NR : 1); ++r) {
         const double tot = group_fold256(acc.a[r], scratch, j, 1);
@@ -426,7 +395,8 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
       // batched: the systems are completed by batch_finish_kernel
     }
   }
-  if constexpr (kHold) flush();
+  // (Tile partials parked per warp with one barrier per 16 tiles, as in
+  // tile_kernel, made the 256^3 FP64 sweep slower here: 197 -> 206 us.)
   if constexpr (!kB && NR > 0) {
     double tot[NR > 0 ? NR : 1];
     if (red.finish && grid_finish<(NR > 0 ? NR : 1)>(red, tot, scratch, s_flag, j, 1)) ep.finish(tot);
