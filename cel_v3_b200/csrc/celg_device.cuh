@@ -171,6 +171,16 @@ __device__ __forceinline__ double vmul<double>(double a, double b) { return __dm
 template <>
 __device__ __forceinline__ float vmul<float>(float a, float b) { return __fmul_rn(a, b); }
 
+// acc + a b accumulated as dadd(acc, dmul(a, b)).  With float operands the
+// product is exact in double (24 + 24 significant bits), so one fused
+// multiply-add gives the same bits with one rounding instruction less.
+__device__ __forceinline__ double dacc_prod(double acc, float a, float b) {
+  return __fma_rn((double)a, (double)b, acc);
+}
+__device__ __forceinline__ double dacc_prod(double acc, double a, double b) {
+  return dadd(acc, dmul(a, b));
+}
+
 __device__ __forceinline__ double warp_fold(double v) {
 #pragma unroll
   for (int off = 16; off >= 1; off >>= 1) v = dadd(v, __shfl_xor_sync(0xffffffffu, v, off));

@@ -174,7 +174,7 @@ struct EpiAp {
   __device__ void row(long i, VT s, double* acc) const {
     const VT vi = vadd(VT(0), s);
     v[i] = vi;
-    acc[0] = dadd(acc[0], dmul(D(vi), D(__ldg(p + i))));
+    acc[0] = dacc_prod(acc[0], vi, __ldg(p + i));
   }
   __device__ void finish(double* tot) const {
     PcgState* st = a.st;

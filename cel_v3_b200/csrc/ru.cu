@@ -169,7 +169,7 @@ struct OpRuStep {
     r[i] = ri;
     const double z = dmul((double)ri, (double)g.J);
     acc[0] = dadd(acc[0], dmul((double)ri, z));
-    acc[1] = dadd(acc[1], dmul((double)ri, (double)ri));
+    acc[1] = dacc_prod(acc[1], ri, ri);
   }
   __device__ void finish(double* tot) const {
     RuState* st = a.st;
