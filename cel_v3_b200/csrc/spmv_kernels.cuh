@@ -280,6 +280,33 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
         int len[kPR], vb[kPR], fbr[kPR];
         // row indices as unsigned: s0 * kSub + j < n + kPR * kSub < 2^32
         const unsigned row0 = (unsigned)s0 * (unsigned)kSub + (unsigned)j;
+        // a full pass -- kPR whole sub-tiles, all staged -- runs without
+        // per-row bound and fallback tests (the same sums)
+        bool full_pass = nr == kPR && (s0 + kPR) * kSub <= (long)n;
+#pragma unroll
+        for (int r = 0; r < kPR; ++r) full_pass = full_pass && meta[2 * stg[r] + 1] == 0;
+        if (full_pass) {
+          const VT* vsr[kPR];
+#pragma unroll
+          for (int r = 0; r < kPR; ++r) {
+            const unsigned char* sb = stages + (size_t)stg[r] * L.bytes;
+            const int* rps = reinterpret_cast<const int*>(sb);
+            const int b = rps[j];
+            len[r] = rps[j + 1] - b;
+            vsr[r] = reinterpret_cast<const VT*>(sb + L.v_off) + (b - meta[2 * stg[r]]);
+            const int4* pq =
+                reinterpret_cast<const int4*>(s_dict + (int)(sb + L.ci_off)[j] * kPatLen);
+            const int4 q0 = pq[0], q1 = pq[1];
+            const int po[kPatLen] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+            const VT* xr = x + (row0 + (unsigned)(r * kSub));
+#pragma unroll
+            for (int u = 0; u < kPatLen; ++u) xv[r][u] = ldg_at(xr, po[u]);
+          }
+#pragma unroll
+          for (int r = 0; r < kPR; ++r)
+            ep.row((long)(row0 + (unsigned)(r * kSub)), pat_dot_len<false>(len[r], vsr[r], xv[r]),
+                   acc.a);
+        } else {
 #pragma unroll
         for (int r = 0; r < kPR; ++r) {
           len[r] = 0;
@@ -316,6 +343,7 @@ __global__ void __launch_bounds__(kCsrThreads, sizeof(VT) == 4 ? 4 : (sizeof(CT)
                              xv[r]);
             ep.row((long)row, sum, acc.a);
           }
+        }
         }
         __syncwarp();
         if (lane == 0) {
