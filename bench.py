@@ -324,10 +324,17 @@ def batch_form(h, celgpu, torch, stream):
     def batched_fp32_ir():
         return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p32)
 
+    # FP32 PCG with FP64 reliable updates of every system
+    p32ru = celgpu.params(eps_rel=1e-8, iter_max=5000, x0_mode=celgpu.X0_ZERO,
+                          precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
+
+    def batched_fp32_ru():
+        return h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], p32ru)
+
     out = {}
     x64 = None
     for name, fn in (("one_by_one", one_by_one), ("batched", batched),
-                     ("batched_fp32_ir", batched_fp32_ir)):
+                     ("batched_fp32_ir", batched_fp32_ir), ("batched_fp32_ru", batched_fp32_ru)):
         fn()
         torch.cuda.synchronize()
         reps = 3
@@ -344,10 +351,12 @@ def batch_form(h, celgpu, torch, stream):
                      "all_ok": all(i.status == celgpu.OK for i in infos)}
         if name == "batched":
             x64 = [x.clone() for x in xs]
-        elif name == "batched_fp32_ir":
+        elif name in ("batched_fp32_ir", "batched_fp32_ru"):
             out[name]["worst_err_vs_fp64"] = max(rel_err(x, y) for x, y in zip(xs, x64))
     out["speedup_batched_vs_one_by_one"] = out["batched"]["solves_per_s"] / out["one_by_one"]["solves_per_s"]
     out["speedup_batched_fp32_ir_vs_one_by_one"] = (out["batched_fp32_ir"]["solves_per_s"] /
+                                                    out["one_by_one"]["solves_per_s"])
+    out["speedup_batched_fp32_ru_vs_one_by_one"] = (out["batched_fp32_ru"]["solves_per_s"] /
                                                     out["one_by_one"]["solves_per_s"])
     out["systems"] = len(mats)
     out["rows"] = int(sum(s ** 3 for s, *_ in probs))
@@ -521,6 +530,7 @@ def forms_summary(forms, value):
         "fp64_diffusion_solves_s": g("precision_diffusion256", "fp64_pcg", "solves_per_s"),
         "batched_x": g("batched_64", "speedup_batched_vs_one_by_one"),
         "batched_fp32_ir_x": g("batched_64", "speedup_batched_fp32_ir_vs_one_by_one"),
+        "batched_fp32_ru_x": g("batched_64", "speedup_batched_fp32_ru_vs_one_by_one"),
         "multirhs_x": g("multirhs_128_k32", "speedup_multirhs_vs_one_by_one"),
         "multirhs_fp32_ir_x": g("multirhs_128_k32", "speedup_multirhs_fp32_ir_vs_one_by_one"),
         "multirhs_fp32_ru_x": g("multirhs_128_k32", "speedup_multirhs_fp32_ru_vs_one_by_one"),

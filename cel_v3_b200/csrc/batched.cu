@@ -397,6 +397,242 @@ __global__ void ir_count_kernel(int nsys, IrState ir, const int* inner_iter, con
 
 // ---- completion of a batched sweep ------------------------------------------------
 
+// ---- FP32 PCG with FP64 reliable updates of every system (CELG_PREC_FP32_RU) ---
+// The recurrence of ru_solve (ru.cu) for all systems at once: one FP32 SpMV
+// and vector sweep pair per iteration over the concatenated systems, and the
+// FP64 correction of the systems that are due, under one IF node.  Each
+// system's reductions are the single solve's (per-system finishers), so each
+// system's result equals ru_solve on it alone, bit for bit.
+
+struct BatchRu {
+  double* maxr;     // ||r64|| at the system's last reliable update
+  double* rz_prev;  // rz before the system's current step
+  double* norm64;   // the system's last FP64 residual norm
+  int* updates;     // reliable updates so far (the set-up residual included)
+  int* upd;         // the system's reliable update is due
+  int* n_upd;       // some system's update is due
+  double delta;
+  cudaGraphConditionalHandle cond_update;  // IF node of the update (0: none)
+};
+
+__device__ __forceinline__ int bru_go(const BatchArgs& a, const BatchRu& u, int s) {
+  return (a.err[s] == 0 && *(volatile const int*)a.errw == 0 && a.iter[s] < a.iter_max &&
+          u.norm64[s] > a.eps[s])
+             ? 1
+             : 0;
+}
+
+// set-up: every system with rows starts with a reliable update
+__global__ void bru_init_kernel(int nsys, const int* sys_ntiles, BatchRu u) {
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x) {
+    u.updates[s] = 0;
+    u.upd[s] = sys_ntiles[s] > 0 ? 1 : 0;
+  }
+  if (threadIdx.x == 0) *u.n_upd = 1;
+}
+
+// the flushed systems owe no d += sigma p any more
+__global__ void bru_clear_kernel(int nsys, int* xpend, const int* upd) {
+  for (int s = threadIdx.x; s < nsys; s += blockDim.x)
+    if (upd[s]) xpend[s] = 0;
+}
+
+// FP64 residual of the systems due for an update, and its FP32 copy:
+//   r64 = b - (0 + A x);  r = (float) r64;  z = (double) r * J;  rz = r.z;  ||r64||^2
+// init: also p = (float) z.
+struct BEpiRuResidual {
+  static constexpr int NRED = 2;
+  static constexpr bool kBatched = true;
+  const double* b;
+  float* r;
+  float* p;  // set-up only
+  const float* J;
+  BatchArgs a;
+  BatchRu u;
+  int init;
+  __device__ bool active() const { return *(volatile int*)u.n_upd != 0; }
+  __device__ TileInfo tile_info(long t) const {
+    return TileInfo{*(volatile int*)&u.upd[a.sys_of(t)], 0.0};
+  }
+  __device__ void begin_tile(const TileInfo&) {}
+  __device__ bool sys_active(int s) const { return *(volatile int*)&u.upd[s] != 0; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void row(long i, double s, double* acc) const {
+    const double r64 = __dsub_rn(b[i], dadd(0.0, s));
+    const float rf = (float)r64;
+    r[i] = rf;
+    const double z = dmul((double)rf, (double)J[i]);
+    if (init) p[i] = (float)z;
+    acc[0] = dadd(acc[0], dmul((double)rf, z));
+    acc[1] = dadd(acc[1], dmul(r64, r64));
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    u.norm64[s] = sqrt(tot[1]);
+    u.maxr[s] = u.norm64[s];
+    u.upd[s] = 0;
+    u.updates[s] += 1;
+    if (init) {
+      a.alpha[s] = tot[0];
+      a.norm[s] = u.norm64[s];
+    } else {
+      a.beta[s] = tot[0] / u.rz_prev[s];
+      a.alpha[s] = tot[0];
+    }
+    if (!bru_go(a, u, s) && a.active[s]) {
+      a.active[s] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {
+    *u.n_upd = 0;
+    set_cond(a.cond, *(volatile int*)a.n_active > 0);
+  }
+};
+
+// r -= sigma v in FP32 arithmetic; rz' = r.J r, ||r||^2; the system's update
+// decision.  d += sigma p is left pending (xpend) for the flush or the
+// direction sweep.
+struct BOpRuStep {
+  static constexpr int NRED = 2;
+  static constexpr bool kBatched = true;
+  struct Regs { float r, v, J; };
+  float* r;
+  const float* v;
+  const float* J;
+  BatchArgs a;
+  BatchRu u;
+  float nsg = 0.0f;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    return TileInfo{*(volatile int*)&a.active[s], a.sigma[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) { nsg = (float)(-ti.s); }
+  __device__ bool sys_active(int s) const { return *(volatile int*)&a.active[s] != 0; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const {
+    g.r = r[i];
+    g.v = __ldcs(v + i);
+    g.J = __ldg(J + i);
+  }
+  __device__ void compute(long i, Regs& g, double* acc) const {
+    const float ri = fadd(g.r, fmul(nsg, g.v));
+    r[i] = ri;
+    const double z = dmul((double)ri, (double)g.J);
+    acc[0] = dadd(acc[0], dmul((double)ri, z));
+    acc[1] = dacc_prod(acc[1], ri, ri);
+  }
+  __device__ void finish_sys(int s, double* tot) const {
+    u.rz_prev[s] = a.alpha[s];
+    a.beta[s] = tot[0] / a.alpha[s];
+    a.alpha[s] = tot[0];
+    a.norm[s] = sqrt(tot[1]);
+    a.iter[s] += 1;
+    a.xpend[s] = 1;
+    const int upd = (a.norm[s] < u.delta * u.maxr[s]) || (a.norm[s] <= a.eps[s]) ||
+                    (a.iter[s] >= a.iter_max);
+    if (upd) {
+      u.upd[s] = 1;
+      atomicAdd(u.n_upd, 1);
+    } else if (!(a.err[s] == 0 && *(volatile const int*)a.errw == 0 && a.iter[s] < a.iter_max &&
+                 fabs(a.alpha[s]) > 0.0)) {
+      a.active[s] = 0;
+      atomicSub(a.n_active, 1);
+    }
+  }
+  __device__ void finish_global() const {
+    set_cond(u.cond_update, *(volatile int*)u.n_upd > 0);
+    set_cond(a.cond, *(volatile int*)a.n_active > 0);
+  }
+};
+
+// x64 += (double) d ; d = 0 for the systems due for an update (every system
+// with `always`).  A pending d += sigma p is applied first, with the step's
+// rounding.  TileInfo.act: bit 0 flush, bit 1 d += sigma p pending.
+struct BOpRuFlush {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { double x; float d, p; };
+  double* x;
+  float* d;
+  const float* p;  // null: nothing pending (the final flush)
+  BatchArgs a;
+  BatchRu u;
+  int always;
+  int dp = 0;
+  double sg = 0.0;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    const int f = (always || *(volatile int*)&u.upd[s] != 0 ? 1 : 0) |
+                  (p != nullptr && *(volatile int*)&a.xpend[s] != 0 ? 2 : 0);
+    return TileInfo{f & 1 ? f : 0, a.sigma[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) {
+    dp = ti.act & 2;
+    sg = ti.s;
+  }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const {
+    g.x = x[i];
+    g.d = d[i];
+    if (dp) g.p = __ldg(p + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    const float di = dp ? (float)dadd((double)g.d, dmul(sg, (double)g.p)) : g.d;
+    x[i] = dadd(g.x, (double)di);
+    d[i] = 0.0f;
+  }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// d += sigma p where the step left it pending, then p = beta p + J r while
+// the system goes on (TileInfo.act: bit 0 active, bit 1 pending; s = beta,
+// s2 = sigma).  The marks are cleared by clear_marks_kernel after the sweep.
+struct BOpRuDirection {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { float p, r, J, d; };
+  float* p;
+  const float* r;
+  const float* J;
+  float* d;
+  BatchArgs a;
+  double bt = 0.0, sg = 0.0;
+  int act = 0, dp = 0;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    const int f = (*(volatile int*)&a.active[s] != 0 ? 1 : 0) |
+                  (*(volatile int*)&a.xpend[s] != 0 ? 2 : 0);
+    return TileInfo{f, a.beta[s], a.sigma[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) {
+    act = ti.act & 1;
+    dp = ti.act & 2;
+    bt = ti.s;
+    sg = ti.s2;
+  }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const {
+    g.p = p[i];
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldg(J + i);
+    }
+    if (dp) g.d = __ldcs(d + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (dp) __stcs(d + i, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
+    if (act) p[i] = R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
 // One CTA per system: if the system took part, its tile partials are reduced
 // in the single-solve order (lane j sums partials j, j+256, ... from 0.0;
 // butterfly; warps in order) and finish_sys runs; the last CTA to arrive
@@ -479,6 +715,10 @@ struct Batch {
   double* irtau = nullptr;     // inner tolerance per system
   double* dstate2 = nullptr;   // inner-solve scalars, 7 x nsys
   int* istate2 = nullptr;      // inner-solve counters, 4 x nsys + 1
+  // FP32 with reliable updates: maxr, rz_prev, norm64 (nsys each); updates,
+  // upd (nsys each), n_upd
+  double* rud = nullptr;
+  int* rui = nullptr;
 };
 
 namespace celg {
@@ -505,6 +745,8 @@ void batch_free(Batch* b) {
   cudaFree(b->irtau);
   cudaFree(b->dstate2);
   cudaFree(b->istate2);
+  cudaFree(b->rud);
+  cudaFree(b->rui);
   delete b;
 }
 
@@ -814,10 +1056,13 @@ static int batch_for(celg_handle* h, int count, celg_mat* const* mats, const dou
 
 static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
                           double* const* x_d, const celg_params* p, celg_result* res);
+static int pcg_batched_ru(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                          double* const* x_d, const celg_params* p, celg_result* res);
 
 int pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
                 double* const* x_d, const celg_params* p, celg_result* res) {
   if (p->precision == CELG_PREC_FP32_IR) return pcg_batched_ir(h, count, mats, b_d, x_d, p, res);
+  if (p->precision == CELG_PREC_FP32_RU) return pcg_batched_ru(h, count, mats, b_d, x_d, p, res);
   if (p->precision != CELG_PREC_FP64) return CELG_ERR_ARG;
   Batch* bt = nullptr;
   int st = batch_for(h, count, mats, b_d, x_d, &bt);
@@ -1079,6 +1324,184 @@ static int pcg_batched_ir(celg_handle* h, int count, celg_mat* const* mats, cons
     }
   }
   h->last_iters = inner_max_total;
+  return ret;
+}
+
+// FP32 PCG with FP64 reliable updates of every system: one graph launch with
+// a WHILE node over { FP32 SpMV, step, IF(some system due) { flush, FP64
+// residual }, direction }; self-skipping sweeps from a host loop when graphs
+// are off.
+static int record_batched_ru(celg_handle* h, Batch* bt, const double* const* b_d, double* const* x_d,
+                             const celg_params* p, BatchArgs a, BatchRu u) {
+  const long N = bt->N;
+  float* D32 = bt->F + N;
+  float* R32 = D32 + N;
+  float* P32 = R32 + N;
+  float* V32 = P32 + N;
+  const float* J32 = bt->J32;
+  for (int s = 0; s < bt->nsys; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(bt->B + bt->row_off[s], b_d[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+    if (p->x0_mode == CELG_X0_USER)
+      CELG_CUDA(cudaMemcpyAsync(bt->X + bt->row_off[s], x_d[s], sizeof(double) * (size_t)bt->n[s],
+                                cudaMemcpyDeviceToDevice, h->stream));
+  }
+  // x0, ||b||, eps; every system starts with a reliable update (its residual)
+  const BOpPre<double> pre{bt->B, bt->X, p->x0_mode, p->eps_abs, p->eps_rel, a};
+  int st = launch_tile(h, N, pre);
+  if (!st) st = batch_finish(h, bt, pre);
+  if (!st) {
+    bru_init_kernel<<<1, kLanes, 0, h->stream>>>(bt->nsys, a.br.sys_ntiles, u);
+    CELG_CUDA(cudaGetLastError());
+    CELG_CUDA(cudaMemsetAsync(D32, 0, sizeof(float) * (size_t)std::max(1L, N), h->stream));
+    const BEpiRuResidual r0{bt->B, R32, P32, J32, a, u, 1};
+    st = batch_csr<double>(h, bt, bt->A.v, bt->X, r0);
+    if (!st) st = batch_finish(h, bt, r0);
+  }
+  auto body = [&](bool in_graph) -> int {
+    BatchRu uc = u;
+    if (in_graph) {
+      int s2 = capture_new_handle(h, 0, &uc.cond_update);
+      if (s2) return s2;
+    }
+    const BEpiAp<float> ap{V32, P32, a};
+    const BOpRuStep step{R32, V32, J32, a, uc, 0.0f};
+    int s3 = batch_csr<float>(h, bt, bt->A.v32, P32, ap);
+    if (!s3) s3 = batch_finish(h, bt, ap);
+    if (!s3) s3 = batch_tile(h, bt, step);
+    if (!s3) s3 = batch_finish(h, bt, step);
+    auto update = [&]() -> int {
+      int s4 = batch_tile(h, bt, BOpRuFlush{bt->X, D32, P32, a, uc, 0});
+      if (!s4) {
+        bru_clear_kernel<<<1, kLanes, 0, h->stream>>>(bt->nsys, a.xpend, uc.upd);
+        CELG_CUDA(cudaGetLastError());
+      }
+      const BEpiRuResidual rr{bt->B, R32, nullptr, J32, a, uc, 0};
+      if (!s4) s4 = batch_csr<double>(h, bt, bt->A.v, bt->X, rr);
+      if (!s4) s4 = batch_finish(h, bt, rr);
+      return s4;
+    };
+    if (!s3) s3 = in_graph ? capture_if(h, uc.cond_update, update) : update();
+    if (!s3) s3 = batch_tile(h, bt, BOpRuDirection{P32, R32, J32, D32, a});
+    if (!s3) s3 = clear_marks(h, a);
+    return s3;
+  };
+  if (!st && a.cond) st = capture_while2(h, a.cond, [&]() -> int { return body(true); });
+  for (int it = 0; !st && !a.cond && it < p->iter_max; it += 8) {
+    for (int q = 0; q < 8 && !st; ++q) st = body(false);
+    int live = 0;
+    if (!st) {
+      CELG_CUDA(cudaMemcpyAsync(&live, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      CELG_CUDA(cudaStreamSynchronize(h->stream));
+    }
+    if (!live) break;
+  }
+  // x64 += d for every system, then the FP64 check
+  if (!st) st = batch_tile(h, bt, BOpRuFlush{bt->X, D32, nullptr, a, u, 1});
+  const BEpiVerify ver{bt->B, a};
+  if (!st) st = batch_csr<double>(h, bt, bt->A.v, bt->X, ver);
+  if (!st) st = batch_finish(h, bt, ver);
+  if (st) return st;
+  for (int s = 0; s < bt->nsys; ++s) {
+    if (bt->n[s] == 0) continue;
+    CELG_CUDA(cudaMemcpyAsync(x_d[s], bt->X + bt->row_off[s], sizeof(double) * (size_t)bt->n[s],
+                              cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return CELG_OK;
+}
+
+static int pcg_batched_ru(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
+                          double* const* x_d, const celg_params* p, celg_result* res) {
+  Batch* bt = nullptr;
+  int st = batch_for(h, count, mats, b_d, x_d, &bt);
+  if (!st) st = ensure_partials(h, bt->NT, 2);
+  if (!st) st = batch_tune(h, bt, b_d);
+  if (!st) st = batch_ensure_f32(h, bt);
+  if (st) return st;
+  const int c = bt->nsys;
+  if (!bt->rud) {
+    CELG_CUDA(cudaMalloc(&bt->rud, sizeof(double) * 3 * (size_t)c));
+    CELG_CUDA(cudaMalloc(&bt->rui, sizeof(int) * (2 * (size_t)c + 1)));
+  }
+  BatchRu u;
+  u.maxr = bt->rud;
+  u.rz_prev = u.maxr + c;
+  u.norm64 = u.rz_prev + c;
+  u.updates = bt->rui;
+  u.upd = u.updates + c;
+  u.n_upd = u.upd + c;
+  u.delta = p->inner_eps_rel > 0 ? p->inner_eps_rel : 1e-2;
+  u.cond_update = 0;
+  CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
+  std::string gkey = bt->key;
+  char buf[96];
+  for (int s = 0; s < count; ++s) {
+    std::snprintf(buf, sizeof(buf), "|%p|%p", (const void*)b_d[s], (const void*)x_d[s]);
+    gkey += buf;
+  }
+  std::snprintf(buf, sizeof(buf), "|ru|%d|%.17g|%.17g|%.17g|%d", p->x0_mode, p->eps_abs, p->eps_rel,
+                u.delta, p->iter_max);
+  gkey += buf;
+  if (!graphs_enabled()) {
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    st = record_batched_ru(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, 0, h->err_d), u);
+    if (st) return st;
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  } else {
+    GraphEntry* ge = graph_cache_find(h, gkey);
+    if (!ge) {
+      st = graph_build(h, gkey, [&](cudaGraphConditionalHandle cond) -> int {
+        return record_batched_ru(h, bt, b_d, x_d, p, batch_args(bt, p->iter_max, cond, h->err_d), u);
+      }, &ge);
+      if (st) return st;
+    }
+    CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    CELG_CUDA(cudaGraphLaunch(ge->exec, h->stream));
+    CELG_CUDA(cudaEventRecord(h->ev1, h->stream));
+  }
+  std::vector<double> ds(7 * (size_t)c), rd(3 * (size_t)c);
+  std::vector<int> is(3 * (size_t)c + 1), ri(2 * (size_t)c + 1);
+  CELG_CUDA(cudaMemcpyAsync(ds.data(), bt->dstate, sizeof(double) * ds.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(is.data(), bt->istate, sizeof(int) * is.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(rd.data(), bt->rud, sizeof(double) * rd.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  CELG_CUDA(cudaMemcpyAsync(ri.data(), bt->rui, sizeof(int) * ri.size(), cudaMemcpyDeviceToHost,
+                            h->stream));
+  int err_word = 0;
+  CELG_CUDA(cudaMemcpyAsync(&err_word, h->err_d, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  CELG_CUDA(cudaStreamSynchronize(h->stream));
+  cudaEventElapsedTime(&h->last_ms, h->ev0, h->ev1);
+  if (err_word) return err_word;
+  int ret = CELG_OK, iters = 0;
+  for (int s = 0; s < c; ++s) {
+    if (bt->n[s] == 0) {
+      if (res) {
+        std::memset(&res[s], 0, offsetof(celg_result, history));
+        res[s].history_len = 0;
+      }
+      continue;
+    }
+    const double norm64 = rd[2 * (size_t)c + s], eps = ds[5 * (size_t)c + s];
+    const int it = is[(size_t)s], err = is[2 * (size_t)c + s];
+    int rs = CELG_OK;
+    if (err) rs = err;
+    else if (!(norm64 <= eps)) rs = CELG_ERR_NOCONV;
+    if (rs && !ret) ret = rs;
+    iters = std::max(iters, it);
+    if (res) {
+      res[s].iter_done = it;
+      res[s].final_norm2 = norm64;
+      res[s].bnorm = ds[4 * (size_t)c + s];
+      res[s].verified_relres = ds[6 * (size_t)c + s];
+      res[s].err = rs;
+      res[s].arnoldi_steps = ri[(size_t)s];
+      res[s].history_len = 0;
+    }
+  }
+  h->last_iters = iters;
   return ret;
 }
 

@@ -249,10 +249,13 @@ int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const double* b_hos
  * nullable) receives the per-system reports; history is not recorded.  Each
  * system's result is bit-identical to celg_pcg_jacobi on it alone.  The
  * concatenated copy of the matrices is cached on the handle until another
- * batch or a celg_mat_destroy.  precision CELG_PREC_FP64 or CELG_PREC_FP32_IR
+ * batch or a celg_mat_destroy.  precision CELG_PREC_FP64, CELG_PREC_FP32_IR
  * (FP32 inner solves inside FP64 refinement of every system: iter_done is
  * then the outer step count, arnoldi_steps the inner iterations, as for
- * celg_pcg_jacobi); CELG_PREC_FP32_RU is not offered for batches. */
+ * celg_pcg_jacobi) or CELG_PREC_FP32_RU (FP32 PCG with FP64 reliable updates
+ * of every system: arnoldi_steps = reliable updates, final_norm2 = the last
+ * FP64 residual norm); each system's result equals celg_pcg_jacobi with the
+ * same precision on it alone, bit for bit. */
 int celg_pcg_batched(celg_handle* h, int count, celg_mat* const* mats, const double* const* b_d,
                      double* const* x_d, const celg_params* p, celg_result* res);
 

@@ -107,6 +107,44 @@ def test_batched_fp32_refinement_matches_single_refinement(gpu, mode, monkeypatc
         m.destroy()
 
 
+@pytest.mark.parametrize("mode", ["graph", "host_loop"])
+@pytest.mark.parametrize("iter_max", [3000, 7])
+def test_batched_fp32_reliable_updates_match_single_solves(gpu, mode, iter_max, monkeypatch):
+    """FP32 PCG with FP64 reliable updates of the whole batch
+    (CELG_PREC_FP32_RU): each system's solution, iteration and update counts,
+    last FP64 residual norm, status and verified residual equal the single
+    reliable-update solve's bit for bit, also when the iteration cap forces
+    the last update; an empty system is skipped."""
+    celgpu, h, torch = gpu
+    if mode == "host_loop":
+        monkeypatch.setenv("CELG_GRAPH", "0")
+    sy = systems()
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+    empty = h.matrix_from_csr(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0)).jacobi()
+    bs = [dev(torch, b) for *_, b in sy]
+    xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    kw = dict(eps_rel=1e-10, iter_max=iter_max, precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2,
+              x0_mode=celgpu.X0_ZERO)
+    infos = h.pcg_batched(mats + [empty], [b.data_ptr() for b in bs] + [0],
+                          [x.data_ptr() for x in xs] + [0], **kw)
+    for s, ((rp, ci, v, b), m) in enumerate(zip(sy, mats)):
+        xo = dev(torch, np.zeros(b.size))
+        one = h.pcg_jacobi(m, bs[s].data_ptr(), xo.data_ptr(), **kw)
+        assert infos[s].status == one.status, s
+        assert infos[s].iter_done == one.iter_done, s
+        assert infos[s].arnoldi_steps == one.arnoldi_steps, s      # reliable updates
+        assert infos[s].final_norm2 == one.final_norm2, s
+        assert infos[s].verified_relres == one.verified_relres, s
+        assert np.array_equal(xs[s].cpu().numpy(), xo.cpu().numpy()), s
+        if iter_max == 3000:
+            assert one.status == celgpu.OK and one.verified_relres <= 1e-10
+        else:
+            assert one.status == celgpu.ERR_NOCONV and one.iter_done == iter_max
+    assert infos[-1].iter_done == 0 and infos[-1].status == celgpu.OK
+    for m in mats + [empty]:
+        m.destroy()
+
+
 def test_batched_launch_shapes_give_the_same_bits(gpu, monkeypatch):
     """Every launch shape the batch tuner chooses from (CTAs per SM of the
     SpMV and vector sweeps, forced with CELG_BATCH_SHAPE on a fresh handle)
