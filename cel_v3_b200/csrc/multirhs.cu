@@ -677,39 +677,41 @@ __global__ void __launch_bounds__(kLanes) mtile_kernel(long n, int k, Op op_in, 
   else multi_grid_finish<1>(red, op, 0, scratch, &s_flag, s_tot);
 }
 
-// The same sweeps for FP32 storage with 16-byte accesses (k a multiple of 4,
-// the arrays 16-byte aligned): in a step of 4 rows, lane l works on row
-// l / 8 of the step and columns 4 (l % 8) .. 4 (l % 8) + 3, so every load and
-// store moves 16 bytes per lane instead of 4.  An op with 4-column methods
-// (load4, begin_col4, compute4, store4) returns each element's reduction
-// terms; they are transposed through shared memory to lane = column and
-// added in row order there, so the per-column sums keep the order (and the
-// bits) of mtile_kernel.
+// The same sweeps with 16-byte accesses (k a multiple of W = 16 / element
+// size, the arrays 16-byte aligned): in a step of W rows, lane l works on row
+// l / (32 / W) of the step and the W columns W (l % (32 / W)) .. + W - 1, so
+// every load and store moves 16 bytes per lane (FP32: 4 columns, FP64: 2).
+// An op with W-column methods (loadv, begin_colv, computev, storev; kVecW)
+// returns each element's reduction terms; they are transposed through
+// shared memory to lane = column and added in row order there, so the
+// per-column sums keep the order (and the bits) of mtile_kernel.
 template <class T, class = void>
-struct has_vec4 : std::false_type {};
+struct has_vecw : std::false_type {};
 template <class T>
-struct has_vec4<T, std::void_t<decltype(&T::store4)>> : std::true_type {};
+struct has_vecw<T, std::void_t<decltype(&T::storev)>> : std::true_type {};
 
 template <class Op>
 __global__ void __launch_bounds__(kLanes) mtile4_kernel(long n, int k, Op op_in, RedCtx red) {
-  // 4-row steps whose loads are in flight together (128^3 x 32 reliable-
-  // update step: 233 / 204 / 193 / 183 us for 1 / 2 / 4 / 8; direction sweep
-  // 226 / 215 / 216 / 226 us)
+  constexpr int W = Op::kVecW;
+  static_assert(W == 2 || W == 4, "16-byte vectors of FP64 or FP32");
+  // W-row steps whose loads are in flight together (FP32, 128^3 x 32
+  // reliable-update step: 233 / 204 / 193 / 183 us for 1 / 2 / 4 / 8;
+  // direction sweep 226 / 215 / 216 / 226 us)
   constexpr int RV = 4;
-  static_assert(32 % (4 * RV) == 0, "steps tile the warp's 32 rows");
+  static_assert(32 % (W * RV) == 0, "steps tile the warp's 32 rows");
   constexpr int NR = Op::NRED;
   constexpr int NR1 = NR > 0 ? NR : 1;
   __shared__ double s_w[NR1 * 8 * 32];
   __shared__ double scratch[8];
   __shared__ double s_tot[NR1 * kMaxRhs];
   __shared__ int s_flag;
-  __shared__ __align__(16) double s_c[NR > 0 ? 8 : 1][NR1][4][32];
+  __shared__ __align__(16) double s_c[NR > 0 ? 8 : 1][NR1][W][32];
   Op op = op_in;
   if (!op.prepare()) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gr = lane >> 3, c0 = 4 * (lane & 7);
+  const int gr = lane / (32 / W), c0 = W * (lane % (32 / W));
   const bool von = c0 < k;
-  op.begin_col4(von ? c0 : 0);
+  op.begin_colv(von ? c0 : 0);
   const long ntiles = (n + kTile - 1) / kTile;
   for (long kt = blockIdx.x; kt < ntiles; kt += gridDim.x) {
     const long t = tile_at(kt, ntiles, red.sweep);
@@ -719,40 +721,40 @@ __global__ void __launch_bounds__(kLanes) mtile4_kernel(long n, int k, Op op_in,
     for (int q = 0; q < 4; ++q) {
       const long row0 = t * kTile + q * kSub + warp * 32;
       if (row0 >= n) break;
-      for (int r16 = 0; r16 < 32; r16 += 4 * RV) {
+      for (int r16 = 0; r16 < 32; r16 += W * RV) {
         // the loads of RV steps are issued before the first is used
-        typename Op::Regs4 g[RV];
+        typename Op::RegsV g[RV];
 #pragma unroll
         for (int v = 0; v < RV; ++v) {
-          const long i = row0 + r16 + 4 * v + gr;
-          if (von && i < n) op.load4(i * k + c0, i, g[v]);
+          const long i = row0 + r16 + W * v + gr;
+          if (von && i < n) op.loadv(i * k + c0, i, g[v]);
         }
 #pragma unroll
         for (int v = 0; v < RV; ++v) {
-        const int r4 = r16 + 4 * v;
+        const int r4 = r16 + W * v;
         const long i = row0 + r4 + gr;
         const bool ok = von && i < n;
-        double ct[NR1][4];
+        double ct[NR1][W];
 #pragma unroll
         for (int r = 0; r < NR1; ++r)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) ct[r][j] = 0.0;
+          for (int j = 0; j < W; ++j) ct[r][j] = 0.0;
         if (ok) {
-          op.template compute4<NR1>(g[v], ct);
-          op.store4(i * k + c0, g[v]);
+          op.template computev<NR1>(g[v], ct);
+          op.storev(i * k + c0, g[v]);
         }
         if constexpr (NR > 0) {
           if (von) {
 #pragma unroll
-            for (int r = 0; r < NR1; ++r) {
-              *reinterpret_cast<double2*>(&s_c[warp][r][gr][c0]) = make_double2(ct[r][0], ct[r][1]);
-              *reinterpret_cast<double2*>(&s_c[warp][r][gr][c0 + 2]) = make_double2(ct[r][2], ct[r][3]);
-            }
+            for (int r = 0; r < NR1; ++r)
+#pragma unroll
+              for (int j = 0; j < W; j += 2)
+                *reinterpret_cast<double2*>(&s_c[warp][r][gr][c0 + j]) = make_double2(ct[r][j], ct[r][j + 1]);
           }
           __syncwarp();
           if (lane < k) {
 #pragma unroll
-            for (int gg = 0; gg < 4; ++gg)
+            for (int gg = 0; gg < W; ++gg)
               if (row0 + r4 + gg < n) {
 #pragma unroll
                 for (int r = 0; r < NR1; ++r) acc[r] = dadd(acc[r], s_c[warp][r][gg][lane]);
@@ -982,10 +984,11 @@ struct MOpDirection {
 // The FP32 update and direction sweeps of the refinement's inner solves
 // with 4-column methods for mtile4_kernel (same arithmetic per element).
 struct MOpUpdate32 : MOpUpdate<float> {
-  struct Regs4 { float4 r, v; float J; };
+  static constexpr int kVecW = 4;
+  struct RegsV { float4 r, v; float J; };
   double sg4[4];
   bool act4[4];
-  __device__ void begin_col4(int c0) {
+  __device__ void begin_colv(int c0) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int c = c0 + j < a.k ? c0 + j : 0;
@@ -993,13 +996,13 @@ struct MOpUpdate32 : MOpUpdate<float> {
       act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
     }
   }
-  __device__ void load4(long e, long i, Regs4& g) const {
+  __device__ void loadv(long e, long i, RegsV& g) const {
     g.r = *reinterpret_cast<const float4*>(R + e);
     g.v = __ldcs(reinterpret_cast<const float4*>(V + e));
     g.J = __ldg(J + i);
   }
   template <int NR1>
-  __device__ void compute4(Regs4& g, double (&ct)[NR1][4]) const {
+  __device__ void computev(RegsV& g, double (&ct)[NR1][kVecW]) const {
 #pragma unroll
     for (int j = 0; j < 4; ++j)
       if (act4[j]) {
@@ -1010,15 +1013,16 @@ struct MOpUpdate32 : MOpUpdate<float> {
         ct[1][j] = dmul(D(ri), D(ri));
       }
   }
-  __device__ void store4(long e, const Regs4& g) const { *reinterpret_cast<float4*>(R + e) = g.r; }
+  __device__ void storev(long e, const RegsV& g) const { *reinterpret_cast<float4*>(R + e) = g.r; }
 };
 
 struct MOpDirection32 : MOpDirection<float> {
-  struct Regs4 { float4 p, r, x; float J; };
+  static constexpr int kVecW = 4;
+  struct RegsV { float4 p, r, x; float J; };
   double bt4[4], sg4[4];
   bool xp4[4], act4[4];
   bool anyx = false, anya = false;
-  __device__ void begin_col4(int c0) {
+  __device__ void begin_colv(int c0) {
     const unsigned xm = *(volatile unsigned*)a.xmask;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -1031,7 +1035,7 @@ struct MOpDirection32 : MOpDirection<float> {
     anyx = xp4[0] || xp4[1] || xp4[2] || xp4[3];
     anya = act4[0] || act4[1] || act4[2] || act4[3];
   }
-  __device__ void load4(long e, long i, Regs4& g) const {
+  __device__ void loadv(long e, long i, RegsV& g) const {
     g.p = *reinterpret_cast<const float4*>(P + e);
     if (anya) {
       g.r = __ldcs(reinterpret_cast<const float4*>(R + e));
@@ -1040,7 +1044,7 @@ struct MOpDirection32 : MOpDirection<float> {
     if (anyx) g.x = __ldcs(reinterpret_cast<const float4*>(X + e));
   }
   template <int NR1>
-  __device__ void compute4(Regs4& g, double (&)[NR1][4]) const {
+  __device__ void computev(RegsV& g, double (&)[NR1][kVecW]) const {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const float pj = f4c(g.p, j);
@@ -1049,10 +1053,53 @@ struct MOpDirection32 : MOpDirection<float> {
         f4s(g.p, j, celg::R<float>(dadd(dmul(bt4[j], D(pj)), dmul(D(f4c(g.r, j)), D(g.J)))));
     }
   }
-  __device__ void store4(long e, const Regs4& g) const {
+  __device__ void storev(long e, const RegsV& g) const {
     if (anyx) __stcs(reinterpret_cast<float4*>(X + e), g.x);
     if (anya) *reinterpret_cast<float4*>(P + e) = g.p;
   }
+};
+
+// The FP64 update sweep with 2-column methods for mtile4_kernel (16-byte
+// accesses; same arithmetic per element): 302 -> 283 us at 128^3 x 32.  The
+// direction sweep keeps one column per lane: at 2 columns per lane it needed
+// 128 registers and took 437 us against 421.
+__device__ __forceinline__ double d2c(const double2& v, int j) { return j == 0 ? v.x : v.y; }
+__device__ __forceinline__ void d2s(double2& v, int j, double x) {
+  if (j == 0) v.x = x;
+  else v.y = x;
+}
+
+struct MOpUpdate64 : MOpUpdate<double> {
+  static constexpr int kVecW = 2;
+  struct RegsV { double2 r, v; double J; };
+  double sg2[2];
+  bool act2[2];
+  __device__ void begin_colv(int c0) {
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int c = c0 + j < a.k ? c0 + j : 0;
+      sg2[j] = a.sigma[c];
+      act2[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
+    }
+  }
+  __device__ void loadv(long e, long i, RegsV& g) const {
+    g.r = *reinterpret_cast<const double2*>(R + e);
+    g.v = __ldcs(reinterpret_cast<const double2*>(V + e));
+    g.J = __ldg(J + i);
+  }
+  template <int NR1>
+  __device__ void computev(RegsV& g, double (&ct)[NR1][kVecW]) const {
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      if (act2[j]) {
+        const double ri = dadd(d2c(g.r, j), dmul(-sg2[j], d2c(g.v, j)));
+        d2s(g.r, j, ri);
+        const double z = dmul(ri, g.J);
+        ct[0][j] = dmul(ri, z);
+        ct[1][j] = dmul(ri, ri);
+      }
+  }
+  __device__ void storev(long e, const RegsV& g) const { *reinterpret_cast<double2*>(R + e) = g.r; }
 };
 
 // ||b - A x|| / ||b|| per column
@@ -1201,11 +1248,12 @@ struct MOpRuStep {
     acc[0] = dadd(acc[0], dmul((double)ri, z));
     acc[1] = dadd(acc[1], dmul((double)ri, (double)ri));
   }
-  // 4 columns c0..c0+3 per lane (mtile4_kernel)
-  struct Regs4 { float4 r, v; float J; };
+  // 4 columns c0..c0+3 per lane (mtile4_kernel, W = 4)
+  static constexpr int kVecW = 4;
+  struct RegsV { float4 r, v; float J; };
   float nsg4[4];
   bool act4[4];
-  __device__ void begin_col4(int c0) {
+  __device__ void begin_colv(int c0) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int c = c0 + j < a.k ? c0 + j : 0;
@@ -1213,13 +1261,13 @@ struct MOpRuStep {
       act4[j] = c0 + j < a.k && *(volatile int*)&a.active[c] != 0;
     }
   }
-  __device__ void load4(long e, long i, Regs4& g) const {
+  __device__ void loadv(long e, long i, RegsV& g) const {
     g.r = *reinterpret_cast<const float4*>(R32 + e);
     g.v = __ldcs(reinterpret_cast<const float4*>(V32 + e));
     g.J = __ldg(J32 + i);
   }
   template <int NR1>
-  __device__ void compute4(Regs4& g, double (&ct)[NR1][4]) const {
+  __device__ void computev(RegsV& g, double (&ct)[NR1][kVecW]) const {
 #pragma unroll
     for (int j = 0; j < 4; ++j)
       if (act4[j]) {
@@ -1230,7 +1278,7 @@ struct MOpRuStep {
         ct[1][j] = dmul((double)ri, (double)ri);
       }
   }
-  __device__ void store4(long e, const Regs4& g) const {
+  __device__ void storev(long e, const RegsV& g) const {
     *reinterpret_cast<float4*>(R32 + e) = g.r;
   }
   __device__ void finish_col(int c, double* tot) const {
@@ -1332,12 +1380,13 @@ struct MOpRuDirection {
     if (dp) __stcs(D32 + e, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
     if (act) P32[e] = celg::R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
-  // 4 columns c0..c0+3 per lane (mtile4_kernel)
-  struct Regs4 { float4 p, r, d; float J; };
+  // 4 columns c0..c0+3 per lane (mtile4_kernel, W = 4)
+  static constexpr int kVecW = 4;
+  struct RegsV { float4 p, r, d; float J; };
   double bt4[4], sg4[4];
   bool dp4[4], act4[4];
   bool anyd = false, anya = false;
-  __device__ void begin_col4(int c0) {
+  __device__ void begin_colv(int c0) {
     const unsigned xm = *(volatile unsigned*)a.xmask;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -1350,7 +1399,7 @@ struct MOpRuDirection {
     anyd = dp4[0] || dp4[1] || dp4[2] || dp4[3];
     anya = act4[0] || act4[1] || act4[2] || act4[3];
   }
-  __device__ void load4(long e, long i, Regs4& g) const {
+  __device__ void loadv(long e, long i, RegsV& g) const {
     g.p = *reinterpret_cast<const float4*>(P32 + e);
     if (anya) {
       g.r = __ldcs(reinterpret_cast<const float4*>(R32 + e));
@@ -1359,7 +1408,7 @@ struct MOpRuDirection {
     if (anyd) g.d = __ldcs(reinterpret_cast<const float4*>(D32 + e));
   }
   template <int NR1>
-  __device__ void compute4(Regs4& g, double (&)[NR1][4]) const {
+  __device__ void computev(RegsV& g, double (&)[NR1][kVecW]) const {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const float pj = f4c(g.p, j);
@@ -1368,7 +1417,7 @@ struct MOpRuDirection {
         f4s(g.p, j, celg::R<float>(dadd(dmul(bt4[j], D(pj)), dmul(D(f4c(g.r, j)), D(g.J)))));
     }
   }
-  __device__ void store4(long e, const Regs4& g) const {
+  __device__ void storev(long e, const RegsV& g) const {
     if (anyd) __stcs(reinterpret_cast<float4*>(D32 + e), g.d);
     if (anya) *reinterpret_cast<float4*>(P32 + e) = g.p;
   }
@@ -1627,8 +1676,8 @@ static int launch_mtile(celg_handle* h, long n, int k, const Op& op, bool vec4 =
   const long nt = ntiles_of(n);
   RedCtx red{h->partials, h->ticket, nt};
   red.sweep = next_sweep(h, false);
-  if constexpr (has_vec4<Op>::value) {
-    if (vec4 && (k & 3) == 0) {
+  if constexpr (has_vecw<Op>::value) {
+    if (vec4 && k % Op::kVecW == 0) {
       const int grid =
           grid_for_tiles(h, nt, std::min(8, resident_per_sm<mtile4_kernel<Op>>(kLanes, 0)));
       mtile4_kernel<Op><<<grid, kLanes, 0, h->stream>>>(n, k, op, red);
@@ -1866,9 +1915,12 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     if (!s2) s2 = launch_spmm(h, m->csr, k, X, MEpiInit<double>{B, R, P, m->jacobi, k, ac}, cfg);
     return s2;
   };
+  // the 16-byte update sweep: R and V start at multiples of n k doubles from
+  // a cudaMalloc base
+  const bool vw_r = (k & 1) == 0;
   auto body = [&](const MultiArgs& ac) -> int {
     int s3 = launch_spmm(h, m->csr, k, P, MEpiAp<double>{V, P, k, ac}, cfg);
-    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate<double>{R, V, m->jacobi, ac, 0.0});
+    if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate64{{R, V, m->jacobi, ac, 0.0}}, vw_r);
     if (!s3) s3 = launch_mtile(h, n, k, MOpDirection<double>{P, R, m->jacobi, X, ac});
     return s3;
   };
