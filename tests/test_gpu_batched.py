@@ -174,3 +174,29 @@ def test_batched_launch_shapes_give_the_same_bits(gpu, monkeypatch):
         for m in mats:
             m.destroy()
         hq.close()
+
+
+def test_batched_fp32_reliable_updates_unstructured(gpu):
+    """Unstructured systems (the batch reads int32 columns): each system
+    still equals its single reliable-update solve bit for bit."""
+    celgpu, h, torch = gpu
+    from tests.helpers import random_csr, spd_from_pattern
+    rng = np.random.default_rng(22)
+    sy = []
+    for n in (1500, 700, 2300):
+        rp, ci, v = spd_from_pattern(*random_csr(n, rng, max_len=9, empty_frac=0.0))
+        sy.append((rp, ci, v, rng.uniform(-1.0, 1.0, n)))
+    mats = [h.matrix_from_csr(rp, ci, v).jacobi() for rp, ci, v, _ in sy]
+    bs = [dev(torch, b) for *_, b in sy]
+    xs = [dev(torch, np.zeros(b.size)) for *_, b in sy]
+    kw = dict(eps_rel=1e-10, iter_max=3000, precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2,
+              x0_mode=celgpu.X0_ZERO)
+    infos = h.pcg_batched(mats, [b.data_ptr() for b in bs], [x.data_ptr() for x in xs], **kw)
+    for s, m in enumerate(mats):
+        xo = dev(torch, np.zeros(bs[s].numel()))
+        one = h.pcg_jacobi(m, bs[s].data_ptr(), xo.data_ptr(), **kw)
+        assert infos[s].status == one.status == celgpu.OK, s
+        assert infos[s].iter_done == one.iter_done and infos[s].arnoldi_steps == one.arnoldi_steps, s
+        assert np.array_equal(xs[s].cpu().numpy(), xo.cpu().numpy()), s
+    for m in mats:
+        m.destroy()

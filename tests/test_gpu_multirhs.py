@@ -380,3 +380,27 @@ def test_every_fp32_spmm_shape_is_bitexact(gpu, cfg32, monkeypatch):
     assert np.array_equal(Xd.cpu().numpy(), Xo)
     assert [i.iter_done for i in infos] == its
     m.destroy()
+
+
+def test_multirhs_fp32_reliable_update_unstructured(gpu):
+    """An unstructured matrix with some long rows (no row patterns, no 1-byte
+    offsets: the SpMMs read the int32 columns, long rows past the staging
+    chunks): every column still equals the mirror bit for bit."""
+    celgpu, h, torch = gpu
+    from tests.helpers import random_csr, spd_from_pattern
+    rng = np.random.default_rng(21)
+    rp, ci, v = spd_from_pattern(*random_csr(3000, rng, max_len=9, empty_frac=0.0, long_rows=3,
+                                             long_len=400))
+    n, k = rp.size - 1, 8
+    B = rng.uniform(-1.0, 1.0, (n, k))
+    m = h.matrix_from_csr(rp, ci, v).jacobi()
+    Bd, Xd = dev(torch, B), dev(torch, np.zeros((n, k)))
+    infos = h.pcg_multirhs(m, k, Bd.data_ptr(), Xd.data_ptr(), eps_rel=1e-10, iter_max=3000,
+                           precision=celgpu.PREC_FP32_RU, inner_eps_rel=1e-2)
+    assert m.column_form() == celgpu.COLS_INT32
+    Xo, its, ups, norms = mirror_ru(rp, ci, v, B, 1e-10, 1e-2, 3000)
+    assert np.array_equal(Xd.cpu().numpy(), Xo)
+    assert [i.iter_done for i in infos] == its
+    assert [i.arnoldi_steps for i in infos] == ups
+    assert all(i.status == celgpu.OK and i.verified_relres <= 1e-10 for i in infos)
+    m.destroy()
