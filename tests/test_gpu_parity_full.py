@@ -34,8 +34,8 @@ def dev(torch, a):
 
 
 def close_to_reference_order(info, x, io, xo, tol=1e-10):
-    """north-star parity of a PCG solve against the reference's order:
-    iteration count +-1, history and solution within tol relative."""
+    """Parity of a PCG solve with the reference's reduction order: iteration
+    count within one, history and solution within tol relative."""
     assert abs(io["iter_done"] - info.iter_done) <= 1
     k = min(len(io["history"]), len(info.history))
     hist = np.abs(info.history[:k] - io["history"][:k]) / io["history"][:k]
