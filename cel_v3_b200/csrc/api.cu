@@ -570,6 +570,7 @@ extern "C" int celg_destroy(celg_handle* h) {
   cudaFree(h->wr);
   cudaFree(h->wp);
   cudaFree(h->wv);
+  cudaFree(h->wq);
   cudaFree(h->wz);
   cudaFree(h->state_d);
   cudaFreeHost(h->state_h);

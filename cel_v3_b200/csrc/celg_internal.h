@@ -76,6 +76,7 @@ struct celg_handle {
   double* wr = nullptr;
   double* wp = nullptr;
   double* wv = nullptr;
+  double* wq = nullptr;  // second PCG direction (paired K3)
   size_t wcap = 0;           // elements
   double* wz = nullptr;      // z = M r of block-Jacobi solves (wzcap elements)
   size_t wzcap = 0;

@@ -71,7 +71,7 @@ int ensure_f32(celg_handle* h, size_t n) {
   h->f32 = nullptr;
   h->ir_d = nullptr;
   const size_t cap = std::max<size_t>(n, 1024);
-  CELG_CUDA(cudaMalloc(&h->f32, sizeof(float) * cap * 5));  // 5 float vectors
+  CELG_CUDA(cudaMalloc(&h->f32, sizeof(float) * cap * 6));  // 6 float vectors
   CELG_CUDA(cudaMalloc(&h->ir_d, sizeof(double) * cap));
   h->f32cap = cap;
   h->ircap = cap;
@@ -96,6 +96,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   float* r32 = d32 + cap;
   float* p32 = r32 + cap;
   float* v32 = p32 + cap;
+  float* q32 = v32 + cap;  // second direction of the paired K3
   double* r = h->ir_d;
   double* sd = h->scal_d;
 
@@ -114,6 +115,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   B.x = d32;
   B.r = r32;
   B.p = p32;
+  B.q = q32;
   B.v = v32;
   B.J = m->jacobi32;
 
@@ -173,7 +175,7 @@ int ir_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   cudaEventDestroy(e1);
   if (st) return st;
   h->last_iters = inner_total;
-  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 52.0 * n;
+  h->last_bytes_per_iter = 8.0 * m->csr.nnz + 4.0 * (n + 1) + 50.0 * n;
   if (res) {
     res->iter_done = outer;
     res->final_norm2 = rn;

@@ -43,11 +43,13 @@ int ensure_work(celg_handle* h, size_t n) {
   cudaFree(h->wr);
   cudaFree(h->wp);
   cudaFree(h->wv);
-  h->wr = h->wp = h->wv = nullptr;
+  cudaFree(h->wq);
+  h->wr = h->wp = h->wv = h->wq = nullptr;
   const size_t cap = std::max<size_t>(n, 1024);
   CELG_CUDA(cudaMalloc(&h->wr, cap * sizeof(double)));
   CELG_CUDA(cudaMalloc(&h->wp, cap * sizeof(double)));
   CELG_CUDA(cudaMalloc(&h->wv, cap * sizeof(double)));
+  CELG_CUDA(cudaMalloc(&h->wq, cap * sizeof(double)));
   h->wcap = cap;
   return CELG_OK;
 }
@@ -122,17 +124,21 @@ static int pcg_setup(celg_handle* h, const PcgBind<VT>& B, const celg_params* p,
   return csr_sweep<VT>(h, B, B.vals, B.x, EpiInit<VT>{B.b, B.r, B.p, B.J, a});
 }
 
+// phase 0: one iteration, K3 = OpDirectionX.  Phases 1 and 2: the even and
+// the odd iteration of a pair (B.q set: CSR sweeps, point Jacobi), whose
+// directions are B.p and B.q in turn.
 template <typename VT>
-static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
+static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a, int phase = 0) {
   const long n = B.A->n;
+  VT* pc = phase == 2 ? B.q : B.p;
   int s2 = CELG_OK;
   if constexpr (std::is_same<VT, double>::value) {
     if (B.jad)
       s2 = launch_jad(h, *B.A, *B.jad, B.p, EpiAp<double>{B.v, B.p, a});
     else
-      s2 = csr_sweep<VT>(h, B, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+      s2 = csr_sweep<VT>(h, B, B.vals, pc, EpiAp<VT>{B.v, pc, a});
   } else {
-    s2 = csr_sweep<VT>(h, B, B.vals, B.p, EpiAp<VT>{B.v, B.p, a});
+    s2 = csr_sweep<VT>(h, B, B.vals, pc, EpiAp<VT>{B.v, pc, a});
   }
   if constexpr (std::is_same<VT, double>::value) {
     if (B.bj) {
@@ -142,8 +148,18 @@ static int pcg_body(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
     }
   }
   if (!s2) s2 = launch_tile(h, n, OpUpdate<VT>{B.r, B.v, B.J, a, 0.0});
-  if (!s2) s2 = launch_tile(h, n, OpDirectionX<VT>{B.p, B.r, B.J, B.x, a});
-  return s2;
+  if (s2) return s2;
+  if (phase == 1) return launch_tile(h, n, OpDirectionDefer<VT>{B.p, B.q, B.r, B.J, B.x, a});
+  if (phase == 2) return launch_tile(h, n, OpDirectionPair<VT>{B.p, B.q, B.r, B.J, B.x, a});
+  return launch_tile(h, n, OpDirectionX<VT>{B.p, B.r, B.J, B.x, a});
+}
+
+// Two iterations: a pair when B.q is set, else the one-iteration body twice.
+template <typename VT>
+static int pcg_body2(celg_handle* h, const PcgBind<VT>& B, PcgArgs a) {
+  int st = pcg_body(h, B, a, B.q ? 1 : 0);
+  if (!st) st = pcg_body(h, B, a, B.q ? 2 : 0);
+  return st;
 }
 
 template <typename VT>
@@ -166,7 +182,7 @@ template <typename VT>
 static int record_pcg(celg_handle* h, const PcgBind<VT>& B, const celg_params* p, PcgArgs a) {
   int st = pcg_setup(h, B, p, a);
   if (st) return st;
-  st = capture_while2(h, a.cond, [&]() -> int { return pcg_body(h, B, a); });
+  st = capture_while(h, a.cond, [&]() -> int { return pcg_body2(h, B, a); });
   if (st) return st;
   return pcg_tail(h, B, a);
 }
@@ -181,7 +197,7 @@ static int run_host_loop(celg_handle* h, const PcgBind<VT>& B, const celg_params
   a.cond = 0;
   int st = pcg_setup(h, B, p, a);
   for (int it = 0; !st && it < p->iter_max; it += 8) {
-    for (int k = 0; k < 8 && !st; ++k) st = pcg_body(h, B, a);
+    for (int k = 0; k < 4 && !st; ++k) st = pcg_body2(h, B, a);
     if (st) break;
     CELG_CUDA(cudaMemcpyAsync(h->state_h, h->state_d, sizeof(PcgState), cudaMemcpyDeviceToHost,
                               h->stream));
@@ -196,9 +212,9 @@ template <typename VT>
 static std::string pcg_key(const PcgBind<VT>& B, const celg_params* p, int hist_cap,
                            const void* mat) {
   char buf[640];
-  std::snprintf(buf, sizeof(buf), "pcg%d|%p|%d|%d|%p|%p|%p|%p|%p|%p|%d|%.17g|%.17g|%d|%d|%p|%p|%p|%d|%p|%d",
+  std::snprintf(buf, sizeof(buf), "pcg%d|%p|%d|%d|%p|%p|%p|%p|%p|%p|%p|%d|%.17g|%.17g|%d|%d|%p|%p|%p|%d|%p|%d",
                 (int)sizeof(VT), mat, B.A->n, B.jad ? 1 : 0, (const void*)B.b, (const void*)B.x,
-                (const void*)B.r, (const void*)B.p, (const void*)B.v, (const void*)B.J,
+                (const void*)B.r, (const void*)B.p, (const void*)B.q, (const void*)B.v, (const void*)B.J,
                 p->x0_mode, p->eps_abs, p->eps_rel, p->iter_max, hist_cap,
                 (const void*)B.vals, (const void*)B.verify_vals, (const void*)B.bj, B.bs,
                 (const void*)B.z, B.dict ? 1 : 0);
@@ -305,16 +321,19 @@ int pcg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const cel
     B.z = h->wz;
   } else if (p->precond != CELG_PRECOND_JACOBI) {
     return CELG_ERR_ARG;
+  } else if (!jad) {
+    B.q = h->wq;
   }
   PcgState s;
   std::memset(&s, 0, sizeof(s));
   const int ret = pcg_run<double>(h, B, p, m, &s);
   h->last_iters = s.iter;
   // K1 reads 8 bytes per non-zero and one per row with the row patterns, 9 per
-  // non-zero with the 1-byte offsets, else 12
+  // non-zero with the 1-byte offsets, else 12; the paired K3 reads and stores
+  // x once per two iterations (92 instead of 96 bytes per row)
   h->last_bytes_per_iter =
       (B.dict && m->csr.pid ? 8.0 * m->csr.nnz + 1.0 * n : (B.dict ? 9.0 : 12.0) * m->csr.nnz) +
-      4.0 * (n + 1) + 96.0 * n;
+      4.0 * (n + 1) + (B.q ? 92.0 : 96.0) * n;
   if (res) {
     res->iter_done = s.iter;
     res->final_norm2 = s.norm;

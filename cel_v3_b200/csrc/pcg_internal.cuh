@@ -14,6 +14,8 @@ struct PcgState {
   double alpha, sigma, beta, norm, bnorm, eps, pvd, rz, vres;
   int iter, active, err, hist_len;
   int xpend;  // K2 ran: K3 owes x += sigma p
+  int xprev;  // paired form: the odd K3 owes x += sigprev p_prev first
+  double sigprev;
 };
 
 struct PcgArgs {
@@ -36,6 +38,7 @@ struct PcgBind {
   VT* x = nullptr;
   VT* r = nullptr;
   VT* p = nullptr;
+  VT* q = nullptr;  // second direction buffer: the paired K3 (CSR, Jacobi only)
   VT* v = nullptr;
   const VT* J = nullptr;
   // block Jacobi (FP64 CSR only): inverse rows, block size, z = M r
@@ -114,6 +117,8 @@ struct OpPre {
     st->alpha = st->sigma = st->beta = st->pvd = st->rz = 0.0;
     st->vres = 0.0;
     st->xpend = 0;
+    st->xprev = 0;
+    st->sigprev = 0.0;
   }
 };
 
@@ -278,6 +283,109 @@ struct OpDirectionX {
     if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
   }
   __device__ void finish(double*) const { a.st->xpend = 0; }
+};
+
+// The paired form of K3 for two iterations, k (even sweep) and k+1 (odd
+// sweep), whose directions live in two buffers: p_k in p, p_k+1 in q.  The
+// even sweep writes p_k+1 = beta p_k + J r into q and leaves x += sigma_k p_k
+// pending (xprev, sigprev); the odd sweep applies both updates to x in
+// order, x = (x + sigma_k p_k) + sigma_k+1 p_k+1, and writes p_k+2 over p_k.
+// x is read and stored once per two iterations instead of every iteration,
+// and each element gets the same operations in the same order as with
+// OpDirectionX.  When K2 ended the solve in the even iteration, the even
+// sweep applies its own update at once.
+template <typename VT>
+struct OpDirectionDefer {
+  static constexpr int NRED = 0;
+  static constexpr int kTilesPerPass = sizeof(VT) == 4 ? 2 : 1;
+  static constexpr bool kFinishAlways = true;
+  struct Regs { VT p, r, J, x; };
+  const VT* p;
+  VT* q;
+  const VT* r;
+  const VT* J;
+  VT* x;
+  PcgArgs a;
+  double bt = 0.0, sg = 0.0;
+  int xp = 0, act = 0;
+  __device__ bool prepare() {
+    xp = *(volatile int*)&a.st->xpend;
+    act = *(volatile int*)&a.st->active;
+    if (!xp && !act) return false;
+    bt = a.st->beta;
+    sg = a.st->sigma;
+    return true;
+  }
+  // p_k is read again by the odd sweep, after the SpMV and K2 of the next
+  // iteration: streamed, so that L2 keeps the new direction for that SpMV
+  __device__ void load(long i, Regs& g) const {
+    g.p = __ldcs(p + i);
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldcs(J + i);
+    } else if (xp) {
+      g.x = __ldcs(x + i);
+    }
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (act) q[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+    else if (xp) __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+  }
+  __device__ void finish(double*) const {
+    if (xp && act) {
+      a.st->sigprev = sg;
+      a.st->xprev = 1;
+    }
+    a.st->xpend = 0;
+  }
+};
+
+template <typename VT>
+struct OpDirectionPair {
+  static constexpr int NRED = 0;
+  static constexpr int kTilesPerPass = sizeof(VT) == 4 ? 2 : 1;
+  static constexpr bool kFinishAlways = true;
+  struct Regs { VT p, q, r, J, x; };
+  VT* p;
+  const VT* q;
+  const VT* r;
+  const VT* J;
+  VT* x;
+  PcgArgs a;
+  double bt = 0.0, sg = 0.0, sp = 0.0;
+  int xq = 0, xp = 0, act = 0;
+  __device__ bool prepare() {
+    xq = *(volatile int*)&a.st->xprev;
+    xp = *(volatile int*)&a.st->xpend;
+    act = *(volatile int*)&a.st->active;
+    if (!xq && !xp && !act) return false;
+    bt = a.st->beta;
+    sg = a.st->sigma;
+    sp = a.st->sigprev;
+    return true;
+  }
+  __device__ void load(long i, Regs& g) const {
+    if (xq) g.p = __ldcs(p + i);
+    if (xp || act) g.q = q[i];
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldcs(J + i);
+    }
+    if (xq || xp) g.x = __ldcs(x + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (xq || xp) {
+      VT xv = g.x;
+      if (xq) xv = R<VT>(dadd(D(xv), dmul(sp, D(g.p))));
+      if (xp) xv = R<VT>(dadd(D(xv), dmul(sg, D(g.q))));
+      __stcs(x + i, xv);
+    }
+    if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.q)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish(double*) const {
+    a.st->xprev = 0;
+    a.st->xpend = 0;
+  }
 };
 
 // verification: ||b - A x|| / ||b|| (residual not stored)

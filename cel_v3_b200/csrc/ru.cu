@@ -90,6 +90,8 @@ struct OpRuPre {
     r->update = 1;  // the set-up residual is a reliable update
     r->updates = 0;
     r->s.xpend = 0;
+    r->s.xprev = 0;
+    r->s.sigprev = 0.0;
   }
 };
 
@@ -198,75 +200,47 @@ struct OpRuStep {
 };
 
 // x64 += (double) d ; d = 0   (pending update, or unconditionally at the end).
-// A d += sigma p still pending from the step is applied first, with the
-// step's rounding, and the last CTA clears the mark.
+// The d += sigma p updates still pending are applied first, in order and
+// with the step's rounding: the even iteration's (s.xprev, direction pp)
+// when the flush follows the odd step of a pair, then the step's own
+// (s.xpend, direction p).  The last CTA clears both marks.
 struct OpRuFlush {
   static constexpr int NRED = 0;
   static constexpr bool kFinishAlways = true;
-  struct Regs { double x; float d, p; };
+  struct Regs { double x; float d, p, pp; };
   double* x;
   float* d;
   const float* p;
+  const float* pp;
   RuArgs a;
   int always;
-  int dp = 0;
-  double sg = 0.0;
+  int dp = 0, dq = 0;
+  double sg = 0.0, sp = 0.0;
   __device__ bool prepare() {
     if (!(always || *(volatile int*)&a.st->update != 0)) return false;
     dp = p != nullptr && *(volatile int*)&a.st->s.xpend;
+    dq = pp != nullptr && *(volatile int*)&a.st->s.xprev;
     sg = a.st->s.sigma;
+    sp = a.st->s.sigprev;
     return true;
   }
   __device__ void load(long i, Regs& g) const {
     g.x = x[i];
     g.d = d[i];
     if (dp) g.p = __ldg(p + i);
+    if (dq) g.pp = __ldg(pp + i);
   }
   __device__ void compute(long i, Regs& g, double*) const {
-    const float di = dp ? (float)dadd((double)g.d, dmul(sg, (double)g.p)) : g.d;
+    float di = g.d;
+    if (dq) di = (float)dadd((double)di, dmul(sp, (double)g.pp));
+    if (dp) di = (float)dadd((double)di, dmul(sg, (double)g.p));
     x[i] = dadd(g.x, (double)di);
     d[i] = 0.0f;
   }
-  __device__ void finish(double*) const { a.st->s.xpend = 0; }
-};
-
-// K3: d += sigma p when the step left it pending (no reliable update in
-// between; also after the step stopped the solve), then p = beta p + J r
-// while the solve goes on.  The last CTA clears the mark.
-struct OpRuDirection {
-  static constexpr int NRED = 0;
-  static constexpr int kTilesPerPass = 2;
-  static constexpr bool kFinishAlways = true;
-  struct Regs { float p, r, J, d; };
-  float* p;
-  const float* r;
-  const float* J;
-  float* d;
-  RuArgs a;
-  int dp = 0, act = 0;
-  double bt = 0.0, sg = 0.0;
-  __device__ bool prepare() {
-    dp = *(volatile int*)&a.st->s.xpend;
-    act = *(volatile int*)&a.st->s.active;
-    if (!dp && !act) return false;
-    bt = a.st->s.beta;
-    sg = a.st->s.sigma;
-    return true;
+  __device__ void finish(double*) const {
+    a.st->s.xpend = 0;
+    a.st->s.xprev = 0;
   }
-  // r, J and d are streamed (evict-first), so that L2 keeps the new p
-  __device__ void load(long i, Regs& g) const {
-    g.p = p[i];
-    if (act) {
-      g.r = __ldcs(r + i);
-      g.J = __ldcs(J + i);
-    }
-    if (dp) g.d = __ldcs(d + i);
-  }
-  __device__ void compute(long i, Regs& g, double*) const {
-    if (dp) __stcs(d + i, (float)dadd((double)g.d, dmul(sg, (double)g.p)));
-    if (act) p[i] = R<float>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
-  }
-  __device__ void finish(double*) const { a.st->s.xpend = 0; }
 };
 
 // final check ||b - A x|| / ||b|| in FP64
@@ -307,31 +281,38 @@ static int ru_setup(celg_handle* h, celg_mat* m, const double* b, double* x, con
 
 // One iteration: K1, K2, then (only when K2 asked for it) the reliable
 // update -- inside an IF conditional node when recorded into a graph, as
-// self-skipping kernels otherwise -- then K3.
+// self-skipping kernels otherwise -- then K3.  Iterations run in pairs
+// whose directions are pv and pq in turn (odd = false, then true); K3 is
+// the paired direction sweep of the PCG (OpDirectionDefer, OpDirectionPair)
+// with the correction d in place of x, so d is read and stored once per
+// pair.
 static int ru_body(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* r,
-                   float* pv, float* v, float* d, bool in_graph) {
+                   float* pv, float* pq, float* v, float* d, bool odd, bool in_graph) {
   const long n = m->csr.n;
   if (in_graph) {
     int st = capture_new_handle(h, 0, &a.cond_update);
     if (st) return st;
   }
   PcgArgs pa = a.pcg();
-  int st = launch_csr<float>(h, m->csr, m->csr.v32, pv, EpiAp<float>{v, pv, pa});
+  float* pc = odd ? pq : pv;
+  int st = launch_csr<float>(h, m->csr, m->csr.v32, pc, EpiAp<float>{v, pc, pa});
   if (!st) st = launch_tile(h, n, OpRuStep{r, v, m->jacobi32, a, 0.0f});
   auto update = [&]() -> int {
-    int s2 = launch_tile(h, n, OpRuFlush{x, d, pv, a, 0});
+    int s2 = launch_tile(h, n, OpRuFlush{x, d, pc, odd ? pv : nullptr, a, 0});
     if (!s2)
       s2 = launch_csr<double>(h, m->csr, m->csr.v, x,
                               EpiRuResidual{b, r, nullptr, m->jacobi32, a, 0});
     return s2;
   };
   if (!st) st = in_graph ? capture_if(h, a.cond_update, update) : update();
-  if (!st) st = launch_tile(h, n, OpRuDirection{pv, r, m->jacobi32, d, a});
-  return st;
+  if (st) return st;
+  const float* J = m->jacobi32;
+  if (odd) return launch_tile(h, n, OpDirectionPair<float>{pv, pq, r, J, d, pa});
+  return launch_tile(h, n, OpDirectionDefer<float>{pv, pq, r, J, d, pa});
 }
 
 static int ru_tail(celg_handle* h, celg_mat* m, const double* b, double* x, RuArgs a, float* d) {
-  int st = launch_tile(h, m->csr.n, OpRuFlush{x, d, nullptr, a, 1});
+  int st = launch_tile(h, m->csr.n, OpRuFlush{x, d, nullptr, nullptr, a, 1});
   if (!st) st = launch_csr<double>(h, m->csr, m->csr.v, x, EpiRuVerify{b, a.st});
   return st;
 }
@@ -361,6 +342,7 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   float* pv = r + cap;
   float* v = pv + cap;
   float* d = v + cap;
+  float* pq = d + cap;
   CELG_CUDA(cudaMemsetAsync(h->err_d, 0, sizeof(int), h->stream));
 
   char kb[512];
@@ -373,7 +355,8 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
     CELG_CUDA(cudaEventRecord(h->ev0, h->stream));
     st = ru_setup(h, m, b, x, p, a0, r, pv, d);
     for (int it = 0; !st && it < p->iter_max; it += 8) {
-      for (int k = 0; k < 8 && !st; ++k) st = ru_body(h, m, b, x, a0, r, pv, v, d, false);
+      for (int k = 0; k < 8 && !st; ++k)
+        st = ru_body(h, m, b, x, a0, r, pv, pq, v, d, (k & 1) != 0, false);
       if (st) break;
       CELG_CUDA(cudaMemcpyAsync(sh, sd, sizeof(RuState), cudaMemcpyDeviceToHost, h->stream));
       CELG_CUDA(cudaStreamSynchronize(h->stream));
@@ -389,7 +372,11 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
         RuArgs a{sd, h->hist_d, hist_cap, p->iter_max, cond, h->err_d, 0};
         int s2 = ru_setup(h, m, b, x, p, a, r, pv, d);
         if (!s2)
-          s2 = capture_while2(h, cond, [&]() -> int { return ru_body(h, m, b, x, a, r, pv, v, d, true); });
+          s2 = capture_while(h, cond, [&]() -> int {
+            int s3 = ru_body(h, m, b, x, a, r, pv, pq, v, d, false, true);
+            if (!s3) s3 = ru_body(h, m, b, x, a, r, pv, pq, v, d, true, true);
+            return s3;
+          });
         if (!s2) s2 = ru_tail(h, m, b, x, a, d);
         return s2;
       }, &ge);
@@ -412,9 +399,10 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   else if (!(s.norm64 <= s.s.eps)) ret = CELG_ERR_NOCONV;
   h->last_iters = s.s.iter;
   // K1 (matrix, p gathered, v stored: 8 n), K2 (r, v, J read, r stored:
-  // 16 n), K3 (p, r, J, d read, p, d stored: 24 n); 5 bytes per non-zero
-  // with the 1-byte column offsets, else 8
-  h->last_bytes_per_iter = (m->csr.ci8 ? 5.0 : 8.0) * m->csr.nnz + 4.0 * (n + 1) + 48.0 * n;
+  // 16 n), K3 (p, r, J read, p stored, d read and stored once per pair of
+  // iterations: 20 n on average); 5 bytes per non-zero with the 1-byte
+  // column offsets, else 8
+  h->last_bytes_per_iter = (m->csr.ci8 ? 5.0 : 8.0) * m->csr.nnz + 4.0 * (n + 1) + 44.0 * n;
   if (res) {
     res->iter_done = s.s.iter;
     res->final_norm2 = s.norm64;
