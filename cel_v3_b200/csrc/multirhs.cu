@@ -38,6 +38,10 @@ struct MultiArgs {
   // columns whose update sweep ran and whose x += sigma p the direction
   // sweep still owes (bit c = column c)
   unsigned* xmask;
+  // paired direction sweeps (FP64): columns whose x += sigma p_k the odd
+  // sweep owes from the even one (bit c), with that sigma
+  unsigned* pmask;
+  double* sigprev;
   int k;
   int iter_max;
   cudaGraphConditionalHandle cond;
@@ -821,6 +825,7 @@ struct MOpPre {
   __device__ void finish_global() const {
     *a.n_active = part_count ? *part_count : a.k;
     *a.xmask = 0u;
+    *a.pmask = 0u;
   }
 };
 
@@ -979,6 +984,119 @@ struct MOpDirection {
   }
   __device__ void finish_col(int, double*) const {}
   __device__ void finish_global() const { *a.xmask = 0u; }
+};
+
+// The FP64 direction sweeps for a pair of iterations whose directions live
+// in two blocks, p_k in P and p_k+1 in Q.  The even sweep writes p_k+1 =
+// beta p_k + J r into Q and leaves x += sigma_k p_k pending for the columns
+// that go on (bit c of pmask, sigma_k in sigprev[c]); a column that K2 just
+// stopped gets its update at once.  The odd sweep applies x = (x + sigma_k
+// p_k) + sigma_k+1 p_k+1 and writes p_k+2 over P.  X is read and stored once
+// per two iterations, and every element gets the same roundings in the
+// same order as with MOpDirection.
+template <typename VT>
+struct MOpDirectionDefer {
+  static constexpr int NRED = 0;
+  struct Regs { VT p, r, J, x; };
+  const VT* P;
+  VT* Q;
+  const VT* R;
+  const VT* J;
+  VT* X;
+  MultiArgs a;
+  double bt = 0.0, sg = 0.0;
+  bool xp = false, act = false;
+  __device__ bool prepare() {
+    return *(volatile int*)a.n_active > 0 || *(volatile unsigned*)a.xmask != 0u;
+  }
+  __device__ bool col_active(int c) const {
+    return *(volatile int*)&a.active[c] != 0 || ((*(volatile unsigned*)a.xmask >> c) & 1u);
+  }
+  __device__ void begin_col(int c) {
+    bt = a.beta[c];
+    sg = a.sigma[c];
+    act = *(volatile int*)&a.active[c] != 0;
+    xp = ((*(volatile unsigned*)a.xmask >> c) & 1u) != 0;
+  }
+  // p_k is read again by the odd sweep, after the next SpMM: streamed
+  __device__ void load(long e, long i, Regs& g) const {
+    g.p = __ldcs(P + e);
+    if (act) {
+      g.r = __ldcs(R + e);
+      g.J = __ldg(J + i);
+    } else if (xp) {
+      g.x = __ldcs(X + e);
+    }
+  }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    if (act) Q[e] = celg::R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+    else if (xp) __stcs(X + e, celg::R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {
+    const unsigned xm = *(volatile unsigned*)a.xmask;
+    unsigned pm = 0u;
+    for (int c = 0; c < a.k; ++c)
+      if (((xm >> c) & 1u) && *(volatile int*)&a.active[c] != 0) {
+        a.sigprev[c] = a.sigma[c];
+        pm |= 1u << c;
+      }
+    *a.pmask = pm;
+    *a.xmask = 0u;
+  }
+};
+
+template <typename VT>
+struct MOpDirectionPair {
+  static constexpr int NRED = 0;
+  struct Regs { VT p, q, r, J, x; };
+  VT* P;
+  const VT* Q;
+  const VT* R;
+  const VT* J;
+  VT* X;
+  MultiArgs a;
+  double bt = 0.0, sg = 0.0, sp = 0.0;
+  bool xq = false, xp = false, act = false;
+  __device__ bool prepare() {
+    return *(volatile int*)a.n_active > 0 || *(volatile unsigned*)a.xmask != 0u ||
+           *(volatile unsigned*)a.pmask != 0u;
+  }
+  __device__ bool col_active(int c) const {
+    return *(volatile int*)&a.active[c] != 0 ||
+           (((*(volatile unsigned*)a.xmask | *(volatile unsigned*)a.pmask) >> c) & 1u);
+  }
+  __device__ void begin_col(int c) {
+    bt = a.beta[c];
+    sg = a.sigma[c];
+    sp = a.sigprev[c];
+    act = *(volatile int*)&a.active[c] != 0;
+    xp = ((*(volatile unsigned*)a.xmask >> c) & 1u) != 0;
+    xq = ((*(volatile unsigned*)a.pmask >> c) & 1u) != 0;
+  }
+  __device__ void load(long e, long i, Regs& g) const {
+    if (xq) g.p = __ldcs(P + e);
+    if (xp || act) g.q = __ldcs(Q + e);
+    if (act) {
+      g.r = __ldcs(R + e);
+      g.J = __ldg(J + i);
+    }
+    if (xq || xp) g.x = __ldcs(X + e);
+  }
+  __device__ void compute(long e, long, Regs& g, double*) const {
+    if (xq || xp) {
+      VT xv = g.x;
+      if (xq) xv = celg::R<VT>(dadd(D(xv), dmul(sp, D(g.p))));
+      if (xp) xv = celg::R<VT>(dadd(D(xv), dmul(sg, D(g.q))));
+      __stcs(X + e, xv);
+    }
+    if (act) P[e] = celg::R<VT>(dadd(dmul(bt, D(g.q)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish_col(int, double*) const {}
+  __device__ void finish_global() const {
+    *a.xmask = 0u;
+    *a.pmask = 0u;
+  }
 };
 
 // The FP32 update and direction sweeps of the refinement's inner solves
@@ -1699,6 +1817,8 @@ struct Multi {
   int tuned_n = -1, tuned_k = -1, cfg = 0;
   size_t cap = 0;        // n*k of the work vectors
   double* work = nullptr;  // R, P, V
+  size_t qcap = 0;
+  double* work_q = nullptr;  // Q: the second direction block of the FP64 pairs
   double* dstate = nullptr;
   int* istate = nullptr;
   // FP32 refinement (allocated on first use)
@@ -1731,6 +1851,7 @@ void multi_forget_matrix(Multi* m, const void* mat) {
 void multi_free(Multi* m) {
   if (!m) return;
   cudaFree(m->work);
+  cudaFree(m->work_q);
   cudaFree(m->dstate);
   cudaFree(m->istate);
   cudaFree(m->f32);
@@ -1843,6 +1964,8 @@ static MultiArgs multi_args(double* ds, int* is, int k, int iter_max, cudaGraphC
   a.err = a.active + kMaxRhs;
   a.n_active = a.err + kMaxRhs;
   a.xmask = reinterpret_cast<unsigned*>(a.n_active + 1);
+  a.pmask = a.xmask + 1;
+  a.sigprev = a.vres + kMaxRhs;
   a.k = k;
   a.iter_max = iter_max;
   a.errw = errw;
@@ -1876,14 +1999,23 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     mu->cap = nk;
   }
   if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
+  }
+  if (nk > mu->qcap || !mu->work_q) {
+    CELG_CUDA(cudaStreamSynchronize(h->stream));
+    graph_cache_clear(h);
+    cudaFree(mu->work_q);
+    mu->work_q = nullptr;
+    CELG_CUDA(cudaMalloc(&mu->work_q, sizeof(double) * std::max<size_t>(nk, 1)));
+    mu->qcap = nk;
   }
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
   double* R = mu->work;
   double* P = R + nk;
   double* V = P + nk;
+  double* Q = mu->work_q;
   MultiArgs a;
   a.alpha = mu->dstate;
   a.sigma = a.alpha + kMaxRhs;
@@ -1897,6 +2029,8 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   a.err = a.active + kMaxRhs;
   a.n_active = a.err + kMaxRhs;
   a.xmask = reinterpret_cast<unsigned*>(a.n_active + 1);
+  a.pmask = a.xmask + 1;
+  a.sigprev = a.vres + kMaxRhs;
   a.k = k;
   a.iter_max = p->iter_max;
   a.errw = h->err_d;
@@ -1918,11 +2052,14 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
   // the 16-byte update sweep: R and V start at multiples of n k doubles from
   // a cudaMalloc base
   const bool vw_r = (k & 1) == 0;
-  auto body = [&](const MultiArgs& ac) -> int {
-    int s3 = launch_spmm(h, m->csr, k, P, MEpiAp<double>{V, P, k, ac}, cfg);
+  // one iteration of a pair: directions in P, then in Q
+  auto body = [&](const MultiArgs& ac, bool odd) -> int {
+    double* Pc = odd ? Q : P;
+    int s3 = launch_spmm(h, m->csr, k, Pc, MEpiAp<double>{V, Pc, k, ac}, cfg);
     if (!s3) s3 = launch_mtile(h, n, k, MOpUpdate64{{R, V, m->jacobi, ac, 0.0}}, vw_r);
-    if (!s3) s3 = launch_mtile(h, n, k, MOpDirection<double>{P, R, m->jacobi, X, ac});
-    return s3;
+    if (s3) return s3;
+    if (odd) return launch_mtile(h, n, k, MOpDirectionPair<double>{P, Q, R, m->jacobi, X, ac});
+    return launch_mtile(h, n, k, MOpDirectionDefer<double>{P, Q, R, m->jacobi, X, ac});
   };
   auto tail = [&](const MultiArgs& ac) -> int {
     return launch_spmm(h, m->csr, k, X, MEpiVerify{B, k, ac}, cfg);
@@ -1933,7 +2070,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     a.cond = 0;
     st = setup(a);
     for (int it = 0; !st && it < p->iter_max; it += 8) {
-      for (int q = 0; q < 8 && !st; ++q) st = body(a);
+      for (int q = 0; q < 8 && !st; ++q) st = body(a, (q & 1) != 0);
       int act = 0;
       if (!st) {
         CELG_CUDA(cudaMemcpyAsync(&act, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1949,7 +2086,11 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
       MultiArgs ac = a;
       ac.cond = cond;
       int s2 = setup(ac);
-      if (!s2) s2 = capture_while2(h, cond, [&]() -> int { return body(ac); });
+      if (!s2) s2 = capture_while(h, cond, [&]() -> int {
+        int s3 = body(ac, false);
+        if (!s3) s3 = body(ac, true);
+        return s3;
+      });
       if (!s2) s2 = tail(ac);
       return s2;
     };
@@ -1996,7 +2137,7 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     }
   }
   h->last_iters = iters;
-  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 80.0 * (double)nk + 16.0 * n;
+  h->last_bytes_per_iter = 12.0 * m->csr.nnz + 4.0 * (n + 1) + 76.0 * (double)nk + 16.0 * n;
   return ret;
 }
 
@@ -2064,8 +2205,8 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
     mu->cap = nk;
   }
   if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
   }
   if (nk > mu->f32cap || !mu->f32) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
@@ -2078,8 +2219,8 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
   if (!mu->irs) {
     CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
     CELG_CUDA(cudaMalloc(&mu->irtau, sizeof(double) * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 2)));
+    CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 8 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 3)));
   }
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
@@ -2205,8 +2346,8 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
     mu->cap = nk;
   }
   if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 7 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 2)));
+    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
   }
   if (nk > mu->f32cap || !mu->f32) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
