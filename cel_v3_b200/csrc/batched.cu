@@ -29,6 +29,10 @@ struct BatchArgs {
   double *alpha, *sigma, *beta, *norm, *bnorm, *eps, *vres;
   int *iter, *active, *err, *n_active;
   int* xpend;  // per system: the update sweep ran, the direction sweep owes x += sigma p
+  // paired direction sweeps (FP64 solve only; null otherwise): the odd
+  // sweep owes x += sigprev p_k from the even one
+  int* xprev;
+  double* sigprev;
   BatchRed br;
   int nsys;
   int nlive;  // systems with rows (empty systems are never active)
@@ -78,6 +82,7 @@ struct BOpPre {
   }
   __device__ void finish_sys(int s, double* tot) const {
     a.xpend[s] = 0;
+    if (a.xprev) a.xprev[s] = 0;
     a.bnorm[s] = sqrt(tot[0]);
     double e = eps_abs;
     const double er = eps_rel_sys ? eps_rel_sys[s] : eps_rel;
@@ -247,6 +252,127 @@ struct BOpDirection {
   __device__ void finish_sys(int, double*) const {}
   __device__ void finish_global() const {}
 };
+
+// The FP64 direction sweeps for a pair of iterations whose directions live
+// in two vectors, p_k in p and p_k+1 in q.  The even sweep writes p_k+1 =
+// beta p_k + J r into q; a system that goes on keeps its x += sigma_k p_k
+// pending (defer_marks_kernel moves the mark to xprev with sigma_k), and a
+// system that the update sweep just stopped gets its update at once.  The
+// odd sweep applies x = (x + sigma_k p_k) + sigma_k+1 p_k+1 and writes p_k+2
+// over p_k.  x is read and stored once per two iterations, and each element
+// gets the same roundings in the same order as with BOpDirection.
+// TileInfo.act of the odd sweep: bit 0 active, bit 1 x pending, bit 2 the
+// even iteration's update pending; s = beta, s2 = sigma, s3 = sigma_k.
+template <typename VT>
+struct BOpDirectionDefer {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { VT p, r, J, x; };
+  const VT* p;
+  VT* q;
+  const VT* r;
+  const VT* J;
+  VT* x;
+  BatchArgs a;
+  double bt = 0.0, sg = 0.0;
+  int act = 0, xp = 0;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    const int f = (*(volatile int*)&a.active[s] != 0 ? 1 : 0) |
+                  (*(volatile int*)&a.xpend[s] != 0 ? 2 : 0);
+    return TileInfo{f, a.beta[s], a.sigma[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) {
+    act = ti.act & 1;
+    xp = ti.act & 2;
+    bt = ti.s;
+    sg = ti.s2;
+  }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  // p_k is read again by the odd sweep, after the next SpMV: streamed
+  __device__ void load(long i, Regs& g) const {
+    g.p = __ldcs(p + i);
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldg(J + i);
+    } else if (xp) {
+      g.x = __ldcs(x + i);
+    }
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (act) q[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
+    else if (xp) __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
+  }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+template <typename VT>
+struct BOpDirectionPair {
+  static constexpr int NRED = 0;
+  static constexpr bool kBatched = true;
+  struct Regs { VT p, q, r, J, x; };
+  VT* p;
+  const VT* q;
+  const VT* r;
+  const VT* J;
+  VT* x;
+  BatchArgs a;
+  double bt = 0.0, sg = 0.0, sp = 0.0;
+  int act = 0, xp = 0, xq = 0;
+  __device__ bool prepare() { return true; }
+  __device__ TileInfo tile_info(long t) const {
+    const int s = a.sys_of(t);
+    const int f = (*(volatile int*)&a.active[s] != 0 ? 1 : 0) |
+                  (*(volatile int*)&a.xpend[s] != 0 ? 2 : 0) |
+                  (*(volatile int*)&a.xprev[s] != 0 ? 4 : 0);
+    return TileInfo{f, a.beta[s], a.sigma[s], a.sigprev[s]};
+  }
+  __device__ void begin_tile(const TileInfo& ti) {
+    act = ti.act & 1;
+    xp = ti.act & 2;
+    xq = ti.act & 4;
+    bt = ti.s;
+    sg = ti.s2;
+    sp = ti.s3;
+  }
+  __device__ bool sys_active(int) const { return false; }
+  __device__ const BatchRed& bred() const { return a.br; }
+  __device__ void load(long i, Regs& g) const {
+    if (xq) g.p = __ldcs(p + i);
+    if (xp || act) g.q = __ldcs(q + i);
+    if (act) {
+      g.r = __ldcs(r + i);
+      g.J = __ldg(J + i);
+    }
+    if (xq || xp) g.x = __ldcs(x + i);
+  }
+  __device__ void compute(long i, Regs& g, double*) const {
+    if (xq || xp) {
+      VT xv = g.x;
+      if (xq) xv = R<VT>(dadd(D(xv), dmul(sp, D(g.p))));
+      if (xp) xv = R<VT>(dadd(D(xv), dmul(sg, D(g.q))));
+      __stcs(x + i, xv);
+    }
+    if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.q)), dmul(D(g.r), D(g.J))));
+  }
+  __device__ void finish_sys(int, double*) const {}
+  __device__ void finish_global() const {}
+};
+
+// After the even sweep: a system whose update is still pending and that goes
+// on owes it to the odd sweep (xprev, sigprev); every xpend mark is cleared.
+__global__ void defer_marks_kernel(int count, int* xpend, int* xprev, const int* active,
+                                   const double* sigma, double* sigprev) {
+  for (int s = threadIdx.x; s < count; s += blockDim.x) {
+    const int d = xpend[s] != 0 && active[s] != 0;
+    if (d) sigprev[s] = sigma[s];
+    xprev[s] = d;
+    xpend[s] = 0;
+  }
+}
 
 __global__ void clear_marks_kernel(int* marks, int count) {
   for (int s = threadIdx.x; s < count; s += blockDim.x) marks[s] = 0;
@@ -701,8 +827,9 @@ struct Batch {
   double *B = nullptr, *X = nullptr, *R = nullptr, *P = nullptr, *V = nullptr;
   int* tile_arrays = nullptr;  // tile_sys[NT], sys_tile0[nsys], sys_ntiles[nsys]
   unsigned* sys_ticket = nullptr;
-  double* dstate = nullptr;    // 7 x nsys doubles
-  int* istate = nullptr;       // 3 x nsys ints + n_active + nsys pending marks
+  double* dstate = nullptr;    // 8 x nsys doubles
+  int* istate = nullptr;       // 3 x nsys ints + n_active + 2 x nsys pending marks
+  double* Q = nullptr;         // second direction of the paired FP64 sweeps
   int nlive = 0;               // systems with at least one row
   // launch shape picked by batch_tune (index into kBatchShapes, -1: not tuned)
   int shape = -1;
@@ -787,11 +914,11 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
   ok(cudaMalloc(&A.ci, sizeof(int) * ((size_t)NNZ + 8)));
   ok(cudaMalloc(&A.v, sizeof(double) * ((size_t)NNZ + 8)));
   ok(cudaMalloc(&bt->J, sizeof(double) * std::max<size_t>(N, 1)));
-  ok(cudaMalloc(&bt->B, sizeof(double) * std::max<size_t>(N, 1) * 5));
+  ok(cudaMalloc(&bt->B, sizeof(double) * std::max<size_t>(N, 1) * 6));
   ok(cudaMalloc(&bt->tile_arrays, sizeof(int) * ((size_t)bt->NT + 2 * (size_t)count + 1)));
   ok(cudaMalloc(&bt->sys_ticket, sizeof(unsigned) * (size_t)count));
-  ok(cudaMalloc(&bt->dstate, sizeof(double) * 7 * (size_t)count));
-  ok(cudaMalloc(&bt->istate, sizeof(int) * (4 * (size_t)count + 1)));
+  ok(cudaMalloc(&bt->dstate, sizeof(double) * 8 * (size_t)count));
+  ok(cudaMalloc(&bt->istate, sizeof(int) * (5 * (size_t)count + 1)));
   if (e != cudaSuccess) {
     batch_free(bt);
     return cuda_status(e, "batch allocation");
@@ -800,7 +927,8 @@ static int batch_build(celg_handle* h, int count, celg_mat* const* mats, const s
   bt->R = bt->X + N;
   bt->P = bt->R + N;
   bt->V = bt->P + N;
-  ok(cudaMemsetAsync(bt->B, 0, sizeof(double) * (size_t)N * 5, h->stream));
+  bt->Q = bt->V + N;
+  ok(cudaMemsetAsync(bt->B, 0, sizeof(double) * (size_t)N * 6, h->stream));
   ok(cudaMemsetAsync(A.ci + NNZ, 0, sizeof(int) * 8, h->stream));
   ok(cudaMemsetAsync(A.v + NNZ, 0, sizeof(double) * 8, h->stream));
   ok(cudaMemsetAsync(bt->sys_ticket, 0, sizeof(unsigned) * (size_t)count, h->stream));
@@ -895,6 +1023,8 @@ static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle 
   a.err = a.active + c;
   a.n_active = a.err + c;
   a.xpend = a.n_active + 1;
+  a.xprev = inner ? nullptr : a.xpend + c;
+  a.sigprev = inner ? nullptr : a.vres + c;
   a.br.tile_sys = bt->tile_arrays;
   a.br.sys_tile0 = bt->tile_arrays + bt->NT;
   a.br.sys_ntiles = bt->tile_arrays + bt->NT + c;
@@ -936,17 +1066,46 @@ static int batch_setup(celg_handle* h, Batch* bt, int x0_mode, double eps_abs, d
 }
 
 // One iteration of every running system: K1, sigma, K2, beta and the test,
-// K3 (with the deferred x update), then the pending marks cleared.
-static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a) {
-  const BEpiAp<double> ap{bt->V, bt->P, a};
+// K3 (with the deferred x update), then the pending marks cleared.  Phase 0:
+// one iteration with BOpDirection; phases 1 and 2: the even and the odd
+// iteration of a pair, directions in P and then in Q.
+static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a, int phase = 0) {
+  double* pc = phase == 2 ? bt->Q : bt->P;
+  const BEpiAp<double> ap{bt->V, pc, a};
   const BOpUpdate<double> upd{bt->R, bt->V, bt->J, a, 0.0};
-  int s2 = batch_csr<double>(h, bt, bt->A.v, bt->P, ap);
+  int s2 = batch_csr<double>(h, bt, bt->A.v, pc, ap);
   if (!s2) s2 = batch_finish(h, bt, ap);
   if (!s2) s2 = batch_tile(h, bt, upd);
   if (!s2) s2 = batch_finish(h, bt, upd);
-  if (!s2) s2 = batch_tile(h, bt, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
+  if (s2) return s2;
+  if (phase == 1) {
+    s2 = batch_tile(h, bt, BOpDirectionDefer<double>{bt->P, bt->Q, bt->R, bt->J, bt->X, a});
+    if (!s2) {
+      defer_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.nsys, a.xpend, a.xprev, a.active, a.sigma,
+                                                      a.sigprev);
+      CELG_CUDA(cudaGetLastError());
+    }
+    return s2;
+  }
+  if (phase == 2) {
+    s2 = batch_tile(h, bt, BOpDirectionPair<double>{bt->P, bt->Q, bt->R, bt->J, bt->X, a});
+    if (!s2) {
+      // xpend and xprev are adjacent
+      clear_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.xpend, 2 * a.nsys);
+      CELG_CUDA(cudaGetLastError());
+    }
+    return s2;
+  }
+  s2 = batch_tile(h, bt, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
   if (!s2) s2 = clear_marks(h, a);
   return s2;
+}
+
+// A pair of iterations (the loop body of the FP64 solve).
+static int batch_pair(celg_handle* h, Batch* bt, const BatchArgs& a) {
+  int st = batch_iteration(h, bt, a, 1);
+  if (!st) st = batch_iteration(h, bt, a, 2);
+  return st;
 }
 
 // The batch tuner: times a few iterations of the batch's own systems with
@@ -976,10 +1135,10 @@ static int batch_tune(celg_handle* h, Batch* bt, const double* const* b_d) {
   for (int c = 0; c < kNumBatchShapes && !st; ++c) {
     bt->shape = c;
     st = batch_setup(h, bt, CELG_X0_ZERO, 0.0, 0.0, a);
-    if (!st) st = batch_iteration(h, bt, a);  // warm-up
+    if (!st) st = batch_pair(h, bt, a);  // warm-up
     if (st) break;
     cudaEventRecord(e0, h->stream);
-    for (int k = 0; k < 4 && !st; ++k) st = batch_iteration(h, bt, a);
+    for (int k = 0; k < 2 && !st; ++k) st = batch_pair(h, bt, a);
     cudaEventRecord(e1, h->stream);
     if (cudaEventSynchronize(e1) != cudaSuccess) st = CELG_ERR_CUDA;
     float ms = 0.f;
@@ -1006,10 +1165,10 @@ static int record_batched(celg_handle* h, Batch* bt, const double* const* b_d, d
                                 cudaMemcpyDeviceToDevice, h->stream));
   }
   int st = batch_setup(h, bt, p->x0_mode, p->eps_abs, p->eps_rel, a);
-  auto body = [&]() -> int { return batch_iteration(h, bt, a); };
-  if (!st && a.cond) st = capture_while2(h, a.cond, body);
+  auto body = [&]() -> int { return batch_pair(h, bt, a); };
+  if (!st && a.cond) st = capture_while(h, a.cond, body);
   for (int it = 0; !st && !a.cond && it < p->iter_max; it += 8) {
-    for (int q = 0; q < 8 && !st; ++q) st = body();
+    for (int q = 0; q < 4 && !st; ++q) st = body();
     int live = 0;
     if (!st) {
       CELG_CUDA(cudaMemcpyAsync(&live, a.n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));

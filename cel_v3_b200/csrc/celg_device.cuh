@@ -366,6 +366,7 @@ struct TileInfo {
   int act;
   double s;
   double s2 = 0.0;
+  double s3 = 0.0;
 };
 
 template <class T, class = void>
