@@ -1023,8 +1023,8 @@ static BatchArgs batch_args(Batch* bt, int iter_max, cudaGraphConditionalHandle 
   a.err = a.active + c;
   a.n_active = a.err + c;
   a.xpend = a.n_active + 1;
-  a.xprev = inner ? nullptr : a.xpend + c;
-  a.sigprev = inner ? nullptr : a.vres + c;
+  a.xprev = a.xpend + c;
+  a.sigprev = a.vres + c;
   a.br.tile_sys = bt->tile_arrays;
   a.br.sys_tile0 = bt->tile_arrays + bt->NT;
   a.br.sys_ntiles = bt->tile_arrays + bt->NT + c;
@@ -1054,6 +1054,25 @@ static int clear_marks(celg_handle* h, const BatchArgs& a) {
   return CELG_OK;
 }
 
+// The direction sweep of the even (odd = false) or odd iteration of a pair,
+// with the marks moved or cleared after it (xpend and xprev are adjacent).
+template <typename VT>
+static int batch_direction_pair(celg_handle* h, const Batch* bt, const BatchArgs& a, bool odd, VT* P,
+                                VT* Q, const VT* R, const VT* J, VT* X) {
+  if (!odd) {
+    const int st = batch_tile(h, bt, BOpDirectionDefer<VT>{P, Q, R, J, X, a});
+    if (st) return st;
+    defer_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.nsys, a.xpend, a.xprev, a.active, a.sigma,
+                                                    a.sigprev);
+  } else {
+    const int st = batch_tile(h, bt, BOpDirectionPair<VT>{P, Q, R, J, X, a});
+    if (st) return st;
+    clear_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.xpend, 2 * a.nsys);
+  }
+  CELG_CUDA(cudaGetLastError());
+  return CELG_OK;
+}
+
 // x0, ||b||, eps, then r = b - A x, p = J r and the first scalars per system
 static int batch_setup(celg_handle* h, Batch* bt, int x0_mode, double eps_abs, double eps_rel,
                        const BatchArgs& a) {
@@ -1078,24 +1097,7 @@ static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a, int ph
   if (!s2) s2 = batch_tile(h, bt, upd);
   if (!s2) s2 = batch_finish(h, bt, upd);
   if (s2) return s2;
-  if (phase == 1) {
-    s2 = batch_tile(h, bt, BOpDirectionDefer<double>{bt->P, bt->Q, bt->R, bt->J, bt->X, a});
-    if (!s2) {
-      defer_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.nsys, a.xpend, a.xprev, a.active, a.sigma,
-                                                      a.sigprev);
-      CELG_CUDA(cudaGetLastError());
-    }
-    return s2;
-  }
-  if (phase == 2) {
-    s2 = batch_tile(h, bt, BOpDirectionPair<double>{bt->P, bt->Q, bt->R, bt->J, bt->X, a});
-    if (!s2) {
-      // xpend and xprev are adjacent
-      clear_marks_kernel<<<1, kLanes, 0, h->stream>>>(a.xpend, 2 * a.nsys);
-      CELG_CUDA(cudaGetLastError());
-    }
-    return s2;
-  }
+  if (phase) return batch_direction_pair<double>(h, bt, a, phase == 2, bt->P, bt->Q, bt->R, bt->J, bt->X);
   s2 = batch_tile(h, bt, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
   if (!s2) s2 = clear_marks(h, a);
   return s2;
@@ -1309,12 +1311,12 @@ static int batch_ensure_f32(celg_handle* h, Batch* bt) {
   auto ok = [&](cudaError_t x) { if (e == cudaSuccess) e = x; return e == cudaSuccess; };
   ok(cudaMalloc(&bt->A.v32, sizeof(float) * (NNZ + 32)));
   ok(cudaMalloc(&bt->J32, sizeof(float) * N));
-  ok(cudaMalloc(&bt->F, sizeof(float) * N * 5));
+  ok(cudaMalloc(&bt->F, sizeof(float) * N * 6));
   ok(cudaMalloc(&bt->irs, sizeof(int) * (5 * c + 1)));
   ok(cudaMalloc(&bt->irtau, sizeof(double) * c));
-  ok(cudaMalloc(&bt->dstate2, sizeof(double) * 7 * c));
-  ok(cudaMalloc(&bt->istate2, sizeof(int) * (4 * c + 1)));
-  ok(cudaMemsetAsync(bt->F, 0, sizeof(float) * N * 5, h->stream));
+  ok(cudaMalloc(&bt->dstate2, sizeof(double) * 8 * c));
+  ok(cudaMalloc(&bt->istate2, sizeof(int) * (5 * c + 1)));
+  ok(cudaMemsetAsync(bt->F, 0, sizeof(float) * N * 6, h->stream));
   ok(cudaMemsetAsync(bt->A.v32 + NNZ, 0, sizeof(float) * 32, h->stream));
   if (e != cudaSuccess) return cuda_status(e, "batch FP32 allocation");
   int st = launch_to_f32(h, (long)NNZ, bt->A.v, bt->A.v32);
@@ -1322,13 +1324,14 @@ static int batch_ensure_f32(celg_handle* h, Batch* bt) {
   return st;
 }
 
+// `pair` records two iterations
 template <class Body>
 static int run_while(celg_handle* h, cudaGraphConditionalHandle cond, const int* n_active, int iter_max,
-                     Body&& body) {
-  if (cond) return capture_while2(h, cond, body);
+                     Body&& pair) {
+  if (cond) return capture_while(h, cond, pair);
   for (int it = 0; it < iter_max; it += 8) {
     int st = CELG_OK;
-    for (int q = 0; q < 8 && !st; ++q) st = body();
+    for (int q = 0; q < 4 && !st; ++q) st = pair();
     if (st) return st;
     int live = 0;
     CELG_CUDA(cudaMemcpyAsync(&live, n_active, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -1345,10 +1348,10 @@ static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, Ba
   float* R32 = D32 + N;
   float* P32 = R32 + N;
   float* V32 = P32 + N;
+  float* Q32 = V32 + N;  // second direction of the paired sweeps
   const BOpPre<float> pre{B32, D32, CELG_X0_ZERO, 0.0, ir.tau, ai, ir.part, ir.part_count,
                           ir.tau_sys};
   const BEpiInit<float> init{B32, R32, P32, bt->J32, ai};
-  const BEpiAp<float> ap{V32, P32, ai};
   const BOpUpdate<float> upd{R32, V32, bt->J32, ai, 0.0};
   int st = launch_tile(h, N, pre);
   if (!st) st = batch_finish(h, bt, pre);
@@ -1356,12 +1359,16 @@ static int record_batched_inner(celg_handle* h, Batch* bt, const IrState& ir, Ba
   if (!st) st = batch_finish(h, bt, init);
   if (!st)
     st = run_while(h, ai.cond, ai.n_active, ai.iter_max, [&]() -> int {
-      int s2 = batch_csr<float>(h, bt, bt->A.v32, P32, ap);
-      if (!s2) s2 = batch_finish(h, bt, ap);
-      if (!s2) s2 = batch_tile(h, bt, upd);
-      if (!s2) s2 = batch_finish(h, bt, upd);
-      if (!s2) s2 = batch_tile(h, bt, BOpDirection<float>{P32, R32, bt->J32, D32, ai});
-      if (!s2) s2 = clear_marks(h, ai);
+      int s2 = CELG_OK;
+      for (int odd = 0; odd < 2 && !s2; ++odd) {
+        float* pc = odd ? Q32 : P32;
+        const BEpiAp<float> ap{V32, pc, ai};
+        s2 = batch_csr<float>(h, bt, bt->A.v32, pc, ap);
+        if (!s2) s2 = batch_finish(h, bt, ap);
+        if (!s2) s2 = batch_tile(h, bt, upd);
+        if (!s2) s2 = batch_finish(h, bt, upd);
+        if (!s2) s2 = batch_direction_pair<float>(h, bt, ai, odd != 0, P32, Q32, R32, bt->J32, D32);
+      }
       return s2;
     });
   return st;
