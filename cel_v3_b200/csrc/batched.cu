@@ -206,61 +206,15 @@ struct BOpUpdate {
   __device__ void finish_global() const { set_cond(a.cond, *(volatile int*)a.n_active > 0); }
 };
 
-// K3: per system, x += sigma p when the update sweep left it pending (also
-// after that sweep stopped the system), then p = beta p + J r while the
-// system goes on.  TileInfo.act: bit 0 active, bit 1 x pending; s = beta,
-// s2 = sigma.  The marks are cleared by clear_marks_kernel after the sweep.
-template <typename VT>
-struct BOpDirection {
-  static constexpr int NRED = 0;
-  static constexpr bool kBatched = true;
-  struct Regs { VT p, r, J, x; };
-  VT* p;
-  const VT* r;
-  const VT* J;
-  VT* x;
-  BatchArgs a;
-  double bt = 0.0, sg = 0.0;
-  int act = 0, xp = 0;
-  __device__ bool prepare() { return true; }
-  __device__ TileInfo tile_info(long t) const {
-    const int s = a.sys_of(t);
-    const int f = (*(volatile int*)&a.active[s] != 0 ? 1 : 0) |
-                  (*(volatile int*)&a.xpend[s] != 0 ? 2 : 0);
-    return TileInfo{f, a.beta[s], a.sigma[s]};
-  }
-  __device__ void begin_tile(const TileInfo& ti) {
-    act = ti.act & 1;
-    xp = ti.act & 2;
-    bt = ti.s;
-    sg = ti.s2;
-  }
-  __device__ bool sys_active(int) const { return false; }
-  __device__ const BatchRed& bred() const { return a.br; }
-  __device__ void load(long i, Regs& g) const {
-    g.p = p[i];
-    if (act) {
-      g.r = __ldcs(r + i);
-      g.J = __ldg(J + i);
-    }
-    if (xp) g.x = __ldcs(x + i);
-  }
-  __device__ void compute(long i, Regs& g, double*) const {
-    if (xp) __stcs(x + i, R<VT>(dadd(D(g.x), dmul(sg, D(g.p)))));
-    if (act) p[i] = R<VT>(dadd(dmul(bt, D(g.p)), dmul(D(g.r), D(g.J))));
-  }
-  __device__ void finish_sys(int, double*) const {}
-  __device__ void finish_global() const {}
-};
-
-// The FP64 direction sweeps for a pair of iterations whose directions live
-// in two vectors, p_k in p and p_k+1 in q.  The even sweep writes p_k+1 =
-// beta p_k + J r into q; a system that goes on keeps its x += sigma_k p_k
-// pending (defer_marks_kernel moves the mark to xprev with sigma_k), and a
-// system that the update sweep just stopped gets its update at once.  The
-// odd sweep applies x = (x + sigma_k p_k) + sigma_k+1 p_k+1 and writes p_k+2
-// over p_k.  x is read and stored once per two iterations, and each element
-// gets the same roundings in the same order as with BOpDirection.
+// K3: the direction sweeps for a pair of iterations whose directions live
+// in two vectors, p_k in p and p_k+1 in q (FP64 solve, FP32 inner solves).
+// The even sweep writes p_k+1 = beta p_k + J r into q; a system that goes
+// on keeps its x += sigma_k p_k pending (defer_marks_kernel moves the mark
+// to xprev with sigma_k), and a system that the update sweep just stopped
+// gets its update at once.  The odd sweep applies x = (x + sigma_k p_k) +
+// sigma_k+1 p_k+1 and writes p_k+2 over p_k.  x is read and stored once per
+// two iterations, and each element gets the same roundings in the same
+// order as two consecutive x += sigma p.
 // TileInfo.act of the odd sweep: bit 0 active, bit 1 x pending, bit 2 the
 // even iteration's update pending; s = beta, s2 = sigma, s3 = sigma_k.
 template <typename VT>
@@ -1085,11 +1039,10 @@ static int batch_setup(celg_handle* h, Batch* bt, int x0_mode, double eps_abs, d
 }
 
 // One iteration of every running system: K1, sigma, K2, beta and the test,
-// K3 (with the deferred x update), then the pending marks cleared.  Phase 0:
-// one iteration with BOpDirection; phases 1 and 2: the even and the odd
-// iteration of a pair, directions in P and then in Q.
-static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a, int phase = 0) {
-  double* pc = phase == 2 ? bt->Q : bt->P;
+// then K3 with the marks moved or cleared after it: the even (odd = false)
+// or the odd iteration of a pair, directions in P and then in Q.
+static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a, bool odd) {
+  double* pc = odd ? bt->Q : bt->P;
   const BEpiAp<double> ap{bt->V, pc, a};
   const BOpUpdate<double> upd{bt->R, bt->V, bt->J, a, 0.0};
   int s2 = batch_csr<double>(h, bt, bt->A.v, pc, ap);
@@ -1097,16 +1050,13 @@ static int batch_iteration(celg_handle* h, Batch* bt, const BatchArgs& a, int ph
   if (!s2) s2 = batch_tile(h, bt, upd);
   if (!s2) s2 = batch_finish(h, bt, upd);
   if (s2) return s2;
-  if (phase) return batch_direction_pair<double>(h, bt, a, phase == 2, bt->P, bt->Q, bt->R, bt->J, bt->X);
-  s2 = batch_tile(h, bt, BOpDirection<double>{bt->P, bt->R, bt->J, bt->X, a});
-  if (!s2) s2 = clear_marks(h, a);
-  return s2;
+  return batch_direction_pair<double>(h, bt, a, odd, bt->P, bt->Q, bt->R, bt->J, bt->X);
 }
 
 // A pair of iterations (the loop body of the FP64 solve).
 static int batch_pair(celg_handle* h, Batch* bt, const BatchArgs& a) {
-  int st = batch_iteration(h, bt, a, 1);
-  if (!st) st = batch_iteration(h, bt, a, 2);
+  int st = batch_iteration(h, bt, a, false);
+  if (!st) st = batch_iteration(h, bt, a, true);
   return st;
 }
 
