@@ -906,6 +906,7 @@ extern "C" int celg_solve_host(celg_handle* h, celg_mat* m, int solver, const do
     cudaFree(h->sb);
     cudaFree(h->sx);
     h->sb = h->sx = nullptr;
+    h->scap = 0;  // a failed allocation below leaves no stale capacity behind
     const size_t cap = std::max<size_t>(n, 1024);
     CELG_CUDA(cudaMalloc(&h->sb, sizeof(double) * cap));
     CELG_CUDA(cudaMalloc(&h->sx, sizeof(double) * cap));

@@ -1536,10 +1536,8 @@ static int pcg_batched_ru(celg_handle* h, int count, celg_mat* const* mats, cons
   if (!st) st = batch_ensure_f32(h, bt);
   if (st) return st;
   const int c = bt->nsys;
-  if (!bt->rud) {
-    CELG_CUDA(cudaMalloc(&bt->rud, sizeof(double) * 3 * (size_t)c));
-    CELG_CUDA(cudaMalloc(&bt->rui, sizeof(int) * (2 * (size_t)c + 1)));
-  }
+  if (!bt->rud) CELG_CUDA(cudaMalloc(&bt->rud, sizeof(double) * 3 * (size_t)c));
+  if (!bt->rui) CELG_CUDA(cudaMalloc(&bt->rui, sizeof(int) * (2 * (size_t)c + 1)));
   BatchRu u;
   u.maxr = bt->rud;
   u.rz_prev = u.maxr + c;

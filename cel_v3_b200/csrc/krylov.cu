@@ -417,10 +417,8 @@ int cg_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
 // V[0..M], Z[0..M-1] and H ((M+1) x M), plus the device state.
 static int ensure_gmres_work(celg_handle* h, size_t nn, int M) {
   const size_t need = nn * (size_t)(2 * M + 1) + (size_t)(M + 1) * M + 8;
-  if (!h->gm_state_d) {
-    CELG_CUDA(cudaMalloc(&h->gm_state_d, sizeof(GmState)));
-    CELG_CUDA(cudaMallocHost(&h->gm_state_h, sizeof(GmState)));
-  }
+  if (!h->gm_state_d) CELG_CUDA(cudaMalloc(&h->gm_state_d, sizeof(GmState)));
+  if (!h->gm_state_h) CELG_CUDA(cudaMallocHost(&h->gm_state_h, sizeof(GmState)));
   if (need <= h->gm_cap && h->gm_work) return CELG_OK;
   CELG_CUDA(cudaStreamSynchronize(h->stream));
   graph_cache_clear(h);

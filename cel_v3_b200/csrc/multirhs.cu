@@ -1998,10 +1998,8 @@ int pcg_multirhs(celg_handle* h, celg_mat* m, int k, const double* B, double* X,
     CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
     mu->cap = nk;
   }
-  if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
-  }
+  if (!mu->dstate) CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+  if (!mu->istate) CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
   if (nk > mu->qcap || !mu->work_q) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
     graph_cache_clear(h);
@@ -2204,10 +2202,8 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
     CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
     mu->cap = nk;
   }
-  if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
-  }
+  if (!mu->dstate) CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+  if (!mu->istate) CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
   if (nk > mu->f32cap || !mu->f32) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
     graph_cache_clear(h);
@@ -2216,12 +2212,10 @@ static int multirhs_ir(celg_handle* h, celg_mat* m, int k, const double* B, doub
     CELG_CUDA(cudaMalloc(&mu->f32, sizeof(float) * std::max<size_t>(nk, 1) * 5));
     mu->f32cap = nk;
   }
-  if (!mu->irs) {
-    CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
-    CELG_CUDA(cudaMalloc(&mu->irtau, sizeof(double) * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 8 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 3)));
-  }
+  if (!mu->irs) CELG_CUDA(cudaMalloc(&mu->irs, sizeof(int) * (5 * kMaxRhs + 1)));
+  if (!mu->irtau) CELG_CUDA(cudaMalloc(&mu->irtau, sizeof(double) * kMaxRhs));
+  if (!mu->dstate2) CELG_CUDA(cudaMalloc(&mu->dstate2, sizeof(double) * 8 * kMaxRhs));
+  if (!mu->istate2) CELG_CUDA(cudaMalloc(&mu->istate2, sizeof(int) * (3 * kMaxRhs + 3)));
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
   double* Rr = mu->work;
@@ -2345,10 +2339,8 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
     CELG_CUDA(cudaMalloc(&mu->work, sizeof(double) * std::max<size_t>(nk, 1) * 3));
     mu->cap = nk;
   }
-  if (!mu->dstate) {
-    CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
-  }
+  if (!mu->dstate) CELG_CUDA(cudaMalloc(&mu->dstate, sizeof(double) * 8 * kMaxRhs));
+  if (!mu->istate) CELG_CUDA(cudaMalloc(&mu->istate, sizeof(int) * (3 * kMaxRhs + 3)));
   if (nk > mu->f32cap || !mu->f32) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
     graph_cache_clear(h);
@@ -2357,10 +2349,8 @@ static int multirhs_ru(celg_handle* h, celg_mat* m, int k, const double* B, doub
     CELG_CUDA(cudaMalloc(&mu->f32, sizeof(float) * std::max<size_t>(nk, 1) * 5));
     mu->f32cap = nk;
   }
-  if (!mu->rud) {
-    CELG_CUDA(cudaMalloc(&mu->rud, sizeof(double) * 3 * kMaxRhs));
-    CELG_CUDA(cudaMalloc(&mu->rui, sizeof(int) * (kMaxRhs + 1)));
-  }
+  if (!mu->rud) CELG_CUDA(cudaMalloc(&mu->rud, sizeof(double) * 3 * kMaxRhs));
+  if (!mu->rui) CELG_CUDA(cudaMalloc(&mu->rui, sizeof(int) * (kMaxRhs + 1)));
   int st = ensure_partials(h, ntiles_of(n), 2 * k);
   if (st) return st;
   float* D32 = mu->f32;

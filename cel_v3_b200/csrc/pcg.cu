@@ -45,6 +45,7 @@ int ensure_work(celg_handle* h, size_t n) {
   cudaFree(h->wv);
   cudaFree(h->wq);
   h->wr = h->wp = h->wv = h->wq = nullptr;
+  h->wcap = 0;  // a failed allocation below leaves no stale capacity behind
   const size_t cap = std::max<size_t>(n, 1024);
   CELG_CUDA(cudaMalloc(&h->wr, cap * sizeof(double)));
   CELG_CUDA(cudaMalloc(&h->wp, cap * sizeof(double)));
@@ -55,15 +56,14 @@ int ensure_work(celg_handle* h, size_t n) {
 }
 
 int ensure_state(celg_handle* h, int hist_cap) {
-  if (!h->state_d) {
-    CELG_CUDA(cudaMalloc(&h->state_d, sizeof(PcgState)));
-    CELG_CUDA(cudaMallocHost(&h->state_h, sizeof(PcgState)));
-  }
+  if (!h->state_d) CELG_CUDA(cudaMalloc(&h->state_d, sizeof(PcgState)));
+  if (!h->state_h) CELG_CUDA(cudaMallocHost(&h->state_h, sizeof(PcgState)));
   if (hist_cap > h->hist_cap) {
     CELG_CUDA(cudaStreamSynchronize(h->stream));
     graph_cache_clear(h);
     cudaFree(h->hist_d);
     h->hist_d = nullptr;
+    h->hist_cap = 0;
     CELG_CUDA(cudaMalloc(&h->hist_d, sizeof(double) * (size_t)hist_cap));
     h->hist_cap = hist_cap;
   }

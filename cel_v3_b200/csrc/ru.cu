@@ -331,10 +331,8 @@ int ru_solve(celg_handle* h, celg_mat* m, const double* b, double* x, const celg
   const int hist_cap = p->iter_max + 1;
   if (!st) st = ensure_state(h, hist_cap);
   if (st) return st;
-  if (!h->ru_state_d) {
-    CELG_CUDA(cudaMalloc(&h->ru_state_d, sizeof(RuState)));
-    CELG_CUDA(cudaMallocHost(&h->ru_state_h, sizeof(RuState)));
-  }
+  if (!h->ru_state_d) CELG_CUDA(cudaMalloc(&h->ru_state_d, sizeof(RuState)));
+  if (!h->ru_state_h) CELG_CUDA(cudaMallocHost(&h->ru_state_h, sizeof(RuState)));
   RuState* sd = static_cast<RuState*>(h->ru_state_d);
   RuState* sh = static_cast<RuState*>(h->ru_state_h);
   const size_t cap = h->f32cap;
