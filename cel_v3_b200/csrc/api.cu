@@ -233,14 +233,16 @@ static int build_row_patterns(celg_handle* h, CsrDev& A) {
   CELG_CUDA(cudaMalloc(&table, sizeof(unsigned long long) * kPatSlots + 2 * sizeof(int)));
   int* flags = reinterpret_cast<int*>(table + kPatSlots);
   std::vector<unsigned long long> init(kPatSlots, kPatEmpty);
-  CELG_CUDA(cudaMemcpyAsync(table, init.data(), sizeof(unsigned long long) * kPatSlots,
-                            cudaMemcpyHostToDevice, h->stream));
-  CELG_CUDA(cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream));
-  pat_set_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci8, table, flags);
+  cudaError_t e = cudaMemcpyAsync(table, init.data(), sizeof(unsigned long long) * kPatSlots,
+                                  cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(flags, 0, 2 * sizeof(int), h->stream);
+  if (e == cudaSuccess) {
+    pat_set_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci8, table, flags);
+    e = cudaGetLastError();
+  }
   std::vector<unsigned long long> out(kPatSlots);
   int fl[2] = {0, 0};
   std::vector<int> dict(A.ndict);
-  cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(out.data(), table, sizeof(unsigned long long) * kPatSlots,
                         cudaMemcpyDeviceToHost, h->stream);
@@ -322,13 +324,25 @@ int build_offset_dict_csr(celg_handle* h, CsrDev& A) {
   for (int q = 0; q < kOffSlots; ++q)
     if (out[q] != kOffEmpty) dict.push_back(out[q]);
   std::sort(dict.begin(), dict.end());
-  CELG_CUDA(cudaMalloc(&A.dict, sizeof(int) * dict.size()));
-  CELG_CUDA(cudaMalloc(&A.ci8, (size_t)A.nnz + 32));
-  CELG_CUDA(cudaMemsetAsync(A.ci8 + A.nnz, 0, 32, h->stream));
-  CELG_CUDA(cudaMemcpyAsync(A.dict, dict.data(), sizeof(int) * dict.size(), cudaMemcpyHostToDevice, h->stream));
+  // on any failure the matrix keeps its int32 columns only
+  e = cudaMalloc(&A.dict, sizeof(int) * dict.size());
+  if (e == cudaSuccess) e = cudaMalloc(&A.ci8, (size_t)A.nnz + 32);
+  if (e == cudaSuccess) e = cudaMemsetAsync(A.ci8 + A.nnz, 0, 32, h->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(A.dict, dict.data(), sizeof(int) * dict.size(), cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    offset_index_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci, A.dict,
+                                                               (int)dict.size(), A.ci8);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    cudaFree(A.ci8);
+    cudaFree(A.dict);
+    A.ci8 = nullptr;
+    A.dict = nullptr;
+    return cuda_status(e, "offset dictionary");
+  }
   A.ndict = (int)dict.size();
-  offset_index_kernel<<<ew_grid(h, A.n), 256, 0, h->stream>>>(A.n, A.rp, A.ci, A.dict, A.ndict, A.ci8);
-  CELG_CUDA(cudaGetLastError());
   A.cap_dict = (A.cap + 24 + 15) & ~15;  // 16-entry aligned spans are at most 24 entries wider
   return build_row_patterns(h, A);
 }
